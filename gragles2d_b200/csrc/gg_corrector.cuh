@@ -1,0 +1,432 @@
+// Anisotropic velocity corrector of the convolution stage
+// (LSbox::executeConvolution, src/box.cpp:428-531): per grain, contour
+// sectors around the previous step's junctions are built by one thread into
+// shared memory, then every pixel projects onto the previous contour and
+// blends its convolved value with the sector / junction / boundary weight.
+#pragma once
+
+#include "gg_grain.cuh"
+#include "gg_kernels.cuh"
+
+namespace gg {
+namespace {  // internal linkage: each form's translation unit has its own copy
+
+
+constexpr int kMaxConstSectors = 32;
+constexpr int kMaxSectorJunctions = 48;
+constexpr int kMaxInterpSectors = 2 * kMaxConstSectors;
+
+struct ConstSector {
+    int left, right;  // contour point IDs (-1, -1: whole contour)
+    int nj;
+    int js[kMaxSectorJunctions];
+    double weight;
+};
+
+struct InterpSector {
+    int left, right;
+    int lb, rb;  // left/right boundary constant sector (-1 if none)
+    double length;
+    double left_w, right_w, boundary_w;
+};
+
+struct SectorSet {
+    int nconst, ninterp;
+    uint32_t status;
+    ConstSector cs[kMaxConstSectors];
+    InterpSector is[kMaxInterpSectors];
+};
+
+// characteristics lookup of ExplicitGrainBoundary::getDirectNeighbourCaracteristic
+// (src/grainBoundary.cpp:561-571): by grain ID; a removed grain matches
+// nothing; absent -> default (energy 1, mobility 1).
+__device__ __forceinline__ const Neighbour* find_characteristic(const NetConst& C, int owner, int id) {
+    if (id < 0 || id > C.N || (id != 0 && C.state[id] == G_GONE)) return nullptr;
+    if (owner == 0) return nullptr;  // the boundary grain keeps no neighbour list
+    const Neighbour* nb = C.nb + (int64_t)owner * C.nbmax;
+    const int n = C.nb_n[owner];
+    for (int e = 0; e < n; ++e)
+        if (nb[e].id == id) return &nb[e];
+    return nullptr;
+}
+
+// LSbox::getGBEnergyTimesGBMobility(LSbox*) (src/box.cpp:554-561)
+__device__ __forceinline__ double gb_weight_for(const NetConst& C, int owner, int id) {
+    const Neighbour* c = find_characteristic(C, owner, id);
+    const double e = c ? c->energy : 1.0, mo = c ? c->mobility : 1.0;
+    if (e * mo > 0.01) return e * mo;
+    return 0.01;
+}
+
+// LSbox::getGBEnergyTimesGBMobility(int i, int j) (src/box.cpp:543-553): the
+// IDLocal entry at (row, col) of the previous step's box.
+__device__ __forceinline__ double gb_weight_at(const NetConst& C, int owner, const uint32_t* idl, const Box& ib,
+                                               int row, int col, uint32_t* status) {
+    uint32_t k;
+    if (!buf_index(ib, row, col, &k)) {
+        *status |= S_INDEX;
+        return 1.0;
+    }
+    const uint32_t id = idl[k];
+    if (id > (uint32_t)C.N) return gb_weight_for(C, owner, -1);
+    return gb_weight_for(C, owner, (int)id);
+}
+
+// GrainJunction::getWeight (src/junction.cpp:23-192), mode 4, ResearchMode 0,
+// ResearchProject 0, no twin identification.
+__device__ double junction_weight(const NetConst& C, const Junction& J, int me, uint32_t* status) {
+    uint32_t nbr[4] = {0xFFFFFFu, 0xFFFFFFu, 0xFFFFFFu, 0xFFFFFFu};
+    for (int i = 0, j = 0; i < J.type && i < 4; i++) {
+        if ((uint32_t)me != J.grains[i]) {
+            nbr[j] = J.grains[i];
+            j++;
+        }
+    }
+    if (nbr[0] == 0xFFFFFFu || nbr[1] == 0xFFFFFFu) return 1;
+    const int n0 = (int)nbr[0], n1 = (int)nbr[1];
+    if (n0 > C.N || n1 > C.N) {
+        *status |= S_INDEX;
+        return 1;
+    }
+    if ((n0 != 0 && C.state[n0] == G_GONE) || (n1 != 0 && C.state[n1] == G_GONE)) *status |= S_INDEX;
+    const double* qm = C.quat + 4 * (int64_t)me;
+    const double* q0 = C.quat + 4 * (int64_t)n0;
+    const double* q1 = C.quat + 4 * (int64_t)n1;
+    double averageMobility = 0;
+    double gamma[3];
+    double theta = grain_misorientation(qm, q0);
+    averageMobility += mobility_model(theta, C);
+    gamma[0] = read_shockley(theta, C);
+    theta = grain_misorientation(q0, q1);
+    const Neighbour* c01 = find_characteristic(C, n0, n1);
+    averageMobility += c01 ? c01->mobility : 1.0;
+    gamma[1] = read_shockley(theta, C);
+    theta = grain_misorientation(qm, q1);
+    averageMobility += mobility_model(theta, C);
+    gamma[2] = read_shockley(theta, C);
+    double sigma = gamma[0] - gamma[1] + gamma[2];
+    if (!C.isotropic) {
+        if (C.use_mobility_model > 0 && C.tpd > 0) {
+            averageMobility /= 3;
+            const double drag = 1 / ((1 / (C.ds * C.tpd)) + 1 / averageMobility);
+            sigma *= drag;
+        }
+    }
+    if (sigma < 0.01) sigma = 0.01;
+    return sigma;
+}
+
+__device__ __forceinline__ double seg_len(const CPoint* P, int a, int b) {
+    const double dx = P[a].x - P[b].x, dy = P[a].y - P[b].y;
+    return sqrt(dx * dx + dy * dy);
+}
+
+// ContourSector::isSegmentWithinSector (src/contourSector.cpp:184-198)
+__device__ __forceinline__ bool within(int left, int right, int totalP, int segment) {
+    if (right == left && left == -1) return true;
+    if (right > left) return (segment >= 0 && segment <= left) || (segment >= right && segment < totalP);
+    return segment >= right && segment <= left;
+}
+
+// ExplicitGrainBoundary::setPointsOnBoundary (src/grainBoundary.cpp:524-559)
+__device__ void set_points_on_boundary(const CPoint* P, int size, const Junction& J0, double h, double csr,
+                                       int* left, int* right, uint32_t* status) {
+    const int guard = 4 * size + 8;
+    double dist = 0;
+    int l = J0.segment;
+    {
+        const int nx = periodic(l + 1, size);
+        const double dx = (P[nx].x - P[l].x) * (1 - J0.lambda), dy = (P[nx].y - P[l].y) * (1 - J0.lambda);
+        dist += sqrt(dx * dx + dy * dy) * h;
+    }
+    l = periodic(l + 1, size);
+    int it = 0;
+    while (dist < csr) {
+        dist += seg_len(P, periodic(l + 1, size), l) * h;
+        l = periodic(l + 1, size);
+        if (++it > guard) {
+            *status |= S_WALK_LIMIT;
+            break;
+        }
+    }
+    dist = 0;
+    int r = J0.segment;
+    {
+        const int nx = periodic(r + 1, size);
+        const double dx = (P[nx].x - P[r].x) * J0.lambda, dy = (P[nx].y - P[r].y) * J0.lambda;
+        dist += sqrt(dx * dx + dy * dy) * h;
+    }
+    r = periodic(r, size);
+    it = 0;
+    while (dist < csr) {
+        dist += seg_len(P, periodic(r - 1, size), r) * h;
+        r = periodic(r - 1, size);
+        if (++it > guard) {
+            *status |= S_WALK_LIMIT;
+            break;
+        }
+    }
+    *right = r;
+    *left = l;
+}
+
+// ExplicitGrainBoundary::buildBoundarySectors (src/grainBoundary.cpp:233-342)
+// plus the per-sector weights of ContourSector::getWeight
+// (src/contourSector.cpp:200-272) that do not depend on the pixel.
+__device__ void build_sectors(const NetConst& C, int g, const CPoint* P, int size, const Junction* J, int nj,
+                              const uint32_t* idl, const Box& ib, SectorSet& S) {
+    S.nconst = 0;
+    S.ninterp = 0;
+    S.status = 0;
+    if (nj == 0) return;
+    const double h = C.h;
+    const int real = size - 1;
+    const int guard = 4 * size + 8;
+    auto push_const = [&](int jidx) -> int {
+        if (S.nconst >= kMaxConstSectors) {
+            S.status |= S_JUNCTION_OVERFLOW;
+            return -1;
+        }
+        ConstSector& c = S.cs[S.nconst];
+        c.nj = 1;
+        c.js[0] = jidx;
+        set_points_on_boundary(P, size, J[jidx], h, C.csr, &c.left, &c.right, &S.status);
+        return S.nconst++;
+    };
+    auto merge = [&](ConstSector& c, int jidx) {
+        if (c.nj < kMaxSectorJunctions)
+            c.js[c.nj++] = jidx;
+        else
+            S.status |= S_JUNCTION_OVERFLOW;
+    };
+    push_const(0);
+    int cb = 0;
+    for (int i = 1; i < nj; i++) {
+        int cl, cr;  // current sector's contour points
+        set_points_on_boundary(P, size, J[i], h, C.csr, &cl, &cr, &S.status);
+        if (within(S.cs[cb].left, S.cs[cb].right, real, cr)) {
+            merge(S.cs[cb], i);
+            S.cs[cb].left = cl;
+            if (i == nj - 1) {
+                if (within(S.cs[0].left, S.cs[0].right, real, S.cs[cb].left)) {
+                    if (cb == 0) {
+                        S.cs[0].left = -1;
+                        S.cs[0].right = -1;
+                    } else {
+                        const int cnt = S.cs[cb].nj;
+                        for (int q = 0; q < cnt; q++) merge(S.cs[0], S.cs[cb].js[q]);
+                        S.cs[0].right = S.cs[cb].right;
+                    }
+                }
+            }
+        } else {
+            if (i == nj - 1 && within(S.cs[0].left, S.cs[0].right, real, cl)) {
+                S.cs[0].right = cr;
+                merge(S.cs[0], i);
+            } else {
+                const int k = push_const(i);
+                if (k >= 0) {
+                    S.cs[k].left = cl;
+                    S.cs[k].right = cr;
+                    cb++;
+                }
+            }
+        }
+    }
+    // constant-sector weights: mean of junction weights in list order
+    double jw[64];
+    for (int q = 0; q < nj && q < 64; ++q) jw[q] = junction_weight(C, J[q], g, &S.status);
+    for (int s = 0; s < S.nconst; ++s) {
+        double w = 0;
+        for (int q = 0; q < S.cs[s].nj; ++q) w += jw[S.cs[s].js[q] < 64 ? S.cs[s].js[q] : 63];
+        S.cs[s].weight = w / (double)S.cs[s].nj;
+    }
+    const int sec_len = S.nconst;
+    if (!(S.nconst > 1 || S.cs[0].left != S.cs[0].right)) return;
+    for (int i = 0; i < S.nconst && S.nconst > 1; i++) {
+        const int iR = i, iL = (i + 1 + sec_len) % sec_len;
+        const ConstSector& secR = S.cs[iR];
+        const ConstSector& secL = S.cs[iL];
+        // secR.generateLeftInterpolatingContour (src/contourSector.cpp:103-122)
+        InterpSector nr;
+        {
+            double dist = 0;
+            int j = secR.left, it = 0;
+            for (; dist <= C.isr; j = (j + 1 + real) % real) {
+                dist += seg_len(P, j, (j + 1 + real) % real) * h;
+                if (++it > guard) {
+                    S.status |= S_WALK_LIMIT;
+                    break;
+                }
+            }
+            nr.left = (j + 1 + real) % real;
+            nr.right = secR.left;
+            nr.lb = -1;
+            nr.rb = iR;
+            nr.length = dist;
+        }
+        // secL.generateRightInterpolatingContour (src/contourSector.cpp:145-168)
+        InterpSector nl;
+        {
+            double dist = 0;
+            int j = secL.right, it = 0;
+            for (; dist <= C.isr; j = (j - 1 + real) % real) {
+                dist += seg_len(P, j, (j - 1 + real) % real) * h;
+                if (++it > guard) {
+                    S.status |= S_WALK_LIMIT;
+                    break;
+                }
+            }
+            nl.left = secL.right;
+            nl.right = (j - 1 + real) % real;
+            nl.lb = iL;
+            nl.rb = -1;
+            nl.length = dist;
+        }
+        bool merged = false;
+        {
+            int it = 0;
+            for (int j = nr.right; j != periodic(nr.left + 1, size); j = periodic(j + 1, size)) {
+                if (j == nl.left || j == nl.right) merged = true;
+                if (++it > guard) {
+                    S.status |= S_WALK_LIMIT;
+                    break;
+                }
+            }
+        }
+        if (merged) {
+            // secL.generateInterpolatingSector(secR) (src/contourSector.cpp:124-143)
+            InterpSector r;
+            r.left = secL.right;
+            r.lb = iL;
+            r.right = secR.left;
+            r.rb = iR;
+            double dist = 0;
+            int it = 0;
+            for (int j = r.right; j != r.left; j = (j + 1 + real) % real) {
+                dist += seg_len(P, j, (j - 1 + real) % real) * h;
+                if (++it > guard) {
+                    S.status |= S_WALK_LIMIT;
+                    break;
+                }
+            }
+            r.length = dist;
+            if (S.ninterp < kMaxInterpSectors) S.is[S.ninterp++] = r; else S.status |= S_JUNCTION_OVERFLOW;
+        } else {
+            if (S.ninterp + 1 < kMaxInterpSectors) {
+                S.is[S.ninterp++] = nr;
+                S.is[S.ninterp++] = nl;
+            } else {
+                S.status |= S_JUNCTION_OVERFLOW;
+            }
+        }
+    }
+    // interpolating-sector end weights (pixel independent)
+    for (int s = 0; s < S.ninterp; ++s) {
+        InterpSector& q = S.is[s];
+        if (q.lb >= 0) {
+            q.left_w = S.cs[q.lb].weight;
+        } else {
+            const int sx = (int)P[q.left].x, sy = (int)P[q.left].y;
+            q.left_w = gb_weight_at(C, g, idl, ib, sy, sx, &S.status);
+        }
+        if (q.rb >= 0) {
+            q.right_w = S.cs[q.rb].weight;
+        } else {
+            const int sx = (int)P[q.right].x, sy = (int)P[q.right].y;
+            q.right_w = gb_weight_at(C, g, idl, ib, sy, sx, &S.status);
+        }
+        q.boundary_w = 0;
+        if (q.lb >= 0 && q.rb >= 0) {
+            const CPoint& smp = P[(q.right + 1) % real];
+            q.boundary_w = gb_weight_at(C, g, idl, ib, (int)smp.y, (int)smp.x, &S.status);
+        }
+    }
+}
+
+// ExplicitGrainBoundary::getWeight (src/grainBoundary.cpp:344-363) for one pixel.
+__device__ __forceinline__ double pixel_weight(const NetConst& C, int g, const CPoint* P, int size,
+                                               const SectorSet& S, const uint32_t* idl, const Box& ib, int i, int j,
+                                               uint32_t* status) {
+    double lambda = 0.0;
+    const int segment = project_to_boundary(P, size, (double)j, (double)i, &lambda);
+    const int real = size - 1;
+    for (int q = 0; q < S.nconst; q++)
+        if (within(S.cs[q].left, S.cs[q].right, real, segment)) return S.cs[q].weight;
+    for (int q = 0; q < S.ninterp; q++) {
+        const InterpSector& s = S.is[q];
+        if (!within(s.left, s.right, real, segment)) continue;
+        double interpolator = 0;
+        int k = s.right, it = 0;
+        for (; k != segment; k = (k + 1 + real) % real) {
+            interpolator += seg_len(P, k + 1, k) * C.h;
+            if (++it > size) break;
+        }
+        const int kn = (k + 1 + real) % real;
+        const double ax = (P[kn].x - P[k].x) * lambda, ay = (P[kn].y - P[k].y) * lambda;
+        interpolator += sqrt(ax * ax + ay * ay);
+        interpolator /= s.length;
+        if (interpolator < 0) interpolator = 0;
+        if (interpolator > 1) interpolator = 1;
+        if (s.lb >= 0 && s.rb >= 0) {
+            const double isr = C.isr;
+            const double quot = (s.length > 2 * isr ? 2 * isr : s.length);
+            const double amplitude =
+                (s.boundary_w - (s.left_w + s.right_w) / 2) / (2 * isr) * quot + (s.left_w + s.right_w) / 2;
+            const double a0 = 2 * s.right_w;
+            const double a1 = -4 * amplitude;
+            const double a2 = 2 * s.left_w;
+            const double A = a0 + a1 + a2;
+            const double B = -(a0 * 1.5 + a1 + a2 * 0.5);
+            const double Cc = a0 * 0.5;
+            return A * interpolator * interpolator + B * interpolator + Cc;
+        }
+        return interpolator * s.left_w + (1 - interpolator) * s.right_w;
+    }
+    return gb_weight_at(C, g, idl, ib, i, j, status);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_corrector(NetConst C, NetState* S) {
+    const int g = blockIdx.x + 1;
+    if (g > C.N || C.state[g] != G_EXISTS || C.regular[g] == 0 || S->loop == 0) return;
+    __shared__ SectorSet sec;
+    const CPoint* P = S->contPrev + S->coff_prev[g];
+    const int size = S->cn_prev[g];
+    const Box ib = S->box_prev[g];
+    const uint32_t* idl = S->idPrev + S->off_prev[g];
+    if (threadIdx.x == 0) {
+        build_sectors(C, g, P, size, S->jPrev + (int64_t)g * C.jmax, S->jn_prev[g], idl, ib, sec);
+        if (sec.status) set_status(S, sec.status);
+    }
+    __syncthreads();
+    if (size < 2) return;
+    const Box bo = S->box_cur[g];
+    const int x0 = ib.x0 < bo.x0 ? bo.x0 : ib.x0;
+    const int y0 = ib.y0 < bo.y0 ? bo.y0 : ib.y0;
+    const int x1 = ib.x1 > bo.x1 ? bo.x1 : ib.x1;
+    const int y1 = ib.y1 > bo.y1 ? bo.y1 : ib.y1;
+    if (x1 <= x0 || y1 <= y0) return;
+    const int w = x1 - x0;
+    const int64_t cnt = (int64_t)w * (y1 - y0);
+    const R* in = phiA_of<R>(S) + S->off_cur[g];
+    R* out = phiB_of<R>(S) + S->off_cur[g];
+    const int wo = box_w(bo);
+    const R delta = (R)C.delta;
+    uint32_t st = 0;
+    for (int64_t p = threadIdx.x; p < cnt; p += blockDim.x) {
+        const int i = y0 + (int)(p / w), j = x0 + (int)(p % w);
+        const int64_t k = (int64_t)(i - bo.y0) * wo + (j - bo.x0);
+        const R val = in[k];
+        if (val > -delta) {
+            const double weight = pixel_weight(C, g, P, size, sec, idl, ib, i, j, &st);
+            out[k] = (R)((double)val + ((double)out[k] - (double)val) * weight * 1.0);
+        } else {
+            out[k] = -delta;
+        }
+    }
+    if (st) set_status(S, st);
+}
+
+}  // namespace
+}  // namespace gg

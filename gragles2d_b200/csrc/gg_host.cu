@@ -1,0 +1,1026 @@
+// Host side of the C ABI (include/gg_step.h): settings, voxelized input,
+// host-computed tables, device arenas, the stage sequence of the reference
+// time loop and the state dump.  Host arithmetic that the FP64 form must
+// reproduce (dt, h, delta, Gaussian multipliers, twiddles) is written with
+// the reference's expressions and compiled without FMA contraction.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/gg_step.h"
+#include "gg_device.cuh"
+#include "gg_launch.cuh"
+
+using namespace gg;
+
+namespace {
+
+constexpr double kPiH = 3.14159265358979323846;  // PI, src/ggLS.h:26
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct gg_ctx {
+    gg_params P{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+
+    // derived settings (grainhdl::setSimulationParameter, src/grainhdl.cpp:56-136)
+    int N = 0, nn = 0, m = 0, b = 0, ppg = 0;
+    double h = 0, dt = 0, delta = 0, ds = 0;
+    bool loaded = false, initialised = false;
+
+    std::vector<int32_t> ids;     // nn*nn
+    std::vector<double> euler;    // 3 per grain
+    std::vector<int32_t> bbox;    // 5 per grain
+
+    NetConst C{};
+    NetState hS{};               // host copy of the device NetState (pointers)
+    NetState* dS = nullptr;
+    int32_t* d_ids = nullptr;
+    std::vector<void*> allocs;
+    LaunchCfg cfg{256, 256, 128, 64};
+
+    cudaGraphExec_t graph = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_ms = 0;
+
+    ~gg_ctx() {
+        if (graph) cudaGraphExecDestroy(graph);
+        for (void* p : allocs) cudaFree(p);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+int fail(gg_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_fail(gg_ctx* c, cudaError_t e, const char* where) {
+    return fail(c, GG_E_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define GG_CUDA(ctx, call)                                           \
+    do {                                                             \
+        cudaError_t e_ = (call);                                     \
+        if (e_ != cudaSuccess) return cuda_fail((ctx), e_, #call);   \
+    } while (0)
+
+template <typename T>
+int dalloc(gg_ctx* c, T** out, size_t count) {
+    void* p = nullptr;
+    const size_t bytes = sizeof(T) * (count > 0 ? count : 1);
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc");
+    e = cudaMemsetAsync(p, 0, bytes, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaMemset");
+    c->allocs.push_back(p);
+    *out = reinterpret_cast<T*>(p);
+    return GG_OK;
+}
+
+std::string trim(const std::string& s) {
+    size_t a = s.find_first_not_of(" \t\r\n");
+    if (a == std::string::npos) return "";
+    size_t b = s.find_last_not_of(" \t\r\n");
+    return s.substr(a, b - a + 1);
+}
+
+bool xml_tag(const std::string& doc, const char* tag, std::string* val) {
+    const std::string open = std::string("<") + tag + ">";
+    const std::string close = std::string("</") + tag + ">";
+    size_t a = doc.find(open);
+    if (a == std::string::npos) return false;
+    a += open.size();
+    size_t b = doc.find(close, a);
+    if (b == std::string::npos) return false;
+    *val = doc.substr(a, b - a);
+    return true;
+}
+
+// Euler (Bunge ZXZ) to quaternion: Quaternion::euler2quaternion (src/Quaternion.cpp:168-192)
+void euler2quaternion(const double* e, double* q) {
+    const double p1 = e[0], t = e[1], p2 = e[2];
+    const double co1 = cos(t / 2);
+    const double s1 = sin(t / 2);
+    q[0] = co1 * cos((p1 + p2) / 2);
+    q[1] = s1 * cos((p1 - p2) / 2);
+    q[2] = s1 * sin((p1 - p2) / 2);
+    q[3] = co1 * sin((p1 + p2) / 2);
+}
+
+// DimensionalBuffer::resizeToSquare (src/dimensionalBuffer.h:123-160)
+Box host_resize_to_square(Box r, int maximumLength) {
+    int grid_size = maximumLength - 1;
+    unsigned int height = r.y1 - r.y0;
+    unsigned int width = r.x1 - r.x0;
+    if (width == height) return r;
+    if (width > height) {
+        int diff = width - height;
+        r.y0 -= diff / 2;
+        r.y1 += diff / 2 + diff % 2;
+    } else {
+        int diff = height - width;
+        r.x0 -= diff / 2;
+        r.x1 += diff / 2 + diff % 2;
+    }
+    if (r.x0 < 0) {
+        int d = -r.x0;
+        r.x1 += d;
+        r.x0 += d;
+    } else if (r.x1 > grid_size) {
+        int d = grid_size - r.x1;
+        r.x1 += d;
+        r.x0 += d;
+    }
+    if (r.y0 < 0) {
+        int d = -r.y0;
+        r.y1 += d;
+        r.y0 += d;
+    } else if (r.y1 > grid_size) {
+        int d = grid_size - r.y1;
+        r.y1 += d;
+        r.y0 += d;
+    }
+    return r;
+}
+
+// Twiddle exp(-2 pi i k / n) from libm (same expression as the oracle's FFT).
+void twiddle(int n, int k, double* re, double* im) {
+    double ang = (2.0 * kPiH * (double)k) / (double)n;
+    *re = cos(ang);
+    *im = -sin(ang);
+}
+
+// Gaussian multiplier of LSbox::convolutionGeneratorFFTW (src/box.cpp:674-687).
+double gaussian_multiplier(int n, int i2, int j2, double dt, int nn) {
+    double nsq = nn * nn;
+    double n_nsq = n * n;
+    return exp(-sqrt(2 / kPiH) * (i2 * i2 + j2 * j2) * 4.0 * dt * nsq / n_nsq * kPiH * kPiH) / n_nsq;
+}
+
+int check_status(gg_ctx* c) {
+    uint32_t st = 0;
+    GG_CUDA(c, cudaMemcpyAsync(&st, &c->dS->status, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
+    GG_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (st & (S_ARENA_FULL | S_LIST_OVERFLOW | S_CONTOUR_OVERFLOW | S_JUNCTION_OVERFLOW | S_TABLE_RANGE |
+              S_NEIGHBOUR_OVERFLOW)) {
+        char buf[128];
+        std::snprintf(buf, sizeof buf, "device capacity exceeded (status 0x%x)", st);
+        return fail(c, GG_E_CAPACITY, buf);
+    }
+    if (st & (S_WALK_LIMIT | S_NAN)) {
+        char buf[128];
+        std::snprintf(buf, sizeof buf, "device numeric guard tripped (status 0x%x)", st);
+        return fail(c, GG_E_NUMERIC, buf);
+    }
+    return GG_OK;
+}
+
+int refresh_state(gg_ctx* c) {
+    GG_CUDA(c, cudaMemcpyAsync(&c->hS, c->dS, sizeof(NetState), cudaMemcpyDeviceToHost, c->stream));
+    GG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GG_OK;
+}
+
+int set_loop(gg_ctx* c, int loop) {
+    GG_CUDA(c, cudaMemcpyAsync(&c->dS->loop, &loop, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    return GG_OK;
+}
+
+int launch_stages(gg_ctx* c, int stages) {
+    cudaError_t e = c->P.precision == GG_PRECISION_PLAIN ? plain_stages(c->C, c->dS, stages, c->stream, c->cfg)
+                                                         : batched_stages(c->C, c->dS, stages, c->stream, c->cfg);
+    if (e != cudaSuccess) return cuda_fail(c, e, "stage launch");
+    return GG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gg_params_default(gg_params* p) {
+    if (!p) return GG_E_INVALID;
+    std::memset(p, 0, sizeof(*p));
+    p->struct_size = (int32_t)sizeof(gg_params);
+    p->precision = GG_PRECISION_PLAIN;
+    p->analysis_timestep = 1;
+    p->domain_border_size = 7;
+    p->microstructure_gen_mode = 4;
+    p->convolution_mode = 2;
+    p->hagb_energy = 1.0;
+    p->hagb_mobility = 1.0;
+    p->time_slope = 0.8359;
+    p->theta_ref_deg = 15.0;
+    p->gamma_hagb = 1.0;
+    p->m_hagb = 1.0;
+    return GG_OK;
+}
+
+int gg_params_from_xml(const char* path, gg_params* p) {
+    if (!path || !p) return GG_E_INVALID;
+    std::ifstream f(path);
+    if (!f) return GG_E_IO;
+    std::stringstream ss;
+    ss << f.rdbuf();
+    const std::string doc = ss.str();
+    if (doc.find("<Parameters>") == std::string::npos) return GG_E_IO;
+    std::string v;
+    auto geti = [&](const char* tag, int32_t* dst) {
+        if (xml_tag(doc, tag, &v)) *dst = (int32_t)std::stol(trim(v));
+    };
+    auto getd = [&](const char* tag, double* dst) {
+        if (xml_tag(doc, tag, &v)) *dst = std::stod(trim(v));
+    };
+    auto gets = [&](const char* tag, char* dst, size_t cap) {
+        if (xml_tag(doc, tag, &v)) {
+            std::string t = trim(v);
+            std::strncpy(dst, t.c_str(), cap - 1);
+            dst[cap - 1] = 0;
+        }
+    };
+    try {
+        geti("StartTime", &p->start_time);
+        geti("NumberOfParticles", &p->number_of_particles);
+        geti("NumberOfPointsPerGrain", &p->number_of_points_per_grain);
+        geti("AnalysisTimestep", &p->analysis_timestep);
+        geti("NumberOfTimesteps", &p->number_of_timesteps);
+        geti("BreakupNumber", &p->breakup_number);
+        geti("DomainBorderSize", &p->domain_border_size);
+        geti("MicrostructureGenMode", &p->microstructure_gen_mode);
+        gets("ReadFromFilename", p->read_from_filename, sizeof p->read_from_filename);
+        gets("AdditionalFilename", p->additional_filename, sizeof p->additional_filename);
+        geti("LatticeType", &p->lattice_type);
+        getd("HAGB_Energy", &p->hagb_energy);
+        getd("HAGB_Mobility", &p->hagb_mobility);
+        getd("Physical_Domain_Size", &p->physical_domain_size);
+        getd("TriplePointDrag", &p->triple_point_drag);
+        geti("UseMobilityModel", &p->use_mobility_model);
+        geti("IdentifyTwins", &p->identify_twins);
+        geti("UseMagneticField", &p->use_magnetic_field);
+        geti("IsIsotropicNetwork", &p->is_isotropic_network);
+        geti("GridCoarsement", &p->grid_coarsement);
+        geti("ConvolutionMode", &p->convolution_mode);
+        geti("ResearchMode", &p->research_mode);
+        geti("ResearchProject", &p->research_project);
+        getd("ConstantSectorRadius", &p->constant_sector_radius);
+        getd("InterpolatingSectorRadius", &p->interpolating_sector_radius);
+        geti("UseStoredElasticEnergy", &p->use_stored_elastic_energy);
+        geti("DecoupleGrains", &p->decouple_grains);
+        getd("GaussianKernelUserDefTimeSlope", &p->time_slope);
+        getd("ThetaRefDegrees", &p->theta_ref_deg);
+        getd("HAGB_RelativeEnergy", &p->gamma_hagb);
+        getd("HAGB_RelativeMobility", &p->m_hagb);
+        geti("Precision", &p->precision);
+    } catch (...) {
+        return GG_E_IO;
+    }
+    return GG_OK;
+}
+
+int gg_create(const gg_params* p, int device, gg_ctx** out) {
+    if (!p || !out) return GG_E_INVALID;
+    *out = nullptr;
+    if (p->struct_size != (int32_t)sizeof(gg_params)) return GG_E_INVALID;
+    gg_ctx* c = new gg_ctx();
+    c->P = *p;
+    c->device = device;
+    auto bad = [&](const char* msg) {
+        c->err = msg;
+        *out = c;
+        return GG_E_INVALID;
+    };
+    if (p->convolution_mode != 2) return bad("only ConvolutionMode 2 (Gaussian) is supported");
+    if (p->lattice_type != 0) return bad("only LatticeType 0 (cubic) is supported");
+    if (p->research_mode != 0) return bad("only ResearchMode 0 is supported");
+    if (p->grid_coarsement != 0) return bad("GridCoarsement must be 0");
+    if (p->use_stored_elastic_energy != 0 || p->use_magnetic_field != 0)
+        return bad("stored-energy and magnetic driving forces are not supported");
+    if (p->identify_twins != 0) return bad("IdentifyTwins is not supported");
+    if (p->use_mobility_model < 0 || p->use_mobility_model > 1) return bad("UseMobilityModel must be 0 or 1");
+    if (p->precision != GG_PRECISION_PLAIN && p->precision != GG_PRECISION_BATCHED) return bad("bad precision");
+    if (p->domain_border_size < 1) return bad("DomainBorderSize must be >= 1");
+    if (p->analysis_timestep <= 0) return bad("AnalysisTimestep must be > 0");
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        c->err = std::string("cudaSetDevice: ") + cudaGetErrorString(e);
+        *out = c;
+        return GG_E_CUDA;
+    }
+    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
+    if (e != cudaSuccess) {
+        c->err = std::string("stream/event: ") + cudaGetErrorString(e);
+        *out = c;
+        return GG_E_CUDA;
+    }
+    *out = c;
+    return GG_OK;
+}
+
+void gg_destroy(gg_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    delete ctx;
+}
+
+const char* gg_last_error(const gg_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int gg_load_voxels(gg_ctx* c, int32_t nn, const int32_t* ids, int32_t n_grains, const double* euler,
+                   const int32_t* bbox) {
+    if (!c || !ids || !euler || !bbox || nn <= 0 || n_grains <= 0) return fail(c, GG_E_INVALID, "bad voxel input");
+    if (c->initialised) return fail(c, GG_E_STATE, "network already initialised");
+    c->nn = nn;
+    c->N = n_grains;
+    c->ids.assign(ids, ids + (size_t)nn * nn);
+    c->euler.assign(euler, euler + 3 * (size_t)n_grains);
+    c->bbox.assign(bbox, bbox + 5 * (size_t)n_grains);
+    c->loaded = true;
+    return GG_OK;
+}
+
+int gg_load_voxel_files(gg_ctx* c, const char* base_dir) {
+    if (!c) return GG_E_INVALID;
+    auto join = [&](const char* name) {
+        std::string s(name);
+        if (!s.empty() && s[0] != '/' && base_dir && base_dir[0]) s = std::string(base_dir) + "/" + s;
+        return s;
+    };
+    // read_voxelized_microstructure (src/grainhdl.cpp:336-511): 8 header lines
+    FILE* f = std::fopen(join(c->P.additional_filename).c_str(), "r");
+    if (!f) return fail(c, GG_E_IO, std::string("cannot open ") + join(c->P.additional_filename));
+    char line[4096];
+    int id_offset = 1, NX = 0, NY = 0, grains = 0;
+    for (int i = 1; i <= 8; ++i) {
+        if (!std::fgets(line, sizeof line, f)) {
+            std::fclose(f);
+            return fail(c, GG_E_IO, "truncated .uds header");
+        }
+        char name[256];
+        int val = 0;
+        if (i >= 2 && i <= 7 && std::sscanf(line, "%255s %d", name, &val) == 2) {
+            if (i == 2) id_offset = val;
+            if (i == 5) NX = val;
+            if (i == 6) NY = val;
+            if (i == 7) grains = val;
+        }
+    }
+    if (NX <= 0 || NX != NY || grains <= 0) {
+        std::fclose(f);
+        return fail(c, GG_E_IO, "bad .uds header (need NX == NY > 0 and a grain count)");
+    }
+    std::vector<double> eul(3 * (size_t)grains);
+    std::vector<int32_t> bb(5 * (size_t)grains);
+    for (int k = 0; k < grains; ++k) {
+        int id, xmin, xmax, ymin, ymax, cnt;
+        double x, y, e0, e1, e2, se;
+        if (std::fscanf(f, "%d %lf %lf %lf %lf %lf %d %d %d %d %d %lf", &id, &x, &y, &e0, &e1, &e2, &xmin, &xmax,
+                        &ymin, &ymax, &cnt, &se) != 12) {
+            std::fclose(f);
+            return fail(c, GG_E_IO, "truncated .uds grain table");
+        }
+        if (id - (id_offset - 1) != k + 1) {
+            std::fclose(f);
+            return fail(c, GG_E_IO, "grain IDs in the .uds must be consecutive from the ID offset");
+        }
+        eul[3 * k] = e0;
+        eul[3 * k + 1] = e1;
+        eul[3 * k + 2] = e2;
+        bb[5 * k] = xmin;
+        bb[5 * k + 1] = xmax;
+        bb[5 * k + 2] = ymin;
+        bb[5 * k + 3] = ymax;
+        bb[5 * k + 4] = cnt;
+    }
+    std::fclose(f);
+    FILE* fb = std::fopen(join(c->P.read_from_filename).c_str(), "rb");
+    if (!fb) return fail(c, GG_E_IO, std::string("cannot open ") + join(c->P.read_from_filename));
+    std::vector<int32_t> ids((size_t)NX * NX);
+    const size_t got = std::fread(ids.data(), sizeof(int32_t), ids.size(), fb);
+    std::fclose(fb);
+    if (got != ids.size()) return fail(c, GG_E_IO, "truncated .bin ID field");
+    for (auto& v : ids) {
+        v = v - (id_offset - 1);
+        if (v < 0) v = 0;
+    }
+    return gg_load_voxels(c, NX, ids.data(), grains, eul.data(), bb.data());
+}
+
+int gg_distance_initialisation(gg_ctx* c) {
+    if (!c) return GG_E_INVALID;
+    if (!c->loaded) return fail(c, GG_E_STATE, "no microstructure loaded");
+    if (c->initialised) return fail(c, GG_E_STATE, "already initialised");
+    GG_CUDA(c, cudaSetDevice(c->device));
+    const gg_params& P = c->P;
+    // grainhdl::read_HeaderCPG / setSimulationParameter (src/grainhdl.cpp:56-136, 275-334)
+    c->ppg = (int)(c->nn / sqrt(c->N));
+    const int realDomainSize = c->nn;
+    const double csr_raw = P.constant_sector_radius, isr_raw = P.interpolating_sector_radius;
+    c->ds = (csr_raw * 2 + isr_raw * 2) / double(realDomainSize);
+    const unsigned long ppg_used =
+        P.decouple_grains == 1 ? (unsigned long)P.number_of_points_per_grain : (unsigned long)c->ppg;
+    c->dt = 0.8 / double(realDomainSize * realDomainSize) * ppg_used / 2 / 5.0;
+    c->h = 1.0 / double(realDomainSize);
+    c->delta = (unsigned long)P.domain_border_size * 1 / double(realDomainSize);
+    c->b = P.domain_border_size;
+    c->m = realDomainSize + 2 * c->b;
+    const int N = c->N, m = c->m, b = c->b;
+
+    // boxes of the voxel constructor (src/box.cpp:156-217)
+    std::vector<Box> box0(N + 1, Box{0, 0, 0, 0});
+    std::vector<int32_t> state(N + 1, G_GONE);
+    int maxn = 1;
+    for (int g = 1; g <= N; ++g) {
+        const int32_t* q = &c->bbox[5 * (size_t)(g - 1)];
+        if (q[4] == 0) continue;  // zero-pixel grains are skipped
+        int xmin = m, xmax = 0, ymin = m, ymax = 0;
+        const int vx[4] = {q[0], q[0], q[1], q[1]}, vy[4] = {q[2], q[3], q[2], q[3]};
+        for (int k = 0; k < 4; ++k) {
+            if (vy[k] < ymin) ymin = vy[k];
+            if (vy[k] > ymax) ymax = vy[k];
+            if (vx[k] < xmin) xmin = vx[k];
+            if (vx[k] > xmax) xmax = vx[k];
+        }
+        xmax += 2 * b;
+        ymax += 2 * b;
+        if (ymax > m) ymax = m;
+        if (xmax > m) xmax = m;
+        if (ymin < 0) ymin = 0;
+        if (xmin < 0) xmin = 0;
+        box0[g] = host_resize_to_square(Box{xmin, xmax, ymin, ymax}, m);
+        state[g] = G_EXISTS;
+        maxn = std::max(maxn, box_w(box0[g]));
+    }
+    const int tmax = std::min(m, std::max(160, 2 * maxn + 32));
+
+    // offsets of the initial layout
+    std::vector<int64_t> off(N + 1, 0), soff(N + 1, 0), coff(N + 1, 0);
+    std::vector<int32_t> ccap(N + 1, 0);
+    const int spc = P.precision == GG_PRECISION_PLAIN ? 2 : 1;
+    int64_t a = 0, sp = 0, cc = 0;
+    for (int g = 0; g <= N; ++g) {
+        off[g] = a;
+        soff[g] = sp;
+        coff[g] = cc;
+        if (g >= 1 && state[g] == G_EXISTS) {
+            const int n = box_w(box0[g]);
+            a += box_area(box0[g]);
+            sp += (int64_t)spc * 2 * (int64_t)n * (n / 2 + 1);
+            ccap[g] = contour_capacity(n);
+            cc += ccap[g];
+        }
+    }
+    const int64_t phi_cap = std::max<int64_t>(2 * a, a + (1 << 20));
+    const int64_t spec_cap = std::max<int64_t>(2 * sp, sp + (1 << 20));
+    const int64_t cont_cap = std::max<int64_t>(2 * cc, cc + (1 << 16));
+    const size_t rsz = P.precision == GG_PRECISION_PLAIN ? sizeof(double) : sizeof(float);
+
+    // constant settings
+    NetConst& C = c->C;
+    C.N = N;
+    C.m = m;
+    C.b = b;
+    C.nn = c->nn;
+    C.kmax = 96;
+    C.nbmax = 48;
+    C.jmax = 48;
+    C.tmax = tmax;
+    C.isotropic = P.is_isotropic_network ? 1 : 0;
+    C.use_mobility_model = P.use_mobility_model;
+    C.analysis_timestep = P.analysis_timestep;
+    C.decouple = P.decouple_grains == 1 ? 1 : 0;
+    C.h = c->h;
+    C.delta = c->delta;
+    C.dt = c->dt;
+    C.csr = csr_raw * c->h;
+    C.isr = isr_raw * c->h;
+    C.ds = c->ds;
+    C.tpd = P.triple_point_drag;
+    C.theta_ref = P.theta_ref_deg * kPiH / 180.0;
+    C.gamma_hagb = P.gamma_hagb;
+    C.m_hagb = P.m_hagb;
+
+    int rc;
+#define ALLOC(ptr, cnt) \
+    if ((rc = dalloc(c, &(ptr), (cnt))) != GG_OK) return rc
+    ALLOC(C.state, N + 1);
+    ALLOC(C.regular, N + 1);
+    ALLOC(C.inter_bnd, N + 1);
+    ALLOC(C.newbb, 4 * (size_t)(N + 1));
+    ALLOC(C.volume, N + 1);
+    ALLOC(C.energy, N + 1);
+    ALLOC(C.perimeter, N + 1);
+    ALLOC(C.meanda, N + 1);
+    ALLOC(C.quat, 4 * (size_t)(N + 1));
+    ALLOC(C.cmp_n, N + 1);
+    ALLOC(C.cmp_ids, (size_t)C.kmax * (N + 1));
+    ALLOC(C.sec_n, N + 1);
+    ALLOC(C.sec_ids, (size_t)C.kmax * (N + 1));
+    ALLOC(C.nb_n, N + 1);
+    ALLOC(C.nb, (size_t)C.nbmax * (N + 1));
+
+    // tables: twiddles and Gaussian multipliers (plain), separable kernels (batched)
+    std::vector<int64_t> tw_off(tmax + 1, 0), gk_off(tmax + 1, 0), ck_off(tmax + 1, 0);
+    int64_t twn = 0, gkn = 0, ckn = 0;
+    for (int n = 1; n <= tmax; ++n) {
+        tw_off[n] = twn;
+        twn += n;
+        gk_off[n] = gkn;
+        gkn += (int64_t)(n / 2 + 1) * (n / 2 + 1);
+        ck_off[n] = ckn;
+        ckn += n;
+    }
+    const bool plain = P.precision == GG_PRECISION_PLAIN;
+    std::vector<double> tw(plain ? 2 * twn : 2), gk(plain ? gkn : 1);
+    std::vector<float> ck(plain ? 1 : ckn);
+    if (plain) {
+        for (int n = 1; n <= tmax; ++n) {
+            for (int k = 0; k < n; ++k) twiddle(n, k, &tw[2 * (tw_off[n] + k)], &tw[2 * (tw_off[n] + k) + 1]);
+            const int half = n / 2 + 1;
+            for (int i2 = 0; i2 < half; ++i2)
+                for (int j2 = 0; j2 < half; ++j2)
+                    gk[gk_off[n] + i2 * half + j2] = gaussian_multiplier(n, i2, j2, c->dt, c->nn);
+        }
+    } else {
+        // k_n[r] = (1/n) sum_f g(min(f, n-f)) cos(2 pi f r / n), g(f) = exp(-kappa f^2),
+        // kappa = sqrt(2/pi) 4 dt nn^2 / n^2 pi^2 (the 1/n^2 of G split over both axes)
+        std::vector<double> gf;
+        for (int n = 1; n <= tmax; ++n) {
+            const double kappa = sqrt(2 / kPiH) * 4.0 * c->dt * (double)c->nn * (double)c->nn / ((double)n * n) *
+                                 kPiH * kPiH;
+            gf.assign(n, 0.0);
+            for (int f = 0; f < n; ++f) {
+                const int f2 = std::min(f, n - f);
+                gf[f] = exp(-kappa * (double)f2 * f2);
+            }
+            for (int r = 0; r < n; ++r) {
+                double acc = 0;
+                for (int f = 0; f < n; ++f) acc += gf[f] * cos(2.0 * kPiH * (double)((int64_t)f * r % n) / n);
+                ck[ck_off[n] + r] = (float)(acc / n);
+            }
+        }
+    }
+    double* d_tw;
+    double* d_gk;
+    float* d_ck;
+    int64_t *d_twoff, *d_gkoff, *d_ckoff;
+    ALLOC(d_tw, tw.size());
+    ALLOC(d_gk, gk.size());
+    ALLOC(d_ck, ck.size());
+    ALLOC(d_twoff, tmax + 1);
+    ALLOC(d_gkoff, tmax + 1);
+    ALLOC(d_ckoff, tmax + 1);
+    GG_CUDA(c, cudaMemcpyAsync(d_tw, tw.data(), sizeof(double) * tw.size(), cudaMemcpyHostToDevice, c->stream));
+    GG_CUDA(c, cudaMemcpyAsync(d_gk, gk.data(), sizeof(double) * gk.size(), cudaMemcpyHostToDevice, c->stream));
+    GG_CUDA(c, cudaMemcpyAsync(d_ck, ck.data(), sizeof(float) * ck.size(), cudaMemcpyHostToDevice, c->stream));
+    GG_CUDA(c, cudaMemcpyAsync(d_twoff, tw_off.data(), sizeof(int64_t) * (tmax + 1), cudaMemcpyHostToDevice,
+                               c->stream));
+    GG_CUDA(c, cudaMemcpyAsync(d_gkoff, gk_off.data(), sizeof(int64_t) * (tmax + 1), cudaMemcpyHostToDevice,
+                               c->stream));
+    GG_CUDA(c, cudaMemcpyAsync(d_ckoff, ck_off.data(), sizeof(int64_t) * (tmax + 1), cudaMemcpyHostToDevice,
+                               c->stream));
+    C.tw = d_tw;
+    C.gk = d_gk;
+    C.ck = d_ck;
+    C.tw_off = d_twoff;
+    C.gk_off = d_gkoff;
+    C.ck_off = d_ckoff;
+
+    // rotating state
+    NetState& S = c->hS;
+    std::memset(&S, 0, sizeof S);
+    Box* boxes[3];
+    int64_t* offs[3];
+    int64_t* soffs[2];
+    int64_t* coffs[3];
+    int32_t* ccaps[3];
+    for (int k = 0; k < 3; ++k) {
+        ALLOC(boxes[k], N + 1);
+        ALLOC(offs[k], N + 1);
+        ALLOC(coffs[k], N + 1);
+        ALLOC(ccaps[k], N + 1);
+    }
+    for (int k = 0; k < 2; ++k) ALLOC(soffs[k], N + 1);
+    S.box_prev = boxes[0];
+    S.box_cur = boxes[1];
+    S.box_new = boxes[2];
+    S.off_prev = offs[0];
+    S.off_cur = offs[1];
+    S.off_new = offs[2];
+    S.soff_cur = soffs[0];
+    S.soff_new = soffs[1];
+    S.coff_prev = coffs[0];
+    S.coff_cur = coffs[1];
+    S.coff_new = coffs[2];
+    S.ccap_prev = ccaps[0];
+    S.ccap_cur = ccaps[1];
+    S.ccap_new = ccaps[2];
+    if (plain) {
+        double *pa, *pb, *sp_;
+        ALLOC(pa, phi_cap);
+        ALLOC(pb, phi_cap);
+        ALLOC(sp_, spec_cap);
+        S.phiA = pa;
+        S.phiB = pb;
+        S.spec = sp_;
+    } else {
+        float *pa, *pb, *sp_;
+        ALLOC(pa, phi_cap);
+        ALLOC(pb, phi_cap);
+        ALLOC(sp_, spec_cap);
+        S.phiA = pa;
+        S.phiB = pb;
+        S.spec = sp_;
+    }
+    (void)rsz;
+    ALLOC(S.idPrev, phi_cap);
+    ALLOC(S.idCur, phi_cap);
+    ALLOC(S.contPrev, cont_cap);
+    ALLOC(S.contCur, cont_cap);
+    ALLOC(S.cn_prev, N + 1);
+    ALLOC(S.cn_cur, N + 1);
+    ALLOC(S.jPrev, (size_t)C.jmax * (N + 1));
+    ALLOC(S.jCur, (size_t)C.jmax * (N + 1));
+    ALLOC(S.jn_prev, N + 1);
+    ALLOC(S.jn_cur, N + 1);
+    S.phi_cap = phi_cap;
+    S.spec_cap = spec_cap;
+    S.cont_cap = cont_cap;
+    S.loop = P.start_time;
+    ALLOC(c->dS, 1);
+    ALLOC(c->d_ids, (size_t)c->nn * c->nn);
+#undef ALLOC
+
+    // initial per-grain data
+    std::vector<double> quat(4 * (size_t)(N + 1), 0.0);
+    quat[0] = 1.0;  // boundary grain: Euler (0,0,0) (src/grainhdl.cpp:137)
+    for (int g = 1; g <= N; ++g) euler2quaternion(&c->euler[3 * (size_t)(g - 1)], &quat[4 * (size_t)g]);
+    std::vector<int32_t> ones(N + 1, 1);
+    auto h2d = [&](void* dst, const void* src, size_t bytes) {
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream);
+    };
+    for (int k = 0; k < 3; ++k) {
+        GG_CUDA(c, h2d(boxes[k], box0.data(), sizeof(Box) * (N + 1)));
+        GG_CUDA(c, h2d(offs[k], off.data(), sizeof(int64_t) * (N + 1)));
+        GG_CUDA(c, h2d(coffs[k], coff.data(), sizeof(int64_t) * (N + 1)));
+        GG_CUDA(c, h2d(ccaps[k], ccap.data(), sizeof(int32_t) * (N + 1)));
+    }
+    GG_CUDA(c, h2d(soffs[0], soff.data(), sizeof(int64_t) * (N + 1)));
+    GG_CUDA(c, h2d(C.state, state.data(), sizeof(int32_t) * (N + 1)));
+    GG_CUDA(c, h2d(C.regular, ones.data(), sizeof(int32_t) * (N + 1)));
+    GG_CUDA(c, h2d(C.quat, quat.data(), sizeof(double) * quat.size()));
+    GG_CUDA(c, h2d(c->d_ids, c->ids.data(), sizeof(int32_t) * c->ids.size()));
+    S.phi_used = a;
+    S.spec_used = sp;
+    S.cont_used = cc;
+    GG_CUDA(c, h2d(c->dS, &S, sizeof(NetState)));
+
+    if (!plain) GG_CUDA(c, batched_prepare(tmax));
+    GG_CUDA(c, plain ? plain_init(C, c->dS, c->d_ids, c->stream) : batched_init(C, c->dS, c->d_ids, c->stream));
+    GG_CUDA(c, finalize_only(C, c->dS, 0, c->stream));
+    rc = check_status(c);
+    if (rc != GG_OK) return rc;
+    c->initialised = true;
+    return refresh_state(c);
+}
+
+int gg_find_neighbors(gg_ctx* c) {
+    if (!c) return GG_E_INVALID;
+    if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
+    GG_CUDA(c, find_neighbors_launch(c->C, c->dS, c->stream));
+    return check_status(c);
+}
+
+int gg_set_neighbours(gg_ctx* c, const int32_t* offsets, const int32_t* ids) {
+    if (!c || !offsets || !ids) return GG_E_INVALID;
+    if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
+    const int N = c->N, K = c->C.kmax;
+    std::vector<int32_t> sec((size_t)K * (N + 1), 0), n(N + 1, 0), zero(N + 1, 0);
+    std::vector<Neighbour> nb((size_t)c->C.nbmax * (N + 1));
+    std::vector<int32_t> nbn(N + 1, 0);
+    for (int g = 1; g <= N; ++g) {
+        const int a = offsets[g - 1], e = offsets[g];
+        if (e - a > K) return fail(c, GG_E_CAPACITY, "neighbour list longer than the list capacity");
+        for (int k = a; k < e; ++k) {
+            if (ids[k] < 1 || ids[k] > N) return fail(c, GG_E_INVALID, "neighbour ID out of range");
+            sec[(size_t)g * K + (k - a)] = ids[k];
+            if (k - a < c->C.nbmax) {
+                Neighbour& q = nb[(size_t)g * c->C.nbmax + (k - a)];
+                q.id = ids[k];
+                q.length = q.energy = q.misori = q.mobility = 0;
+                nbn[g]++;
+            }
+        }
+        n[g] = e - a;
+    }
+    GG_CUDA(c, cudaMemcpyAsync(c->C.sec_ids, sec.data(), sizeof(int32_t) * sec.size(), cudaMemcpyHostToDevice,
+                               c->stream));
+    GG_CUDA(c, cudaMemcpyAsync(c->C.sec_n, n.data(), sizeof(int32_t) * n.size(), cudaMemcpyHostToDevice, c->stream));
+    GG_CUDA(c, cudaMemcpyAsync(c->C.cmp_n, zero.data(), sizeof(int32_t) * zero.size(), cudaMemcpyHostToDevice,
+                               c->stream));
+    GG_CUDA(c, cudaMemcpyAsync(c->C.nb, nb.data(), sizeof(Neighbour) * nb.size(), cudaMemcpyHostToDevice,
+                               c->stream));
+    GG_CUDA(c, cudaMemcpyAsync(c->C.nb_n, nbn.data(), sizeof(int32_t) * nbn.size(), cudaMemcpyHostToDevice,
+                               c->stream));
+    GG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GG_OK;
+}
+
+namespace {
+int run_stage(gg_ctx* c, int stages, bool setloop, int loop) {
+    if (!c) return GG_E_INVALID;
+    if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
+    if (setloop) {
+        int r = set_loop(c, loop);
+        if (r) return r;
+    }
+    int r = launch_stages(c, stages);
+    if (r) return r;
+    return check_status(c);
+}
+}  // namespace
+
+int gg_convolution(gg_ctx* c, int32_t loop) { return run_stage(c, ST_CONV, true, loop); }
+int gg_update_second_order_neighbors(gg_ctx* c) { return run_stage(c, ST_SECOND, false, 0); }
+int gg_comparison(gg_ctx* c) { return run_stage(c, ST_COMPARE, false, 0); }
+int gg_level_set(gg_ctx* c, int32_t loop) { return run_stage(c, ST_LEVELSET, true, loop); }
+int gg_redistancing(gg_ctx* c, int32_t loop) { return run_stage(c, ST_REDIST, true, loop); }
+
+int gg_grain_count(gg_ctx* c, int32_t* current, double* max_volume) {
+    if (!c) return GG_E_INVALID;
+    if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
+    int rc = refresh_state(c);
+    if (rc) return rc;
+    if (current) *current = c->hS.live;
+    if (max_volume) *max_volume = c->hS.max_volume;
+    return GG_OK;
+}
+
+int gg_step(gg_ctx* c, int32_t loop, int32_t nsteps) {
+    if (!c) return GG_E_INVALID;
+    if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
+    if (nsteps <= 0) return GG_OK;
+    int rc = set_loop(c, loop);
+    if (rc) return rc;
+    if (c->P.precision == GG_PRECISION_BATCHED) {
+        if (!c->graph) {
+            cudaGraph_t gr;
+            GG_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            cudaError_t e = batched_stages(c->C, c->dS, ST_ALL, c->stream, c->cfg);
+            cudaError_t e2 = cudaStreamEndCapture(c->stream, &gr);
+            if (e != cudaSuccess) return cuda_fail(c, e, "capture");
+            if (e2 != cudaSuccess) return cuda_fail(c, e2, "end capture");
+            e = cudaGraphInstantiate(&c->graph, gr, 0);
+            cudaGraphDestroy(gr);
+            if (e != cudaSuccess) return cuda_fail(c, e, "graph instantiate");
+        }
+        GG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+        for (int s = 0; s < nsteps; ++s) GG_CUDA(c, cudaGraphLaunch(c->graph, c->stream));
+        GG_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    } else {
+        GG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+        for (int s = 0; s < nsteps; ++s) {
+            rc = launch_stages(c, ST_ALL);
+            if (rc) return rc;
+        }
+        GG_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    }
+    GG_CUDA(c, cudaEventSynchronize(c->ev1));
+    float ms = 0;
+    GG_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    c->last_ms = ms;
+    return check_status(c);
+}
+
+int gg_status(gg_ctx* c, uint32_t* status, int32_t clear) {
+    if (!c || !status) return GG_E_INVALID;
+    if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
+    GG_CUDA(c, cudaMemcpyAsync(status, &c->dS->status, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    GG_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (clear) GG_CUDA(c, cudaMemsetAsync(&c->dS->status, 0, sizeof(uint32_t), c->stream));
+    return GG_OK;
+}
+
+int gg_last_step_ms(gg_ctx* c, double* ms) {
+    if (!c || !ms) return GG_E_INVALID;
+    *ms = c->last_ms;
+    return GG_OK;
+}
+
+int gg_dims(gg_ctx* c, int32_t* n_grains, int32_t* ngridpoints, double* h, double* delta, double* dt) {
+    if (!c) return GG_E_INVALID;
+    if (n_grains) *n_grains = c->N;
+    if (ngridpoints) *ngridpoints = c->m;
+    if (h) *h = c->h;
+    if (delta) *delta = c->delta;
+    if (dt) *dt = c->dt;
+    return GG_OK;
+}
+
+int gg_read_grain_stats(gg_ctx* c, gg_grain_stats* out, int32_t capacity) {
+    if (!c || !out) return GG_E_INVALID;
+    if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
+    if (capacity < c->N) return fail(c, GG_E_INVALID, "capacity smaller than the grain count");
+    int rc = refresh_state(c);
+    if (rc) return rc;
+    const int N = c->N;
+    std::vector<int32_t> state(N + 1), reg(N + 1), bnd(N + 1), nbn(N + 1), cn(N + 1);
+    std::vector<double> vol(N + 1), en(N + 1), per(N + 1), mda(N + 1);
+    std::vector<Box> box(N + 1);
+    auto d2h = [&](void* dst, const void* src, size_t bytes) {
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream);
+    };
+    GG_CUDA(c, d2h(state.data(), c->C.state, 4 * (N + 1)));
+    GG_CUDA(c, d2h(reg.data(), c->C.regular, 4 * (N + 1)));
+    GG_CUDA(c, d2h(bnd.data(), c->C.inter_bnd, 4 * (N + 1)));
+    GG_CUDA(c, d2h(nbn.data(), c->C.nb_n, 4 * (N + 1)));
+    GG_CUDA(c, d2h(cn.data(), c->hS.cn_prev, 4 * (N + 1)));
+    GG_CUDA(c, d2h(vol.data(), c->C.volume, 8 * (N + 1)));
+    GG_CUDA(c, d2h(en.data(), c->C.energy, 8 * (N + 1)));
+    GG_CUDA(c, d2h(per.data(), c->C.perimeter, 8 * (N + 1)));
+    GG_CUDA(c, d2h(mda.data(), c->C.meanda, 8 * (N + 1)));
+    GG_CUDA(c, d2h(box.data(), c->hS.box_cur, sizeof(Box) * (N + 1)));
+    GG_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int g = 1; g <= N; ++g) {
+        gg_grain_stats& s = out[g - 1];
+        s.id = g;
+        s.state = state[g];
+        s.motion_regular = reg[g];
+        s.intersects_boundary = bnd[g];
+        s.n_neighbours = nbn[g];
+        s.contour_points = cn[g];
+        s.box[0] = box[g].x0;
+        s.box[1] = box[g].x1;
+        s.box[2] = box[g].y0;
+        s.box[3] = box[g].y1;
+        s.area = vol[g];
+        s.energy = en[g];
+        s.perimeter = per[g];
+        s.mean_da = mda[g];
+    }
+    return GG_OK;
+}
+
+int gg_dump(gg_ctx* c, const char* path, int32_t steps_done, int32_t append) {
+    if (!c || !path) return GG_E_INVALID;
+    if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
+    int rc = refresh_state(c);
+    if (rc) return rc;
+    const int N = c->N;
+    const NetState& S = c->hS;
+    const NetConst& C = c->C;
+    const bool plain = c->P.precision == GG_PRECISION_PLAIN;
+    const size_t rsz = plain ? 8 : 4;
+    std::vector<int32_t> state(N + 1), reg(N + 1), bnd(N + 1), cmpn(N + 1), secn(N + 1), nbn(N + 1), cn(N + 1),
+        jn(N + 1), newbb(4 * (N + 1));
+    std::vector<int32_t> cmp((size_t)C.kmax * (N + 1)), sec((size_t)C.kmax * (N + 1));
+    std::vector<double> vol(N + 1), en(N + 1), per(N + 1), mda(N + 1);
+    std::vector<Box> bcur(N + 1), bprev(N + 1);
+    std::vector<int64_t> ocur(N + 1), oprev(N + 1), coff(N + 1);
+    std::vector<Neighbour> nb((size_t)C.nbmax * (N + 1));
+    std::vector<Junction> js((size_t)C.jmax * (N + 1));
+    std::vector<char> phi((size_t)S.phi_cap * rsz);
+    std::vector<uint32_t> idl((size_t)S.phi_cap);
+    std::vector<CPoint> cont((size_t)S.cont_cap);
+    auto d2h = [&](void* dst, const void* src, size_t bytes) {
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream);
+    };
+    GG_CUDA(c, d2h(state.data(), C.state, 4 * (N + 1)));
+    GG_CUDA(c, d2h(reg.data(), C.regular, 4 * (N + 1)));
+    GG_CUDA(c, d2h(bnd.data(), C.inter_bnd, 4 * (N + 1)));
+    GG_CUDA(c, d2h(cmpn.data(), C.cmp_n, 4 * (N + 1)));
+    GG_CUDA(c, d2h(secn.data(), C.sec_n, 4 * (N + 1)));
+    GG_CUDA(c, d2h(nbn.data(), C.nb_n, 4 * (N + 1)));
+    GG_CUDA(c, d2h(newbb.data(), C.newbb, 16 * (N + 1)));
+    GG_CUDA(c, d2h(cmp.data(), C.cmp_ids, 4 * cmp.size()));
+    GG_CUDA(c, d2h(sec.data(), C.sec_ids, 4 * sec.size()));
+    GG_CUDA(c, d2h(vol.data(), C.volume, 8 * (N + 1)));
+    GG_CUDA(c, d2h(en.data(), C.energy, 8 * (N + 1)));
+    GG_CUDA(c, d2h(per.data(), C.perimeter, 8 * (N + 1)));
+    GG_CUDA(c, d2h(mda.data(), C.meanda, 8 * (N + 1)));
+    GG_CUDA(c, d2h(nb.data(), C.nb, sizeof(Neighbour) * nb.size()));
+    GG_CUDA(c, d2h(bcur.data(), S.box_cur, sizeof(Box) * (N + 1)));
+    GG_CUDA(c, d2h(bprev.data(), S.box_prev, sizeof(Box) * (N + 1)));
+    GG_CUDA(c, d2h(ocur.data(), S.off_cur, 8 * (N + 1)));
+    GG_CUDA(c, d2h(oprev.data(), S.off_prev, 8 * (N + 1)));
+    GG_CUDA(c, d2h(coff.data(), S.coff_prev, 8 * (N + 1)));
+    GG_CUDA(c, d2h(cn.data(), S.cn_prev, 4 * (N + 1)));
+    GG_CUDA(c, d2h(jn.data(), S.jn_prev, 4 * (N + 1)));
+    GG_CUDA(c, d2h(js.data(), S.jPrev, sizeof(Junction) * js.size()));
+    GG_CUDA(c, d2h(phi.data(), S.phiA, phi.size()));
+    GG_CUDA(c, d2h(idl.data(), S.idPrev, 4 * idl.size()));
+    GG_CUDA(c, d2h(cont.data(), S.contPrev, sizeof(CPoint) * cont.size()));
+    GG_CUDA(c, cudaStreamSynchronize(c->stream));
+
+    FILE* f = std::fopen(path, append ? "ab" : "wb");
+    if (!f) return fail(c, GG_E_IO, std::string("cannot open ") + path);
+    auto wi = [&](int32_t v) { std::fwrite(&v, 4, 1, f); };
+    auto wu = [&](uint32_t v) { std::fwrite(&v, 4, 1, f); };
+    auto wd = [&](double v) { std::fwrite(&v, 8, 1, f); };
+    if (!append) {
+        std::fwrite("GGD1", 1, 4, f);
+        wi(1);
+        wi(N);
+        wi(c->m);
+        wi(c->nn);
+        wd(c->h);
+        wd(c->delta);
+        wd(c->dt);
+    }
+    wi(0x52454344);
+    wi(steps_done);
+    wi(S.live);
+    for (int g = 1; g <= N; ++g) {
+        wi(g);
+        if (state[g] == G_GONE) {
+            wi(0);
+            continue;
+        }
+        wi(state[g] == G_EXISTS ? 1 : 2);
+        wi(reg[g]);
+        wi(bnd[g]);
+        wd(vol[g]);
+        wd(en[g]);
+        wd(per[g]);
+        wd(mda[g]);
+        const Box bx = bcur[g];
+        wi(bx.x0);
+        wi(bx.x1);
+        wi(bx.y0);
+        wi(bx.y1);
+        const int64_t area = box_area(bx);
+        for (int64_t k = 0; k < area; ++k) {
+            double v = 0;
+            if (state[g] == G_EXISTS) {
+                if (plain)
+                    v = reinterpret_cast<const double*>(phi.data())[ocur[g] + k];
+                else
+                    v = reinterpret_cast<const float*>(phi.data())[ocur[g] + k];
+            }
+            wd(v);
+        }
+        const Box ib = bprev[g];
+        wi(ib.x0);
+        wi(ib.x1);
+        wi(ib.y0);
+        wi(ib.y1);
+        const int64_t ia = box_area(ib);
+        for (int64_t k = 0; k < ia; ++k) wu(state[g] == G_EXISTS ? idl[oprev[g] + k] : 0xFFFFFFFFu);
+        wi(cmpn[g]);
+        for (int k = 0; k < cmpn[g]; ++k) wi(cmp[(size_t)g * C.kmax + k]);
+        wi(secn[g]);
+        for (int k = 0; k < secn[g]; ++k) wi(sec[(size_t)g * C.kmax + k]);
+        wi(cn[g]);
+        for (int k = 0; k < cn[g]; ++k) {
+            const CPoint& p = cont[coff[g] + k];
+            wd(p.x);
+            wd(p.y);
+            wd(p.energy);
+            wd(p.mob);
+        }
+        wi(jn[g]);
+        for (int k = 0; k < jn[g]; ++k) {
+            const Junction& j = js[(size_t)g * C.jmax + k];
+            wi(j.type);
+            for (int q = 0; q < 4; ++q) wu(j.grains[q]);
+            wi(j.segment);
+            wd(j.lambda);
+            wd(j.x);
+            wd(j.y);
+        }
+        wi(nbn[g]);
+        for (int k = 0; k < nbn[g]; ++k) {
+            const Neighbour& q = nb[(size_t)g * C.nbmax + k];
+            wi(q.id);
+            wd(q.length);
+            wd(q.energy);
+            wd(q.misori);
+            wd(q.mobility);
+        }
+        for (int q = 0; q < 4; ++q) wi(newbb[4 * g + q]);
+    }
+    std::fclose(f);
+    return GG_OK;
+}
+
+}  // extern "C"

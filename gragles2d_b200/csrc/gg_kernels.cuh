@@ -1,0 +1,801 @@
+// Stage kernels of one level-set timestep over all grains, templated on the
+// distance-field element type R (double: plain form; float: batched form).
+// Each kernel cites the reference stage it implements.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "gg_device.cuh"
+#include "gg_grain.cuh"
+
+namespace gg {
+namespace {  // internal linkage: each form's translation unit has its own copy
+
+
+template <typename R>
+__device__ __forceinline__ R* phiA_of(NetState* S) {
+    return reinterpret_cast<R*>(S->phiA);
+}
+template <typename R>
+__device__ __forceinline__ R* phiB_of(NetState* S) {
+    return reinterpret_cast<R*>(S->phiB);
+}
+
+// ---------------------------------------------------------------------------
+// Convolution, plain form (src/box.cpp:622-695 with the FFTW transforms
+// evaluated as separable direct DFTs in a fixed summation order): one CTA
+// per grain, phi_t (arena A) -> convolved field (arena B, same box).
+// Row r2c, column DFT and Gaussian multiply, inverse column DFT, row c2r.
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(256) k_conv_dft(NetConst C, NetState* S) {
+    const int g = blockIdx.x + 1;
+    if (g > C.N || C.state[g] != G_EXISTS) return;
+    const Box bx = S->box_cur[g];
+    const int n = box_w(bx);
+    if (n <= 0) return;
+    if (n != box_h(bx) || n > C.tmax) {
+        if (threadIdx.x == 0) set_status(S, n > C.tmax ? S_TABLE_RANGE : S_INDEX);
+        return;
+    }
+    const int half = n / 2 + 1;
+    const R* in = phiA_of<R>(S) + S->off_cur[g];
+    R* out = phiB_of<R>(S) + S->off_cur[g];
+    R* s1 = reinterpret_cast<R*>(S->spec) + S->soff_cur[g];  // n x half complex
+    R* s2 = s1 + 2 * (int64_t)n * half;                        // n x half complex
+    const double* w = C.tw + 2 * C.tw_off[n];
+    const double* G = C.gk + C.gk_off[n];
+    const int tot = n * half;
+
+    // rows: T[r][f] = sum_c x[r][c] w^(f c)
+    for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
+        const int r = idx / half, f = idx - r * half;
+        R re = 0, im = 0;
+        const R* xr = in + r * n;
+        int k = 0;
+        for (int c = 0; c < n; ++c) {
+            const R v = xr[c];
+            re = re + v * (R)w[2 * k];
+            im = im + v * (R)w[2 * k + 1];
+            k += f;
+            if (k >= n) k -= n;
+        }
+        s1[2 * idx] = re;
+        s1[2 * idx + 1] = im;
+    }
+    __syncthreads();
+    // columns: Y[q][f] = sum_r T[r][f] w^(q r), then * G(f, min(q, n-q))
+    for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
+        const int q = idx / half, f = idx - q * half;
+        R re = 0, im = 0;
+        int k = 0;
+        for (int r = 0; r < n; ++r) {
+            const R a = s1[2 * (r * half + f)], b = s1[2 * (r * half + f) + 1];
+            const R wc = (R)w[2 * k], ws = (R)w[2 * k + 1];
+            re = re + (a * wc - b * ws);
+            im = im + (a * ws + b * wc);
+            k += q;
+            if (k >= n) k -= n;
+        }
+        const int j2 = q < n - q ? q : n - q;
+        const R gv = (R)G[f * half + j2];
+        s2[2 * idx] = re * gv;
+        s2[2 * idx + 1] = im * gv;
+    }
+    __syncthreads();
+    // inverse columns: T[r][f] = sum_q Y[q][f] conj(w)^(q r)
+    for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
+        const int r = idx / half, f = idx - r * half;
+        R re = 0, im = 0;
+        int k = 0;
+        for (int q = 0; q < n; ++q) {
+            const R a = s2[2 * (q * half + f)], b = s2[2 * (q * half + f) + 1];
+            const R wc = (R)w[2 * k], ws = -(R)w[2 * k + 1];
+            re = re + (a * wc - b * ws);
+            im = im + (a * ws + b * wc);
+            k += r;
+            if (k >= n) k -= n;
+        }
+        s1[2 * idx] = re;
+        s1[2 * idx + 1] = im;
+    }
+    __syncthreads();
+    // rows c2r: x[r][c] = T0 + 2 sum_f Re(T_f e^{+i..}) (+ Nyquist)
+    const int hmax = (n - 1) / 2;
+    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+        const int r = idx / n, c = idx - r * n;
+        const R* t = s1 + 2 * (int64_t)r * half;
+        R acc = t[0];
+        int k = 0;
+        for (int f = 1; f <= hmax; ++f) {
+            k += c;
+            if (k >= n) k -= n;
+            acc = acc + (R)2.0 * (t[2 * f] * (R)w[2 * k] + t[2 * f + 1] * (R)w[2 * k + 1]);
+        }
+        if ((n & 1) == 0) {
+            const R nyq = t[2 * (n / 2)];
+            acc = acc + ((c & 1) ? -nyq : nyq);
+        }
+        out[idx] = acc;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// LSbox::computeSecondOrderNeighbours (src/box.cpp:1027-1068): one thread per
+// grain.  New list = existing members of the previous list, in order, then
+// members of their lists whose (convolution) boxes intersect ours, first
+// occurrence only, excluding ourselves.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool boxes_intersect(const Box& a, const Box& b) {  // checkIntersection, src/box.cpp:881-888
+    return !(a.x0 > b.x1 || a.x1 < b.x0 || a.y0 > b.y1 || a.y1 < b.y0);
+}
+
+__global__ void k_second_order(NetConst C, NetState* S) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (g > C.N || C.state[g] != G_EXISTS) return;
+    const int K = C.kmax;
+    const int* sec = C.sec_ids + (int64_t)g * K;
+    const int ns = C.sec_n[g];
+    int* cmp = C.cmp_ids + (int64_t)g * K;
+    int nc = 0;
+    bool overflow = false;
+    for (int a = 0; a < ns; ++a) {
+        const int id = sec[a];
+        if (C.state[id] == G_EXISTS) {
+            if (nc < K) cmp[nc++] = id; else overflow = true;
+        }
+    }
+    const Box mine = S->box_cur[g];
+    for (int a = 0; a < ns; ++a) {
+        const int id = sec[a];
+        const int* s2 = C.sec_ids + (int64_t)id * K;
+        const int n2 = C.sec_n[id];
+        for (int q = 0; q < n2; ++q) {
+            const int c = s2[q];
+            if (C.state[c] != G_EXISTS) continue;
+            if (!boxes_intersect(mine, S->box_cur[c])) continue;
+            if (c == g || c == 0) continue;
+            bool in = false;
+            for (int e = 0; e < nc; ++e)
+                if (cmp[e] == c) {
+                    in = true;
+                    break;
+                }
+            if (!in) {
+                if (nc < K) cmp[nc++] = c; else overflow = true;
+            }
+        }
+    }
+    C.cmp_n[g] = nc;
+    if (overflow) set_status(S, S_LIST_OVERFLOW);
+}
+
+// ---------------------------------------------------------------------------
+// LSbox::executeComparison + boundaryCondition + executeSetComparison
+// (src/box.cpp:890-943, 945-1025, 838-879), one CTA per grain.  Every pixel
+// of the grain's box takes the maximum of its comparison-list neighbours'
+// convolved fields (strict '>', first list member wins ties) and the domain
+// wall distance, records the winner in IDLocal, then blends with its own
+// field inside the 0.7 delta tube; the new bounding box of phi >= 0 is
+// reduced over the CTA.  IDLocal is first resized from the previous box with
+// the reference's keep-the-prefix semantics.
+// ---------------------------------------------------------------------------
+constexpr int kListMaxSmem = 128;
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_compare(NetConst C, NetState* S) {
+    const int g = blockIdx.x + 1;
+    if (g > C.N || C.state[g] != G_EXISTS) return;
+    __shared__ Box s_box[kListMaxSmem];
+    __shared__ int64_t s_off[kListMaxSmem];
+    __shared__ int s_id[kListMaxSmem];
+    __shared__ int s_red[4][8];
+    const int K = C.kmax;
+    const int nl = C.cmp_n[g] < kListMaxSmem ? C.cmp_n[g] : kListMaxSmem;
+    for (int k = threadIdx.x; k < C.cmp_n[g]; k += blockDim.x) {
+        const int id = C.cmp_ids[(int64_t)g * K + k];
+        C.sec_ids[(int64_t)g * K + k] = id;  // m_secondOrderNeighbours = m_comparisonList
+        if (k < kListMaxSmem) {
+            s_id[k] = id;
+            s_box[k] = S->box_cur[id];
+            s_off[k] = S->off_cur[id];
+        }
+    }
+    if (threadIdx.x == 0) C.sec_n[g] = C.cmp_n[g];
+    __syncthreads();
+
+    const Box bc = S->box_cur[g];
+    const int w = box_w(bc);
+    const int64_t area = box_area(bc);
+    const int b = C.b, m = C.m;
+    // BoundaryIntersection (src/box.cpp:945-962): tube = grid_blowup
+    const int lo = b + b, hi = m - b - b;
+    const bool bnd = !(bc.x0 > lo && bc.x1 < hi && bc.y0 > lo && bc.y1 < hi);
+    if (threadIdx.x == 0) C.inter_bnd[g] = bnd ? 1 : 0;
+
+    const R* conv = phiB_of<R>(S);
+    const R* self = conv + S->off_cur[g];
+    R* cmpo = phiA_of<R>(S) + S->off_cur[g];
+    const int64_t prev_area = box_area(S->box_prev[g]);
+    const int64_t keep = prev_area < area ? prev_area : area;
+    const uint32_t* idp = S->idPrev + S->off_prev[g];
+    uint32_t* idc = S->idCur + S->off_cur[g];
+    const R tube = (R)(0.7 * C.delta);
+    const R hh = (R)C.h;
+
+    int xmin = bc.x1, xmax = bc.x0, ymin = bc.y1, ymax = bc.y0;
+    for (int64_t p = threadIdx.x; p < area; p += blockDim.x) {
+        const int i = bc.y0 + (int)(p / w);
+        const int j = bc.x0 + (int)(p - (int64_t)(i - bc.y0) * w);
+        uint32_t id = p < keep ? idp[p] : 0u;
+        R out = (R)-1.0;
+        for (int k = 0; k < nl; ++k) {
+            const Box bk = s_box[k];
+            if (i >= bk.y0 && i < bk.y1 && j >= bk.x0 && j < bk.x1) {
+                const R d = conv[s_off[k] + (int64_t)(i - bk.y0) * (bk.x1 - bk.x0) + (j - bk.x0)];
+                if (d > out) {
+                    out = d;
+                    id = (uint32_t)s_id[k];
+                }
+            }
+        }
+        if (bnd) {
+            const int dxmin = -(j - b), dymin = -(i - b);
+            const int dxmax = (j - (m - b)), dymax = (i - (m - b));
+            const int dx = (abs(dxmin) < abs(dxmax)) ? dxmin : dxmax;
+            const int dy = (abs(dymin) < abs(dymax)) ? dymin : dymax;
+            double dist = 0;
+            if (dx > 0 && dy > 0)
+                dist = sqrt((double)dx * dx + dy * dy);
+            else if (dx < 0 && dy > 0)
+                dist = dy;
+            else if (dx > 0 && dy < 0)
+                dist = dx;
+            else if (dx < 0 && dy < 0)
+                dist = dx > dy ? dx : dy;
+            else if (dx == 0)
+                dist = dy > 0 ? dy : 0;
+            else  // dy == 0
+                dist = dx > 0 ? dx : 0;
+            const R wall = (R)(dist * C.h);
+            if (wall > out) {
+                out = wall;
+                id = 0u;
+            }
+        }
+        const R in = self[p];
+        const R v = (fabs((double)in) < (double)tube) ? (R)0.5 * (in - out) : in;
+        cmpo[p] = v;
+        idc[p] = id;
+        if (v >= 0) {
+            xmin = j < xmin ? j : xmin;
+            xmax = j > xmax ? j : xmax;
+            ymin = i < ymin ? i : ymin;
+            ymax = i > ymax ? i : ymax;
+        }
+        (void)hh;
+    }
+    // CTA reduction of the bounding box
+    for (int o = 16; o > 0; o >>= 1) {
+        xmin = min(xmin, __shfl_xor_sync(0xffffffffu, xmin, o));
+        xmax = max(xmax, __shfl_xor_sync(0xffffffffu, xmax, o));
+        ymin = min(ymin, __shfl_xor_sync(0xffffffffu, ymin, o));
+        ymax = max(ymax, __shfl_xor_sync(0xffffffffu, ymax, o));
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        s_red[0][warp] = xmin;
+        s_red[1][warp] = xmax;
+        s_red[2][warp] = ymin;
+        s_red[3][warp] = ymax;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        for (int q = 1; q < nw; ++q) {
+            xmin = min(xmin, s_red[0][q]);
+            xmax = max(xmax, s_red[1][q]);
+            ymin = min(ymin, s_red[2][q]);
+            ymax = max(ymax, s_red[3][q]);
+        }
+        xmin -= b;
+        xmax += b;
+        ymin -= b;
+        ymax += b;
+        if (xmin >= xmax || ymin >= ymax) {
+            xmin = bc.x0;
+            xmax = bc.x1;
+            ymin = bc.y0;
+            ymax = bc.y1;
+        }
+        int* nb = C.newbb + 4 * (int64_t)g;
+        nb[0] = xmin;
+        nb[1] = xmax;
+        nb[2] = ymin;
+        nb[3] = ymax;
+        if (C.cmp_n[g] > kListMaxSmem) set_status(S, S_LIST_OVERFLOW);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// grainhdl::level_set -> LSbox::extractContour (src/grainhdl.cpp:830-848,
+// src/box.cpp:1089-1153): one thread per grain.  Removes grains marked as
+// vanished, extracts contour and junctions from the compared field, retries
+// after clearing on irregular motion, and computes the next (square) box.
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ bool clear_contour_area(R* phi, const Box& b, const CPoint* P, int n, double h) {
+    // LSbox::clearContourGrainArea (src/box.cpp:1888-1906)
+    if (n == 0) return true;
+    double minx = P[0].x, maxx = P[0].x, miny = P[0].y, maxy = P[0].y;
+    for (int i = 0; i < n; i++) {
+        minx = fmin(minx, P[i].x);
+        maxx = fmax(maxx, P[i].x);
+        miny = fmin(miny, P[i].y);
+        maxy = fmax(maxy, P[i].y);
+    }
+    bool ok = true;
+    for (int i = (int)(miny - 1); i < maxy + 1; i++)
+        for (int j = (int)(minx - 1); j < maxx + 1; j++) {
+            uint32_t k;
+            if (!buf_index(b, i, j, &k)) {
+                ok = false;
+                continue;
+            }
+            if ((double)phi[k] >= 0) phi[k] = (R)(-h);
+        }
+    return ok;
+}
+
+template <typename R>
+__global__ void k_levelset(NetConst C, NetState* S) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (g > C.N) return;
+    const int st = C.state[g];
+    const Box bc = S->box_cur[g];
+    if (st != G_EXISTS) {
+        if (st == G_VANISHED) C.state[g] = G_GONE;  // delete grains[id] (src/grainhdl.cpp:840-842)
+        S->box_new[g] = bc;
+        S->cn_cur[g] = 0;
+        S->jn_cur[g] = 0;
+        return;
+    }
+    C.regular[g] = 1;
+    const int old_len = S->cn_prev[g];
+    R* phi = phiA_of<R>(S) + S->off_cur[g];
+    Field<R> f{phi, bc};
+    const uint32_t* idl = S->idCur + S->off_cur[g];
+    ContourOut o{S->contCur + S->coff_cur[g], S->ccap_cur[g], 0, S->jCur + (int64_t)g * C.jmax, C.jmax, 0, 0};
+    int irregular = 0;
+    bool ok = ms_contour(f, idl, (uint32_t)g, o);
+    if (ok) {
+        project_junctions(o.pts, o.n, o.js, o.jn);
+        double newVolume = contour_volume(o.pts, o.n, C.h);
+        if (!motion_regular(old_len, o.n, C.volume[g], newVolume, C.dt, &irregular)) {
+            int tries = 0;
+            do {
+                if (!clear_contour_area(phi, bc, o.pts, o.n, C.h)) o.status |= S_INDEX;
+                ok = ms_contour(f, idl, (uint32_t)g, o);
+                if (!ok) break;
+                project_junctions(o.pts, o.n, o.js, o.jn);
+                newVolume = contour_volume(o.pts, o.n, C.h);
+                if (++tries > 64) {
+                    o.status |= S_WALK_LIMIT;
+                    break;
+                }
+            } while (!motion_regular(old_len, o.n, C.volume[g], newVolume, C.dt, &irregular));
+        }
+    }
+    if (o.status) set_status(S, o.status);
+    if (!ok) {
+        C.state[g] = G_VANISHED;
+        S->box_new[g] = bc;
+        S->cn_cur[g] = 0;
+        S->jn_cur[g] = 0;
+        return;
+    }
+    if (irregular) C.regular[g] = 0;
+    int* nb = C.newbb + 4 * (int64_t)g;
+    Box nbx = bc;
+    if (!C.decouple) {
+        if (nb[0] < 0) nb[0] = 0;
+        if (nb[2] < 0) nb[2] = 0;
+        if (nb[1] > C.m) nb[1] = C.m;
+        if (nb[3] > C.m) nb[3] = C.m;
+        nbx = resize_to_square(Box{nb[0], nb[1], nb[2], nb[3]}, C.m);
+    }
+    S->box_new[g] = nbx;
+    C.perimeter[g] = contour_perimeter(o.pts, o.n, C.h);
+    S->cn_cur[g] = o.n;
+    S->jn_cur[g] = o.jn;
+}
+
+// ---------------------------------------------------------------------------
+// Arena allocation for the next step: prefix sums of the new boxes' areas
+// (distance fields), spectral scratch and contour capacities; one CTA.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) k_alloc(NetConst C, NetState* S, int spec_per_complex) {
+    __shared__ int64_t s_a[1024], s_s[1024], s_c[1024];
+    const int N = C.N;
+    const int T = blockDim.x;
+    const int per = (N + T) / T;  // slots 0..N
+    const int g0 = threadIdx.x * per;
+    const int g1 = min(N + 1, g0 + per);
+    int64_t a = 0, sp = 0, c = 0;
+    bool range = false;
+    for (int g = g0; g < g1; ++g) {
+        if (g >= 1 && C.state[g] == G_EXISTS) {
+            const Box bx = S->box_new[g];
+            const int n = box_w(bx);
+            a += box_area(bx);
+            sp += (int64_t)spec_per_complex * 2 * (int64_t)n * (n / 2 + 1);
+            c += contour_capacity(n);
+            if (n > C.tmax) range = true;
+        }
+    }
+    s_a[threadIdx.x] = a;
+    s_s[threadIdx.x] = sp;
+    s_c[threadIdx.x] = c;
+    __syncthreads();
+    for (int o = 1; o < T; o <<= 1) {
+        int64_t va = 0, vs = 0, vc = 0;
+        if ((int)threadIdx.x >= o) {
+            va = s_a[threadIdx.x - o];
+            vs = s_s[threadIdx.x - o];
+            vc = s_c[threadIdx.x - o];
+        }
+        __syncthreads();
+        s_a[threadIdx.x] += va;
+        s_s[threadIdx.x] += vs;
+        s_c[threadIdx.x] += vc;
+        __syncthreads();
+    }
+    int64_t ra = s_a[threadIdx.x] - a, rs = s_s[threadIdx.x] - sp, rc = s_c[threadIdx.x] - c;
+    for (int g = g0; g < g1; ++g) {
+        S->off_new[g] = ra;
+        S->soff_new[g] = rs;
+        S->coff_new[g] = rc;
+        if (g >= 1 && C.state[g] == G_EXISTS) {
+            const Box bx = S->box_new[g];
+            const int n = box_w(bx);
+            ra += box_area(bx);
+            rs += (int64_t)spec_per_complex * 2 * (int64_t)n * (n / 2 + 1);
+            const int cc = contour_capacity(n);
+            S->ccap_new[g] = cc;
+            rc += cc;
+        } else {
+            S->ccap_new[g] = 0;
+        }
+    }
+    if (range) set_status(S, S_TABLE_RANGE);
+    if (threadIdx.x == T - 1) {
+        if (s_a[T - 1] > S->phi_cap || s_s[T - 1] > S->spec_cap || s_c[T - 1] > S->cont_cap)
+            set_status(S, S_ARENA_FULL);
+        S->phi_used = s_a[T - 1];
+        S->spec_used = s_s[T - 1];
+        S->cont_used = s_c[T - 1];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// LSbox::computeVolumeAndEnergy + ExplicitGrainBoundary::buildDirectNeighbours
+// (src/box.cpp:1201-1228, src/grainBoundary.cpp:85-199): one thread per grain.
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void k_neighbours(NetConst C, NetState* S) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int loop = S->loop;
+    if (g > C.N || C.state[g] != G_EXISTS || C.regular[g] == 0) return;
+    CPoint* P = S->contCur + S->coff_cur[g];
+    const int n = S->cn_cur[g];
+    const double h = C.h;
+    const double newVolume = fabs(contour_volume(P, n, h));
+    const Box bc = S->box_cur[g];
+    const R* phi = phiA_of<R>(S) + S->off_cur[g];
+    const uint32_t* idl = S->idCur + S->off_cur[g];
+    Neighbour* nb = C.nb + (int64_t)g * C.nbmax;
+    int nn = 0;
+    bool invalid = false, overflow = false;
+    const double* qg = C.quat + 4 * (int64_t)g;
+    for (int i = 0; i < n - 1; i++) {
+        const double px = P[i].x, py = P[i].y;
+        int pxGrid = (int)px, pyGrid = (int)py;
+        uint32_t k;
+        if (!buf_index(bc, pyGrid, pxGrid, &k)) { invalid = true; break; }
+        if ((double)phi[k] > 0) {
+            pxGrid = (int)(px + 1);
+            if (!buf_index(bc, pyGrid, pxGrid, &k)) { invalid = true; break; }
+            if ((double)phi[k] > 0) {
+                pyGrid = (int)(py + 1);
+                if (!buf_index(bc, pyGrid, pxGrid, &k)) { invalid = true; break; }
+                if ((double)phi[k] > 0) pxGrid = (int)px;
+            }
+        }
+        // LSbox::getNeighbourAt (src/box.cpp:2190-2195)
+        if (pyGrid < 0 || pyGrid >= bc.y1 || pxGrid < 0 || pxGrid >= bc.x1) { invalid = true; break; }
+        if (!buf_index(bc, pyGrid, pxGrid, &k)) { invalid = true; break; }
+        const uint32_t cid = idl[k];
+        if (cid != 0 && (cid > (uint32_t)C.N || C.state[cid] == G_GONE)) { invalid = true; break; }
+        const double theta = grain_misorientation(qg, C.quat + 4 * (int64_t)cid);
+        P[i].mob = mobility_model(theta, C);
+        P[i].energy = read_shockley(theta, C);
+        const double dx = P[i].x - P[i + 1].x, dy = P[i].y - P[i + 1].y;
+        const double line_length = sqrt(dx * dx + dy * dy) * h;
+        int e = 0;
+        for (; e < nn; ++e)
+            if (nb[e].id == (int)cid) break;
+        if (e == nn) {
+            if (nn >= C.nbmax) {
+                overflow = true;
+                continue;
+            }
+            nb[nn].id = (int)cid;
+            nb[nn].length = 0;
+            nb[nn].energy = P[i].energy;
+            nb[nn].misori = theta;
+            nb[nn].mobility = P[i].mob;
+            nn++;
+        }
+        nb[e].length += line_length;
+    }
+    C.nb_n[g] = nn;
+    if (overflow) set_status(S, S_NEIGHBOUR_OVERFLOW);
+    if (invalid) {
+        C.regular[g] = 0;  // markAsInvalidMotion (src/box.cpp:1939-1945)
+    } else if (n > 0) {
+        P[n - 1].energy = P[0].energy;
+        P[n - 1].mob = P[0].mob;
+    }
+    C.energy[g] = contour_energy(P, n, h);
+    double dA = newVolume - C.volume[g];
+    dA = dA / C.dt;
+    dA = dA * (3 / kPi);
+    const unsigned int lp = (unsigned int)loop;
+    if ((unsigned long)(lp - 1u) % (unsigned long)C.analysis_timestep == 0 || lp == 0) C.meanda[g] = 0;
+    C.meanda[g] += dA;
+    C.volume[g] = newVolume;
+}
+
+// ---------------------------------------------------------------------------
+// LSbox::executeRedistancing (src/box.cpp:1259-1399): one CTA per grain;
+// compared field (arena A, box_cur) -> phi_{t+1} (arena B, box_new).
+// y sweeps run one thread per column, x sweeps one thread per row.
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ void redistance_grain(const R* __restrict__ in, const Box bi, R* __restrict__ out, const Box bo, R h,
+                                 R delta) {
+    const int wi = box_w(bi), wo = box_w(bo);
+    const int64_t ao = box_area(bo);
+    for (int64_t p = threadIdx.x; p < ao; p += blockDim.x) out[p] = (R)-1.0;
+    __syncthreads();
+    const int ixmin = (bi.x0 < bo.x0) ? bo.x0 : bi.x0;
+    const int iymin = (bi.y0 < bo.y0) ? bo.y0 : bi.y0;
+    const int ixmax = (bi.x1 < bo.x1) ? bi.x1 : bo.x1;
+    const int iymax = (bi.y1 < bo.y1) ? bi.y1 : bo.y1;
+#define GG_IN(i, j) in[(int64_t)((i) - bi.y0) * wi + ((j) - bi.x0)]
+#define GG_OUT(i, j) out[(int64_t)((i) - bo.y0) * wo + ((j) - bo.x0)]
+    for (int j = ixmin + (int)threadIdx.x; j < bo.x1; j += blockDim.x) {
+        for (int i = iymin; i < bo.y1 - 1; i++) {  // y forward
+            R cand;
+            if (j < ixmax && i < iymax - 1) {
+                const R a = GG_IN(i, j), c = GG_IN(i + 1, j);
+                if (a * c <= (R)0.0) {
+                    const R slope = (c - a) / h;
+                    const R dz = -a / slope;
+                    if (fabs(GG_OUT(i, j)) > fabs(dz)) GG_OUT(i, j) = -dz * (R)sgn(slope);
+                }
+                cand = GG_OUT(i, j) + ((R)sgn(c) * h);
+            } else {
+                cand = GG_OUT(i, j) + ((R)sgn(GG_OUT(i + 1, j)) * h);
+            }
+            if (fabs(cand) < fabs(GG_OUT(i + 1, j))) GG_OUT(i + 1, j) = cand;
+        }
+        for (int i = iymax - 1; i > bo.y0; i--) {  // y backward
+            R cand;
+            if (j < ixmax && i > iymin)
+                cand = GG_OUT(i, j) + ((R)sgn(GG_IN(i - 1, j)) * h);
+            else
+                cand = GG_OUT(i, j) + ((R)sgn(GG_OUT(i - 1, j)) * h);
+            if (fabs(cand) < fabs(GG_OUT(i - 1, j))) GG_OUT(i - 1, j) = cand;
+        }
+    }
+    __syncthreads();
+    for (int i = iymin + (int)threadIdx.x; i < bo.y1; i += blockDim.x) {
+        for (int j = ixmin; j < bo.x1 - 1; j++) {  // x forward
+            R cand;
+            if (j < ixmax - 1 && i < iymax) {
+                const R a = GG_IN(i, j), c = GG_IN(i, j + 1);
+                if (a * c <= (R)0.0) {
+                    const R slope = (c - a) / h;
+                    const R dz = -a / slope;
+                    if (fabs(GG_OUT(i, j)) > fabs(dz)) GG_OUT(i, j) = -dz * (R)sgn(slope);
+                }
+                cand = GG_OUT(i, j) + ((R)sgn(c) * h);
+            } else {
+                cand = GG_OUT(i, j) + ((R)sgn(GG_OUT(i, j + 1)) * h);
+            }
+            if (fabs(cand) < fabs(GG_OUT(i, j + 1))) GG_OUT(i, j + 1) = cand;
+        }
+        for (int j = ixmax - 1; j > bo.x0; j--) {  // x backward
+            R cand;
+            if (j > ixmin && i < iymax)
+                cand = GG_OUT(i, j) + ((R)sgn(GG_IN(i, j - 1)) * h);
+            else
+                cand = GG_OUT(i, j) + (R)sgn(GG_OUT(i, j - 1)) * h;
+            if (fabs(cand) < fabs(GG_OUT(i, j - 1))) GG_OUT(i, j - 1) = cand;
+        }
+    }
+#undef GG_IN
+#undef GG_OUT
+    __syncthreads();
+    for (int64_t p = threadIdx.x; p < ao; p += blockDim.x) {  // clampValues(-delta, delta)
+        const R v = out[p];
+        if (v < -delta)
+            out[p] = -delta;
+        else if (v > delta)
+            out[p] = delta;
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_redistance(NetConst C, NetState* S) {
+    const int g = blockIdx.x + 1;
+    if (g > C.N || C.state[g] != G_EXISTS) return;
+    const R* in = phiA_of<R>(S) + S->off_cur[g];
+    R* out = phiB_of<R>(S) + S->off_new[g];
+    redistance_grain<R>(in, S->box_cur[g], out, S->box_new[g], (R)C.h, (R)C.delta);
+}
+
+// ---------------------------------------------------------------------------
+// End of step: grainhdl::get_biggestGrainVol (src/grainhdl.cpp:1744-1754) and
+// the buffer switches; rotates per-step roles in NetState.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) k_finalize(NetConst C, NetState* S, int rotate) {
+    __shared__ int s_cnt[32];
+    __shared__ double s_max[32];
+    int cnt = 0;
+    double mx = 0.0;
+    for (int g = threadIdx.x + 1; g <= C.N; g += blockDim.x) {
+        if (C.state[g] != G_GONE) {
+            cnt++;
+            mx = fmax(mx, C.volume[g]);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        s_cnt[threadIdx.x >> 5] = cnt;
+        s_max[threadIdx.x >> 5] = mx;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    for (int q = 1; q < (int)((blockDim.x + 31) >> 5); ++q) {
+        cnt += s_cnt[q];
+        mx = fmax(mx, s_max[q]);
+    }
+    S->live = cnt;
+    S->max_volume = mx;
+    if (!rotate) return;
+    Box* tb = S->box_prev;
+    S->box_prev = S->box_cur;
+    S->box_cur = S->box_new;
+    S->box_new = tb;
+    int64_t* to = S->off_prev;
+    S->off_prev = S->off_cur;
+    S->off_cur = S->off_new;
+    S->off_new = to;
+    int64_t* ts = S->soff_cur;
+    S->soff_cur = S->soff_new;
+    S->soff_new = ts;
+    void* tp = S->phiA;
+    S->phiA = S->phiB;
+    S->phiB = tp;
+    uint32_t* ti = S->idPrev;
+    S->idPrev = S->idCur;
+    S->idCur = ti;
+    CPoint* tc = S->contPrev;
+    S->contPrev = S->contCur;
+    S->contCur = tc;
+    int64_t* tco = S->coff_prev;
+    S->coff_prev = S->coff_cur;
+    S->coff_cur = S->coff_new;
+    S->coff_new = tco;
+    int32_t* tcc = S->ccap_prev;
+    S->ccap_prev = S->ccap_cur;
+    S->ccap_cur = S->ccap_new;
+    S->ccap_new = tcc;
+    int32_t* tn = S->cn_prev;
+    S->cn_prev = S->cn_cur;
+    S->cn_cur = tn;
+    Junction* tj = S->jPrev;
+    S->jPrev = S->jCur;
+    S->jCur = tj;
+    int32_t* tjn = S->jn_prev;
+    S->jn_prev = S->jn_cur;
+    S->jn_cur = tjn;
+    S->loop += 1;
+}
+
+// ---------------------------------------------------------------------------
+// Initialisation for voxelized input (src/box.cpp:322-341): +-h from the ID
+// field, then the redistancing kernel, then the contour of the result.
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(256) k_init_phi(NetConst C, NetState* S, const int32_t* __restrict__ ids) {
+    const int g = blockIdx.x + 1;
+    if (g > C.N || C.state[g] != G_EXISTS) return;
+    const Box bx = S->box_cur[g];
+    const int w = box_w(bx);
+    const int64_t area = box_area(bx);
+    R* phi = phiA_of<R>(S) + S->off_cur[g];
+    const int lo = C.b, hi = C.m - C.b - 1;
+    const R h = (R)C.h;
+    for (int64_t p = threadIdx.x; p < area; p += blockDim.x) {
+        const int i = bx.y0 + (int)(p / w), j = bx.x0 + (int)(p % w);
+        R v;
+        if (i < lo || i > hi || j < lo || j > hi)
+            v = -h;
+        else
+            v = (ids[(int64_t)(i - lo) * C.nn + (j - lo)] == g) ? h : -h;
+        phi[p] = v;
+    }
+}
+
+template <typename R>
+__global__ void k_init_contour(NetConst C, NetState* S) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (g > C.N || C.state[g] != G_EXISTS) return;
+    const Box bx = S->box_cur[g];
+    Field<R> f{phiA_of<R>(S) + S->off_cur[g], bx};
+    const uint32_t* idl = S->idPrev + S->off_prev[g];
+    ContourOut o{S->contPrev + S->coff_prev[g], S->ccap_prev[g], 0, S->jPrev + (int64_t)g * C.jmax, C.jmax, 0, 0};
+    const bool ok = ms_contour(f, idl, (uint32_t)g, o);
+    if (o.status) set_status(S, o.status);
+    if (!ok) {
+        C.state[g] = G_VANISHED;
+        S->cn_prev[g] = 0;
+        S->jn_prev[g] = 0;
+        C.volume[g] = 0;
+        return;
+    }
+    project_junctions(o.pts, o.n, o.js, o.jn);
+    S->cn_prev[g] = o.n;
+    S->jn_prev[g] = o.jn;
+    C.volume[g] = contour_volume(o.pts, o.n, C.h);
+}
+
+// grainhdl::find_neighbors + LSbox::computeDirectNeighbours
+// (src/grainhdl.cpp:1258-1283, src/box.cpp:2220-2237): every other grain whose
+// closed box overlaps (RTree::Overlap, src/RTree.h:1092-1105), ascending ID.
+__global__ void k_find_neighbors(NetConst C, NetState* S) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (g > C.N || C.state[g] == G_GONE) return;
+    const Box a = S->box_cur[g];
+    int ns = 0, nbn = 0;
+    bool overflow = false;
+    int* sec = C.sec_ids + (int64_t)g * C.kmax;
+    Neighbour* nb = C.nb + (int64_t)g * C.nbmax;
+    for (int k = 1; k <= C.N; ++k) {
+        if (k == g || C.state[k] == G_GONE) continue;
+        const Box b = S->box_cur[k];
+        if (a.x0 > b.x1 || b.x0 > a.x1 || a.y0 > b.y1 || b.y0 > a.y1) continue;
+        if (ns < C.kmax) sec[ns++] = k; else overflow = true;
+        if (nbn < C.nbmax) {
+            nb[nbn].id = k;
+            nb[nbn].length = 0;
+            nb[nbn].energy = 0;
+            nb[nbn].misori = 0;
+            nb[nbn].mobility = 0;
+            nbn++;
+        }
+    }
+    C.sec_n[g] = ns;
+    C.cmp_n[g] = 0;
+    C.nb_n[g] = nbn;
+    if (overflow) set_status(S, S_LIST_OVERFLOW);
+}
+
+}  // namespace
+}  // namespace gg

@@ -1,0 +1,41 @@
+// Launch sequences of the stages, shared by the plain (double) and batched
+// (float) translation units.  Included once per TU with GG_REAL and
+// GG_FORM defined.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "gg_device.cuh"
+
+namespace gg {
+
+// Stage selectors for launch_stages().
+enum : int {
+    ST_CONV = 1 << 0,
+    ST_SECOND = 1 << 1,
+    ST_COMPARE = 1 << 2,
+    ST_LEVELSET = 1 << 3,
+    ST_REDIST = 1 << 4,  // alloc + neighbours + redistancing + end of step
+    ST_ALL = 0x1f
+};
+
+struct LaunchCfg {
+    int conv_threads;
+    int compare_threads;
+    int redist_threads;
+    int grain_threads;  // one-thread-per-grain kernels
+};
+
+// Declared per form; defined in gg_plain.cu / gg_batched.cu.
+cudaError_t plain_stages(const NetConst& C, NetState* dS, int stages, cudaStream_t s, const LaunchCfg& cfg);
+cudaError_t plain_init(const NetConst& C, NetState* dS, const int32_t* d_ids, cudaStream_t s);
+cudaError_t plain_corrector(const NetConst& C, NetState* dS, cudaStream_t s);
+cudaError_t batched_stages(const NetConst& C, NetState* dS, int stages, cudaStream_t s, const LaunchCfg& cfg);
+size_t conv_sep_smem(int tmax);
+cudaError_t batched_prepare(int tmax);
+cudaError_t batched_init(const NetConst& C, NetState* dS, const int32_t* d_ids, cudaStream_t s);
+cudaError_t finalize_only(const NetConst& C, NetState* dS, int rotate, cudaStream_t s);
+cudaError_t swap_phi(NetState* dS, cudaStream_t s);
+cudaError_t find_neighbors_launch(const NetConst& C, NetState* dS, cudaStream_t s);
+
+}  // namespace gg

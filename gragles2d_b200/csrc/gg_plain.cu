@@ -1,0 +1,70 @@
+// Plain form: FP64 kernels compiled without FMA contraction (--fmad=false),
+// so every sum, product and quotient rounds exactly as the reference's
+// host arithmetic does.
+#include "gg_corrector.cuh"
+#include "gg_kernels.cuh"
+#include "gg_launch.cuh"
+
+namespace gg {
+
+__global__ void k_swap_phi(NetState* S) {
+    void* t = S->phiA;
+    S->phiA = S->phiB;
+    S->phiB = t;
+}
+
+cudaError_t swap_phi(NetState* dS, cudaStream_t s) {
+    k_swap_phi<<<1, 1, 0, s>>>(dS);
+    return cudaGetLastError();
+}
+
+cudaError_t finalize_only(const NetConst& C, NetState* dS, int rotate, cudaStream_t s) {
+    k_finalize<<<1, 1024, 0, s>>>(C, dS, rotate);
+    return cudaGetLastError();
+}
+
+cudaError_t find_neighbors_launch(const NetConst& C, NetState* dS, cudaStream_t s) {
+    const int gt = 128;
+    k_find_neighbors<<<(C.N + gt - 1) / gt, gt, 0, s>>>(C, dS);
+    return cudaGetLastError();
+}
+
+cudaError_t plain_init(const NetConst& C, NetState* dS, const int32_t* d_ids, cudaStream_t s) {
+    if (C.N <= 0) return cudaSuccess;
+    k_init_phi<double><<<C.N, 256, 0, s>>>(C, dS, d_ids);
+    k_redistance<double><<<C.N, 256, 0, s>>>(C, dS);
+    k_swap_phi<<<1, 1, 0, s>>>(dS);
+    const int gt = 64;
+    k_init_contour<double><<<(C.N + gt - 1) / gt, gt, 0, s>>>(C, dS);
+    return cudaGetLastError();
+}
+
+cudaError_t plain_corrector(const NetConst& C, NetState* dS, cudaStream_t s) {
+    k_corrector<double><<<C.N, 256, 0, s>>>(C, dS);
+    return cudaGetLastError();
+}
+
+cudaError_t plain_stages(const NetConst& C, NetState* dS, int stages, cudaStream_t s, const LaunchCfg& cfg) {
+    if (C.N <= 0) return cudaSuccess;
+    const int gt = cfg.grain_threads;
+    const int gblocks = (C.N + gt - 1) / gt;
+    if (stages & ST_CONV) {
+        k_conv_dft<double><<<C.N, cfg.conv_threads, 0, s>>>(C, dS);
+        if (!C.isotropic) {
+            cudaError_t e = plain_corrector(C, dS, s);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    if (stages & ST_SECOND) k_second_order<<<gblocks, gt, 0, s>>>(C, dS);
+    if (stages & ST_COMPARE) k_compare<double><<<C.N, cfg.compare_threads, 0, s>>>(C, dS);
+    if (stages & ST_LEVELSET) k_levelset<double><<<gblocks, gt, 0, s>>>(C, dS);
+    if (stages & ST_REDIST) {
+        k_alloc<<<1, 1024, 0, s>>>(C, dS, 2);
+        k_neighbours<double><<<gblocks, gt, 0, s>>>(C, dS);
+        k_redistance<double><<<C.N, cfg.redist_threads, 0, s>>>(C, dS);
+        k_finalize<<<1, 1024, 0, s>>>(C, dS, 1);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace gg

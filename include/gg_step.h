@@ -1,0 +1,193 @@
+/*
+ * gg_step.h -- C ABI of the B200 GraGLeS2D level-set step.
+ *
+ * One context holds one grain network resident on one GPU: per-grain square
+ * boxes (the reference's LSbox, src/box.h:68-111) with their distance
+ * functions, IDLocal maps, comparison lists, contours, junctions and
+ * neighbour characteristics.  The stage entry points are the stage methods
+ * of the reference's time loop (grainhdl, src/grainhdl.h:115-141) and run
+ * every grain of the network in one launch sequence on the device.
+ *
+ * Conventions
+ *  - Grain IDs are the reference's: 1..N for grains, 0 for the domain
+ *    boundary grain (src/grainhdl.h:153-160).
+ *  - Every function returns 0 on success or a positive GG_E_* code; no
+ *    C++ exception crosses this boundary.  gg_last_error() describes the
+ *    last failure of a context.
+ *  - Host arrays passed in are copied; the library owns all device memory.
+ *  - A context is used from one host thread at a time.
+ *  - Precision GG_PRECISION_PLAIN computes in FP64 and reproduces the
+ *    reference's arithmetic; GG_PRECISION_BATCHED computes the bulk stages
+ *    in FP32 (areas and energies still accumulate in FP64) and runs each
+ *    step as one captured CUDA graph.
+ */
+#ifndef GG_STEP_H
+#define GG_STEP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GG_ABI_VERSION 1
+
+enum {
+    GG_OK = 0,
+    GG_E_INVALID = 1,      /* bad argument or unsupported setting */
+    GG_E_CUDA = 2,         /* CUDA runtime error */
+    GG_E_IO = 3,           /* file missing or malformed */
+    GG_E_STATE = 4,        /* call out of order (e.g. step before load) */
+    GG_E_CAPACITY = 5,     /* a device arena, list or table overflowed */
+    GG_E_NUMERIC = 6       /* NaN or walk-limit detected on the device */
+};
+
+enum { GG_PRECISION_PLAIN = 0, GG_PRECISION_BATCHED = 1 };
+
+/* Device status bits reported by gg_status(). */
+enum {
+    GG_S_ARENA_FULL = 1 << 0,
+    GG_S_LIST_OVERFLOW = 1 << 1,
+    GG_S_CONTOUR_OVERFLOW = 1 << 2,
+    GG_S_JUNCTION_OVERFLOW = 1 << 3,
+    GG_S_WALK_LIMIT = 1 << 4,
+    GG_S_TABLE_RANGE = 1 << 5,
+    GG_S_NEIGHBOUR_OVERFLOW = 1 << 6,
+    GG_S_NAN = 1 << 7
+};
+
+/*
+ * Simulation settings used on the step path.  Field names follow the
+ * parameters.xml tags parsed by Settings::initializeParameters
+ * (src/Settings.cpp:111-283).  theta_ref_deg, gamma_hagb and m_hagb are
+ * constants in the reference (src/box.cpp:1786-1787, 1846;
+ * src/junction.cpp:40-41); they default to those constants.
+ */
+typedef struct gg_params {
+    int32_t struct_size;              /* sizeof(gg_params) */
+    int32_t precision;                /* GG_PRECISION_* */
+    int32_t start_time;               /* StartTime */
+    int32_t number_of_timesteps;      /* NumberOfTimesteps */
+    int32_t analysis_timestep;        /* AnalysisTimestep */
+    int32_t breakup_number;           /* BreakupNumber */
+    int32_t number_of_particles;      /* NumberOfParticles */
+    int32_t number_of_points_per_grain; /* NumberOfPointsPerGrain */
+    int32_t domain_border_size;       /* DomainBorderSize */
+    int32_t microstructure_gen_mode;  /* MicrostructureGenMode (4 supported) */
+    int32_t convolution_mode;         /* ConvolutionMode (2 = Gaussian supported) */
+    int32_t lattice_type;             /* LatticeType (0 = cubic supported) */
+    int32_t is_isotropic_network;     /* IsIsotropicNetwork */
+    int32_t use_mobility_model;       /* UseMobilityModel (0, 1) */
+    int32_t identify_twins;           /* IdentifyTwins */
+    int32_t research_mode;            /* ResearchMode (0 supported) */
+    int32_t research_project;         /* ResearchProject */
+    int32_t decouple_grains;          /* DecoupleGrains */
+    int32_t grid_coarsement;          /* GridCoarsement (0 supported) */
+    int32_t use_stored_elastic_energy;/* UseStoredElasticEnergy (0 supported) */
+    int32_t use_magnetic_field;       /* UseMagneticField (0 supported) */
+    int32_t reserved_i[5];
+    double triple_point_drag;         /* TriplePointDrag */
+    double constant_sector_radius;    /* ConstantSectorRadius (grid points) */
+    double interpolating_sector_radius; /* InterpolatingSectorRadius (grid points) */
+    double hagb_energy;               /* HAGB_Energy */
+    double hagb_mobility;             /* HAGB_Mobility */
+    double physical_domain_size;      /* Physical_Domain_Size */
+    double time_slope;                /* GaussianKernelUserDefTimeSlope */
+    double theta_ref_deg;             /* Read-Shockley cut-off angle */
+    double gamma_hagb;                /* relative high-angle boundary energy */
+    double m_hagb;                    /* relative high-angle boundary mobility */
+    double reserved_d[6];
+    char read_from_filename[512];     /* ReadFromFilename (.bin ID field) */
+    char additional_filename[512];    /* AdditionalFilename (.uds header) */
+} gg_params;
+
+/* Per-grain scalars, as reported by the reference's texture output
+ * (TextureData, src/Structs.h; src/box.cpp:2296-2312). */
+typedef struct gg_grain_stats {
+    int32_t id;
+    int32_t state;             /* 0 removed, 1 exists, 2 vanished this step */
+    int32_t motion_regular;    /* LSbox::isMotionRegular */
+    int32_t intersects_boundary;
+    int32_t n_neighbours;      /* direct neighbours */
+    int32_t contour_points;    /* contour length incl. closing point */
+    int32_t box[4];            /* xmin, xmax, ymin, ymax of the current box */
+    double area;               /* m_volume */
+    double energy;             /* m_energy */
+    double perimeter;          /* m_perimeter */
+    double mean_da;            /* m_meanDa */
+} gg_grain_stats;
+
+typedef struct gg_ctx gg_ctx;
+
+/* Fills defaults equal to Settings' static initialisers (src/Settings.cpp:26-79). */
+int gg_params_default(gg_params* p);
+
+/* Parses a parameters.xml (replaces Settings::initializeParameters,
+ * src/Settings.cpp:84-289).  Unknown tags are ignored. */
+int gg_params_from_xml(const char* path, gg_params* p);
+
+/* Creates a context on a CUDA device (replaces grainhdl's constructor and
+ * the settings part of grainhdl::setSimulationParameter,
+ * src/grainhdl.cpp:56-136). */
+int gg_create(const gg_params* p, int device, gg_ctx** out);
+void gg_destroy(gg_ctx* ctx);
+const char* gg_last_error(const gg_ctx* ctx);
+
+/* Loads a voxelized microstructure (replaces grainhdl::read_HeaderCPG and
+ * grainhdl::read_voxelized_microstructure, src/grainhdl.cpp:275-511).
+ * ids: nn*nn int32 grain IDs, row-major, row outer; euler: 3 Bunge angles
+ * per grain (index id-1); bbox: xmin, xmax, ymin, ymax, count per grain in
+ * interior coordinates.  Grains with count 0 are absent, as in the reference. */
+int gg_load_voxels(gg_ctx* ctx, int32_t nn, const int32_t* ids, int32_t n_grains, const double* euler,
+                   const int32_t* bbox);
+/* Same, reading the .uds/.bin pair named by the parameters (paths relative to
+ * base_dir when not absolute). */
+int gg_load_voxel_files(gg_ctx* ctx, const char* base_dir);
+
+/* grainhdl::distanceInitialisation for mode-4 input (src/grainhdl.cpp:728-753,
+ * src/box.cpp:322-341): +-h field, redistancing, contour. */
+int gg_distance_initialisation(gg_ctx* ctx);
+/* grainhdl::find_neighbors (src/grainhdl.cpp:1258-1283): every grain whose box
+ * intersects, in ascending ID order. */
+int gg_find_neighbors(gg_ctx* ctx);
+/* Replaces the initial comparison lists with caller-given ordered lists
+ * (CSR over grains 1..N: offsets[N+1], ids); use to reproduce an exact
+ * neighbour order (ties in the comparison take the first list member). */
+int gg_set_neighbours(gg_ctx* ctx, const int32_t* offsets, const int32_t* ids);
+
+/* Stage calls of one timestep, in the reference loop's order
+ * (src/grainhdl.cpp:1049-1142); buffer switches are implicit.  `loop` is
+ * the reference's loop counter (the corrector is off for loop 0). */
+int gg_convolution(gg_ctx* ctx, int32_t loop);
+int gg_update_second_order_neighbors(gg_ctx* ctx);
+int gg_comparison(gg_ctx* ctx);
+int gg_level_set(gg_ctx* ctx, int32_t loop);
+int gg_redistancing(gg_ctx* ctx, int32_t loop);
+/* grainhdl::get_biggestGrainVol: live-grain count and largest area. */
+int gg_grain_count(gg_ctx* ctx, int32_t* current_nr_grains, double* max_volume);
+
+/* Runs nsteps whole timesteps starting at loop index `loop`.  The batched
+ * form replays one captured CUDA graph per step. */
+int gg_step(gg_ctx* ctx, int32_t loop, int32_t nsteps);
+
+/* Device status word (GG_S_* bits), accumulated since the last clear. */
+int gg_status(gg_ctx* ctx, uint32_t* status, int32_t clear);
+
+/* Per-grain scalars for grains 1..N (out has room for N entries). */
+int gg_read_grain_stats(gg_ctx* ctx, gg_grain_stats* out, int32_t capacity);
+/* Number of grain slots N and the grid size (ngridpoints). */
+int gg_dims(gg_ctx* ctx, int32_t* n_grains, int32_t* ngridpoints, double* h, double* delta, double* dt);
+
+/* Writes the whole network state in the oracle dump format (one record). */
+int gg_dump(gg_ctx* ctx, const char* path, int32_t steps_done, int32_t append);
+
+/* Wall time of the device work of the last gg_step call, in milliseconds
+ * (CUDA events on the context's stream). */
+int gg_last_step_ms(gg_ctx* ctx, double* ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GG_STEP_H */

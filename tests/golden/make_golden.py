@@ -1,0 +1,68 @@
+"""Generates the golden fixtures of the parity tests by running the reference.
+
+For each case: a seeded synthetic voxelized microstructure (``*.uds`` +
+``*.bin``), its ``parameters.xml``, and the state dumps of GraGLeS2D's own
+C++ (``oracle/_ref/gg_ref``, built by ``make -C oracle ref`` from the
+reference sources) after initialisation and after selected steps, gzipped.
+
+Run from the repository root in the build container (it needs the reference
+tree to build the oracle):  python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import gzip
+import json
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.abspath(os.path.join(HERE, "..", ".."))
+sys.path.insert(0, ROOT)
+
+from gragles2d_b200 import microstructure as ms  # noqa: E402
+
+GG_REF = os.path.join(ROOT, "oracle", "_ref", "gg_ref")
+
+# name: (generator, grains, grid, seed, steps, dump_every, parameter overrides)
+CASES = {
+    "iso_v20": ("voronoi", 20, 100, 0, 24, 8, {"IsIsotropicNetwork": 1}),
+    "iso_v60": ("voronoi", 60, 140, 1, 40, 10, {"IsIsotropicNetwork": 1}),
+    "rs_v30": ("voronoi", 30, 120, 2, 20, 5, {"IsIsotropicNetwork": 0}),
+    "mob_v30": ("voronoi", 30, 120, 3, 20, 5,
+                {"IsIsotropicNetwork": 0, "UseMobilityModel": 1, "TriplePointDrag": 5.0}),
+}
+
+
+def make_case(name: str, spec) -> dict:
+    gen, n, nn, seed, steps, every, over = spec
+    d = os.path.join(HERE, name)
+    if os.path.isdir(d):
+        shutil.rmtree(d)
+    micro = ms.voronoi(n, nn, seed) if gen == "voronoi" else ms.clustered(n, nn, seed)
+    xml = ms.make_case(d, name, micro, NumberOfTimesteps=steps, **over)
+    dump = os.path.join(d, "reference.dump")
+    out = subprocess.run([GG_REF, os.path.basename(xml), "reference.dump", str(every), "1"], cwd=d,
+                         check=True, capture_output=True, text=True)
+    info = json.loads(out.stdout.strip().splitlines()[-1])
+    with open(dump, "rb") as f, gzip.open(dump + ".gz", "wb", compresslevel=9) as g:
+        shutil.copyfileobj(f, g)
+    os.remove(dump)
+    info.update({"generator": gen, "grains": n, "grid": nn, "seed": seed, "steps": steps, "dump_every": every,
+                 "overrides": over})
+    with open(os.path.join(d, "case.json"), "w") as f:
+        json.dump(info, f, indent=1)
+    return info
+
+
+def main():
+    if not os.path.exists(GG_REF):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    for name, spec in CASES.items():
+        info = make_case(name, spec)
+        print(name, info)
+
+
+if __name__ == "__main__":
+    main()
