@@ -17,7 +17,7 @@ constexpr int kSepSmemMaxN = 110;  // 2 n^2 + n floats of shared memory
 __global__ void __launch_bounds__(256) k_conv_sep(NetConst C, NetState* S) {
     extern __shared__ float sm[];
     const int g = blockIdx.x + 1;
-    if (g > C.N || C.state[g] != G_EXISTS) return;
+    if (g > C.N || C.state[g] != G_EXISTS || halted(S)) return;
     const Box bx = S->box_cur[g];
     const int n = box_w(bx);
     if (n <= 0) return;

@@ -389,10 +389,11 @@ __device__ __forceinline__ double pixel_weight(const NetConst& C, int g, const C
 template <typename R>
 __global__ void __launch_bounds__(256) k_corrector(NetConst C, NetState* S) {
     const int g = blockIdx.x + 1;
-    if (g > C.N || C.state[g] != G_EXISTS || C.regular[g] == 0 || S->loop == 0) return;
+    if (g > C.N || C.state[g] != G_EXISTS || C.regular[g] == 0 || S->loop == 0 || halted(S)) return;
     __shared__ SectorSet sec;
     const CPoint* P = S->contPrev + S->coff_prev[g];
     const int size = S->cn_prev[g];
+    if (size < 2) return;
     const Box ib = S->box_prev[g];
     const uint32_t* idl = S->idPrev + S->off_prev[g];
     if (threadIdx.x == 0) {
@@ -400,7 +401,6 @@ __global__ void __launch_bounds__(256) k_corrector(NetConst C, NetState* S) {
         if (sec.status) set_status(S, sec.status);
     }
     __syncthreads();
-    if (size < 2) return;
     const Box bo = S->box_cur[g];
     const int x0 = ib.x0 < bo.x0 ? bo.x0 : ib.x0;
     const int y0 = ib.y0 < bo.y0 ? bo.y0 : ib.y0;

@@ -188,4 +188,8 @@ GG_HD void set_status(NetState* S, uint32_t bits) {
 
 GG_HD int contour_capacity(int n) { return 8 * n + 64; }
 
+// Arena offsets are only valid while no allocation overflowed; every kernel
+// that addresses an arena returns early once this bit is set.
+GG_HD bool halted(const NetState* S) { return (S->status & S_ARENA_FULL) != 0; }
+
 }  // namespace gg

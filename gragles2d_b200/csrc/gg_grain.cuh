@@ -265,6 +265,7 @@ __device__ int project_to_boundary(const CPoint* P, int asize, double px, double
         }
     }
     double lam_out = *out_lambda;
+    if (nearest < 0) return 0;  // fewer than two contour points: nothing to project on
     minDist = 1000000.0;
     int next = nearest + 1;
     double ux = P[next].x - P[nearest].x, uy = P[next].y - P[nearest].y;
@@ -306,6 +307,7 @@ __device__ int project_to_boundary(const CPoint* P, int asize, double px, double
 
 // Junction projection of extractBoundaryAndJunctions (src/grainBoundary.cpp:51-61)
 __device__ void project_junctions(const CPoint* P, int n, Junction* js, int jn) {
+    if (n < 2) return;
     double lambda = 0.0;  // one variable for all junctions, as in the reference
     for (int i = 0; i < jn; ++i) {
         int seg = project_to_boundary(P, n, js[i].x, js[i].y, &lambda);

@@ -30,7 +30,7 @@ __device__ __forceinline__ R* phiB_of(NetState* S) {
 template <typename R>
 __global__ void __launch_bounds__(256) k_conv_dft(NetConst C, NetState* S) {
     const int g = blockIdx.x + 1;
-    if (g > C.N || C.state[g] != G_EXISTS) return;
+    if (g > C.N || C.state[g] != G_EXISTS || halted(S)) return;
     const Box bx = S->box_cur[g];
     const int n = box_w(bx);
     if (n <= 0) return;
@@ -185,7 +185,7 @@ constexpr int kListMaxSmem = 128;
 template <typename R>
 __global__ void __launch_bounds__(256) k_compare(NetConst C, NetState* S) {
     const int g = blockIdx.x + 1;
-    if (g > C.N || C.state[g] != G_EXISTS) return;
+    if (g > C.N || C.state[g] != G_EXISTS || halted(S)) return;
     __shared__ Box s_box[kListMaxSmem];
     __shared__ int64_t s_off[kListMaxSmem];
     __shared__ int s_id[kListMaxSmem];
@@ -350,7 +350,7 @@ __device__ bool clear_contour_area(R* phi, const Box& b, const CPoint* P, int n,
 template <typename R>
 __global__ void k_levelset(NetConst C, NetState* S) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    if (g > C.N) return;
+    if (g > C.N || halted(S)) return;
     const int st = C.state[g];
     const Box bc = S->box_cur[g];
     if (st != G_EXISTS) {
@@ -485,7 +485,7 @@ template <typename R>
 __global__ void k_neighbours(NetConst C, NetState* S) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int loop = S->loop;
-    if (g > C.N || C.state[g] != G_EXISTS || C.regular[g] == 0) return;
+    if (g > C.N || C.state[g] != G_EXISTS || C.regular[g] == 0 || halted(S)) return;
     CPoint* P = S->contCur + S->coff_cur[g];
     const int n = S->cn_cur[g];
     const double h = C.h;
@@ -640,7 +640,7 @@ __device__ void redistance_grain(const R* __restrict__ in, const Box bi, R* __re
 template <typename R>
 __global__ void __launch_bounds__(256) k_redistance(NetConst C, NetState* S) {
     const int g = blockIdx.x + 1;
-    if (g > C.N || C.state[g] != G_EXISTS) return;
+    if (g > C.N || C.state[g] != G_EXISTS || halted(S)) return;
     const R* in = phiA_of<R>(S) + S->off_cur[g];
     R* out = phiB_of<R>(S) + S->off_new[g];
     redistance_grain<R>(in, S->box_cur[g], out, S->box_new[g], (R)C.h, (R)C.delta);
@@ -725,7 +725,7 @@ __global__ void __launch_bounds__(1024) k_finalize(NetConst C, NetState* S, int 
 template <typename R>
 __global__ void __launch_bounds__(256) k_init_phi(NetConst C, NetState* S, const int32_t* __restrict__ ids) {
     const int g = blockIdx.x + 1;
-    if (g > C.N || C.state[g] != G_EXISTS) return;
+    if (g > C.N || C.state[g] != G_EXISTS || halted(S)) return;
     const Box bx = S->box_cur[g];
     const int w = box_w(bx);
     const int64_t area = box_area(bx);
@@ -746,7 +746,7 @@ __global__ void __launch_bounds__(256) k_init_phi(NetConst C, NetState* S, const
 template <typename R>
 __global__ void k_init_contour(NetConst C, NetState* S) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    if (g > C.N || C.state[g] != G_EXISTS) return;
+    if (g > C.N || C.state[g] != G_EXISTS || halted(S)) return;
     const Box bx = S->box_cur[g];
     Field<R> f{phiA_of<R>(S) + S->off_cur[g], bx};
     const uint32_t* idl = S->idPrev + S->off_prev[g];
