@@ -1,0 +1,363 @@
+"""Benchmark: grain-updates/s of the batched FP32 level-set step on one B200
+(next to the plain FP64 step on the same GPU and the reference's OpenMP CPU
+path on the host cores).
+
+Workload: 20,000 grains, Voronoi tessellation of uniform seeds (seed 1) on a
+3600 x 3600 grid (mean grain diameter ~25 cells), random uniform SO(3)
+orientations, Read-Shockley boundary energy with a 15 degree cut-off,
+isotropic mobility; seeded synthetic input in the reference's voxelized
+format (its example inputs are not shipped).  A "step" is one level-set
+timestep of the whole network (convolution + corrector, second-order lists,
+comparison, contour / level set, redistancing).  The working set (two FP32
+distance arenas, two IDLocal arenas, contours) is several times the 126 MB
+L2, so no flush is needed between timed steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs N independent replicas (the step does not shard; one process per
+GPU under torchrun) and reports the sum of their throughput over the
+slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "grain-updates/s"
+WORKLOAD = dict(name="voronoi_20000g_3600_rs15", grains=20000, grid=3600, seed=1, iso=0, mobility=0, tpd=0.0)
+SMALL = dict(name="voronoi_1000g_800_iso", grains=1000, grid=800, seed=0, iso=1, mobility=0, tpd=0.0)
+CACHE = os.path.join(tempfile.gettempdir(), "gg_bench_cache")
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "gg_ref")
+
+
+def rank_info():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(
+        os.environ.get("LOCAL_RANK", "0"))
+
+
+def workload_case(w: dict) -> tuple[str, dict]:
+    """Writes (once) the mode-4 input and its parameters.xml; returns the XML path."""
+    from gragles2d_b200 import microstructure as ms
+
+    d = os.path.join(CACHE, w["name"])
+    xml = os.path.join(d, w["name"] + ".xml")
+    if not os.path.exists(xml):
+        micro = ms.voronoi(w["grains"], w["grid"], w["seed"])
+        tmp = d + f".tmp{os.getpid()}"
+        ms.make_case(tmp, w["name"], micro, NumberOfTimesteps=10, IsIsotropicNetwork=w["iso"],
+                     UseMobilityModel=w["mobility"], TriplePointDrag=w["tpd"])
+        try:
+            os.replace(tmp, d)
+        except OSError:
+            shutil.rmtree(tmp, ignore_errors=True)
+    return xml, w
+
+
+def load_inputs(xml: str):
+    """Host buffers of the voxelized input (ids, euler, bbox)."""
+    from gragles2d_b200 import microstructure as ms
+
+    d = os.path.dirname(xml)
+    name = os.path.basename(xml)[:-4]
+    lines = open(os.path.join(d, name + ".uds")).read().splitlines()
+    nn = int(lines[4].split()[1])
+    rows = np.array([l.split() for l in lines[8:]], dtype=np.float64)
+    euler = rows[:, 3:6].copy()
+    bbox = rows[:, 6:11].astype(np.int32)
+    ids = np.fromfile(os.path.join(d, name + ".bin"), dtype="<i4").reshape(nn, nn)
+    return ids, euler, bbox
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                v = [x.strip() for x in out.stdout.strip().split(",")]
+                if len(v) == 7:
+                    self.samples.append(v)
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[3 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def committed_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        return json.load(open(p)).get(kernel)
+    except Exception:
+        return None
+
+
+def stage_bytes(stage: str, s: int, area: int, overlap: int, aniso: bool) -> float:
+    """Algorithmic bytes of one stage over the network (s bytes per field value,
+    u32 IDLocal): convolution reads and writes each box; the corrector reads
+    phi_t, the convolution and IDLocal and writes the convolution; the
+    comparison reads its own and its neighbours' overlapping convolutions and
+    the old IDLocal and writes the compared field and IDLocal; redistancing
+    reads the compared field and writes the new one."""
+    return {
+        "convolution": 2 * s * area,
+        "corrector": (3 * s + 4) * area if aniso else 0,
+        "comparison": s * (2 * area + overlap) + 8 * area,
+        "level_set": s * area,
+        "redistancing": 2 * s * area,
+    }.get(stage, 0)
+
+
+def run_ours(args, rank, world, local_rank):
+    from gragles2d_b200 import gg
+
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+        dist = tdist
+    device = local_rank
+    xml, w = workload_case(WORKLOAD)
+    ids, euler, bbox = load_inputs(xml)
+    K, W = args.steps, args.warmup
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    # ---- e2e through the C ABI from host buffers (batched form) ----
+    barrier()
+    t0 = time.perf_counter()
+    sb = gg.Settings(xml, precision=gg.PRECISION_BATCHED)
+    hb = gg.GrainHandler(sb, device=device)
+    hb.load_voxels(ids, euler, bbox)
+    hb.distanceInitialisation()
+    hb.find_neighbors()
+    stats_bytes = 0
+    for _ in range(W + K):
+        hb.step(1)
+        st = hb.grain_stats()
+        stats_bytes += len(st) * 64
+    t_e2e = time.perf_counter() - t0
+    upd_e2e = hb.grain_updates()
+    areas_b = np.array([s.area if s.state == 1 else np.nan for s in hb.grain_stats()])
+    h2d = ids.nbytes + euler.nbytes + bbox.nbytes
+
+    # ---- device-timed batched steps ----
+    hb.step(W)
+    u0 = hb.grain_updates()
+    barrier()
+    with ClockSampler(device) as clk:
+        ms_b = hb.step(K)
+    barrier()
+    upd_b = hb.grain_updates() - u0
+    # roofline of the dominant stage
+    area, overlap, nex = hb.traffic()
+    prof = hb.profile_steps(2)
+    area2, overlap2, _ = hb.traffic()
+    status_b = hb.status()
+    hb.close()
+
+    # ---- plain FP64 on the same GPU ----
+    sp = gg.Settings(xml, precision=gg.PRECISION_PLAIN)
+    hp = gg.GrainHandler(sp, device=device)
+    hp.load_voxels(ids, euler, bbox)
+    hp.distanceInitialisation()
+    hp.find_neighbors()
+    hp.step(W + K)
+    areas_p = np.array([s.area if s.state == 1 else np.nan for s in hp.grain_stats()])
+    u0p = hp.grain_updates()
+    kp = max(1, min(K, args.plain_steps))
+    ms_p = hp.step(kp)
+    upd_p = hp.grain_updates() - u0p
+    hp.close()
+
+    both = np.isfinite(areas_b) & np.isfinite(areas_p) & (areas_p > 0)
+    area_err = float(np.max(np.abs(areas_b[both] - areas_p[both]) / areas_p[both])) if both.any() else None
+
+    # ---- max over ranks ----
+    t_ms = ms_b
+    if dist:
+        import torch
+
+        t = torch.tensor([ms_b, t_e2e], dtype=torch.float64, device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms, t_e2e = float(t[0]), float(t[1])
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
+
+    value = world * upd_b / (t_ms / 1e3)
+    aniso = not w["iso"]
+    peak, peak_kind = measured_peak_hbm()
+    stage_ms = {k: v / 2 for k, v in prof.items()}
+    ab = {k: stage_bytes(k, 4, (area + area2) // 2, (overlap + overlap2) // 2, aniso) for k in stage_ms}
+    dom = max(stage_ms, key=lambda k: stage_ms[k])
+    dom_bytes = ab.get(dom, 0)
+    achieved = dom_bytes / (stage_ms[dom] / 1e3) / 1e9 if dom_bytes else None
+    kernel_names = {"convolution": "k_conv_sep", "corrector": "k_corrector", "comparison": "k_compare",
+                    "level_set": "k_levelset", "redistancing": "k_redistance"}
+    out = {
+        "metric": METRIC,
+        "value": value,
+        "unit": METRIC,
+        "n_gpus": world,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": t_ms / K,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "20000-grain Voronoi (seed 1) on 3600x3600, Read-Shockley 15 deg, "
+                               "batched FP32 graph-captured step", "grains": w["grains"], "grid": w["grid"],
+                   "l2": "working set larger than L2 (no flush)", "parallelism": f"replicas{world}"},
+        "e2e": {"value": world * upd_e2e / t_e2e, "unit": METRIC, "h2d_bytes_per_step": h2d / (W + K),
+                "d2h_bytes_per_step": stats_bytes / (W + K),
+                "includes": "load from host buffers + distance init + neighbour search + W+K steps with "
+                            "per-step grain-stat reads"},
+        "roofline": {"bound": "hbm", "kernel": kernel_names.get(dom, dom), "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None,
+                     "traffic": committed_traffic(kernel_names.get(dom, dom)),
+                     "algorithmic_bytes_per_launch": dom_bytes, "stage_ms": stage_ms},
+        "plain_fp64": {"value": upd_p / (ms_p / 1e3), "ms_per_step": ms_p / kp, "steps": kp},
+        "batched_vs_plain": (upd_b / (t_ms / 1e3)) / (upd_p / (ms_p / 1e3)),
+        "area_rel_err_max": area_err,
+        "clocks": clk.summary(),
+        "gpu_launches": (9 if aniso else 8) * K,
+        "status": status_b,
+    }
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(xml, args.cpu_steps)
+    return out
+
+
+def cpu_baseline(xml: str, steps: int) -> dict:
+    """The reference's OpenMP path (oracle/_ref/gg_ref) on the host cores, on a
+    bounded sample of the same workload (its first `steps` timesteps)."""
+    if not os.path.exists(REF_BIN):
+        return {"value": None, "unit": METRIC, "cores": os.cpu_count(), "kind": "reference",
+                "sample": "unavailable: oracle/_ref/gg_ref not built"}
+    d = tempfile.mkdtemp(prefix="gg_ref_")
+    src = os.path.dirname(xml)
+    for f in os.listdir(src):
+        os.symlink(os.path.join(src, f), os.path.join(d, f))
+    name = os.path.basename(xml)
+    txt = open(xml).read()
+    import re
+
+    txt = re.sub(r"<NumberOfTimesteps>[^<]*</NumberOfTimesteps>", f"<NumberOfTimesteps> {steps - 1} </NumberOfTimesteps>",
+                 txt)
+    os.remove(os.path.join(d, name))
+    open(os.path.join(d, name), "w").write(txt)
+    env = dict(os.environ)
+    cores = os.cpu_count() or 1
+    env["OMP_NUM_THREADS"] = str(cores)
+    out = subprocess.run([REF_BIN, name, "-", "0", "1"], cwd=d, capture_output=True, text=True, env=env,
+                         timeout=1800)
+    shutil.rmtree(d, ignore_errors=True)
+    info = json.loads(out.stdout.strip().splitlines()[-1])
+    return {"value": info["grain_updates"] / info["loop_s"], "unit": METRIC, "cores": info["threads"],
+            "kind": "reference",
+            "sample": f"first {info['steps']} timesteps of the same workload (reference + shim FFT, "
+                      f"{info['grain_updates']} grain-updates in {info['loop_s']:.2f} s; init excluded)"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    xml, w = workload_case(WORKLOAD)
+    # a bounded sample: the reference needs seconds per step of this workload
+    steps = min(args.warmup + args.steps, args.ref_max_steps)
+    cb = cpu_baseline(xml, steps)
+    if cb["value"] is None:
+        return {"impl": "reference", "unavailable": cb["sample"]}
+    v = cb["value"]
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "20000-grain Voronoi (seed 1) on 3600x3600, Read-Shockley 15 deg",
+                       "grains": w["grains"], "grid": w["grid"]},
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--plain-steps", type=int, default=20)
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-max-steps", type=int, default=6)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank, world, local_rank = rank_info()
+    os.makedirs(CACHE, exist_ok=True)
+    res = run_reference(args, rank, world) if args.impl == "reference" else run_ours(args, rank, world, local_rank)
+    if res is not None:
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -82,6 +82,23 @@ cudaError_t batched_init(const NetConst& C, NetState* dS, const int32_t* d_ids, 
     return cudaGetLastError();
 }
 
+cudaError_t batched_stage_kernel(const NetConst& C, NetState* dS, int which, cudaStream_t s, const LaunchCfg& cfg) {
+    const int gt = cfg.grain_threads;
+    const int gblocks = (C.N + gt - 1) / gt;
+    switch (which) {
+        case 0: k_conv_sep<<<C.N, cfg.conv_threads, conv_sep_smem(C.tmax), s>>>(C, dS); break;
+        case 1: if (!C.isotropic) k_corrector<float><<<C.N, 256, 0, s>>>(C, dS); break;
+        case 2: k_second_order<<<gblocks, gt, 0, s>>>(C, dS); break;
+        case 3: k_compare<float><<<C.N, cfg.compare_threads, 0, s>>>(C, dS); break;
+        case 4: k_levelset<float><<<gblocks, gt, 0, s>>>(C, dS); break;
+        case 5: k_alloc<<<1, 1024, 0, s>>>(C, dS, 1); break;
+        case 6: k_neighbours<float><<<gblocks, gt, 0, s>>>(C, dS); break;
+        case 7: k_redistance<float><<<C.N, cfg.redist_threads, 0, s>>>(C, dS); break;
+        default: k_finalize<<<1, 1024, 0, s>>>(C, dS, 1); break;
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t batched_stages(const NetConst& C, NetState* dS, int stages, cudaStream_t s, const LaunchCfg& cfg) {
     if (C.N <= 0) return cudaSuccess;
     const int gt = cfg.grain_threads;

@@ -176,6 +176,10 @@ struct NetState {
     int32_t live;        // grains not removed (grainhdl::currentNrGrains)
     int32_t pad;
     double max_volume;
+    unsigned long long updates;   // sum over steps of grains alive at step start
+    unsigned long long t_area;    // traffic model scratch (k_traffic)
+    unsigned long long t_overlap;
+    unsigned long long t_exists;
 };
 
 GG_HD void set_status(NetState* S, uint32_t bits) {

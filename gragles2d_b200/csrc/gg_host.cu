@@ -821,6 +821,55 @@ int gg_status(gg_ctx* c, uint32_t* status, int32_t clear) {
     return GG_OK;
 }
 
+int gg_grain_updates(gg_ctx* c, int64_t* updates) {
+    if (!c || !updates) return GG_E_INVALID;
+    if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
+    int rc = refresh_state(c);
+    if (rc) return rc;
+    *updates = (int64_t)c->hS.updates;
+    return GG_OK;
+}
+
+int gg_profile_steps(gg_ctx* c, int32_t loop, int32_t nsteps, double* stage_ms) {
+    if (!c || !stage_ms) return GG_E_INVALID;
+    if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
+    int rc = set_loop(c, loop);
+    if (rc) return rc;
+    cudaEvent_t ev[GG_NSTAGES + 1];
+    for (int k = 0; k <= GG_NSTAGES; ++k) GG_CUDA(c, cudaEventCreate(&ev[k]));
+    const bool plain = c->P.precision == GG_PRECISION_PLAIN;
+    for (int s = 0; s < nsteps; ++s) {
+        GG_CUDA(c, cudaEventRecord(ev[0], c->stream));
+        for (int k = 0; k < GG_NSTAGES; ++k) {
+            GG_CUDA(c, plain ? plain_stage_kernel(c->C, c->dS, k, c->stream, c->cfg)
+                             : batched_stage_kernel(c->C, c->dS, k, c->stream, c->cfg));
+            GG_CUDA(c, cudaEventRecord(ev[k + 1], c->stream));
+        }
+        GG_CUDA(c, cudaEventSynchronize(ev[GG_NSTAGES]));
+        for (int k = 0; k < GG_NSTAGES; ++k) {
+            float ms = 0;
+            GG_CUDA(c, cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+            stage_ms[k] += ms;
+        }
+    }
+    for (int k = 0; k <= GG_NSTAGES; ++k) cudaEventDestroy(ev[k]);
+    return check_status(c);
+}
+
+int gg_traffic(gg_ctx* c, int64_t* sum_area, int64_t* sum_overlap, int32_t* n_exists) {
+    if (!c) return GG_E_INVALID;
+    if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
+    unsigned long long z[3] = {0, 0, 0};
+    GG_CUDA(c, cudaMemcpyAsync(&c->dS->t_area, z, sizeof z, cudaMemcpyHostToDevice, c->stream));
+    GG_CUDA(c, traffic_launch(c->C, c->dS, c->stream));
+    int rc = refresh_state(c);
+    if (rc) return rc;
+    if (sum_area) *sum_area = (int64_t)c->hS.t_area;
+    if (sum_overlap) *sum_overlap = (int64_t)c->hS.t_overlap;
+    if (n_exists) *n_exists = (int32_t)c->hS.t_exists;
+    return GG_OK;
+}
+
 int gg_last_step_ms(gg_ctx* c, double* ms) {
     if (!c || !ms) return GG_E_INVALID;
     *ms = c->last_ms;

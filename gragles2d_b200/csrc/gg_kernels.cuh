@@ -675,6 +675,7 @@ __global__ void __launch_bounds__(1024) k_finalize(NetConst C, NetState* S, int 
         cnt += s_cnt[q];
         mx = fmax(mx, s_max[q]);
     }
+    if (rotate) S->updates += (unsigned long long)S->live;  // grains alive at this step's start
     S->live = cnt;
     S->max_volume = mx;
     if (!rotate) return;
@@ -716,6 +717,23 @@ __global__ void __launch_bounds__(1024) k_finalize(NetConst C, NetState* S, int 
     S->jn_prev = S->jn_cur;
     S->jn_cur = tjn;
     S->loop += 1;
+}
+
+// Traffic model: box areas and comparison-list overlaps of existing grains.
+__global__ void k_traffic(NetConst C, NetState* S) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (g > C.N || C.state[g] != G_EXISTS) return;
+    const Box a = S->box_cur[g];
+    unsigned long long ov = 0;
+    const int n = C.cmp_n[g];
+    for (int k = 0; k < n; ++k) {
+        const Box b = S->box_cur[C.cmp_ids[(int64_t)g * C.kmax + k]];
+        const int x0 = max(a.x0, b.x0), x1 = min(a.x1, b.x1), y0 = max(a.y0, b.y0), y1 = min(a.y1, b.y1);
+        if (x1 > x0 && y1 > y0) ov += (unsigned long long)(x1 - x0) * (unsigned long long)(y1 - y0);
+    }
+    atomicAdd(&S->t_area, (unsigned long long)box_area(a));
+    atomicAdd(&S->t_overlap, ov);
+    atomicAdd(&S->t_exists, 1ull);
 }
 
 // ---------------------------------------------------------------------------

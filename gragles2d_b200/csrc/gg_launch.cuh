@@ -37,5 +37,9 @@ cudaError_t batched_init(const NetConst& C, NetState* dS, const int32_t* d_ids, 
 cudaError_t finalize_only(const NetConst& C, NetState* dS, int rotate, cudaStream_t s);
 cudaError_t swap_phi(NetState* dS, cudaStream_t s);
 cudaError_t find_neighbors_launch(const NetConst& C, NetState* dS, cudaStream_t s);
+cudaError_t traffic_launch(const NetConst& C, NetState* dS, cudaStream_t s);
+// One launch of a single stage kernel (index 0..8 as in GG_NSTAGES order).
+cudaError_t plain_stage_kernel(const NetConst& C, NetState* dS, int which, cudaStream_t s, const LaunchCfg& cfg);
+cudaError_t batched_stage_kernel(const NetConst& C, NetState* dS, int which, cudaStream_t s, const LaunchCfg& cfg);
 
 }  // namespace gg

@@ -39,6 +39,29 @@ cudaError_t plain_init(const NetConst& C, NetState* dS, const int32_t* d_ids, cu
     return cudaGetLastError();
 }
 
+cudaError_t traffic_launch(const NetConst& C, NetState* dS, cudaStream_t s) {
+    const int gt = 128;
+    k_traffic<<<(C.N + gt - 1) / gt, gt, 0, s>>>(C, dS);
+    return cudaGetLastError();
+}
+
+cudaError_t plain_stage_kernel(const NetConst& C, NetState* dS, int which, cudaStream_t s, const LaunchCfg& cfg) {
+    const int gt = cfg.grain_threads;
+    const int gblocks = (C.N + gt - 1) / gt;
+    switch (which) {
+        case 0: k_conv_dft<double><<<C.N, cfg.conv_threads, 0, s>>>(C, dS); break;
+        case 1: if (!C.isotropic) k_corrector<double><<<C.N, 256, 0, s>>>(C, dS); break;
+        case 2: k_second_order<<<gblocks, gt, 0, s>>>(C, dS); break;
+        case 3: k_compare<double><<<C.N, cfg.compare_threads, 0, s>>>(C, dS); break;
+        case 4: k_levelset<double><<<gblocks, gt, 0, s>>>(C, dS); break;
+        case 5: k_alloc<<<1, 1024, 0, s>>>(C, dS, 2); break;
+        case 6: k_neighbours<double><<<gblocks, gt, 0, s>>>(C, dS); break;
+        case 7: k_redistance<double><<<C.N, cfg.redist_threads, 0, s>>>(C, dS); break;
+        default: k_finalize<<<1, 1024, 0, s>>>(C, dS, 1); break;
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t plain_corrector(const NetConst& C, NetState* dS, cudaStream_t s) {
     k_corrector<double><<<C.N, 256, 0, s>>>(C, dS);
     return cudaGetLastError();

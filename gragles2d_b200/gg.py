@@ -28,7 +28,11 @@ EXPORTS = (
     "gg_load_voxel_files", "gg_distance_initialisation", "gg_find_neighbors", "gg_set_neighbours",
     "gg_convolution", "gg_update_second_order_neighbors", "gg_comparison", "gg_level_set", "gg_redistancing",
     "gg_grain_count", "gg_step", "gg_status", "gg_read_grain_stats", "gg_dims", "gg_dump", "gg_last_step_ms",
+    "gg_grain_updates", "gg_profile_steps", "gg_traffic",
 )
+NSTAGES = 9
+STAGE_NAMES = ("convolution", "corrector", "second_order", "comparison", "level_set", "alloc",
+               "volume_energy_neighbours", "redistancing", "end_of_step")
 
 
 class GGError(RuntimeError):
@@ -103,6 +107,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "gg_dims": (I, [V, P(I), P(I), P(D), P(D), P(D)]),
         "gg_dump": (I, [V, ctypes.c_char_p, I, I]),
         "gg_last_step_ms": (I, [V, P(D)]),
+        "gg_grain_updates": (I, [V, P(ctypes.c_int64)]),
+        "gg_profile_steps": (I, [V, I, I, P(D)]),
+        "gg_traffic": (I, [V, P(ctypes.c_int64), P(ctypes.c_int64), P(I)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -281,6 +288,23 @@ class GrainHandler:
     def areas(self) -> np.ndarray:
         st = self.grain_stats()
         return np.array([s.area if s.state == 1 else np.nan for s in st])
+
+    def grain_updates(self) -> int:
+        v = ctypes.c_int64()
+        self._check(self.lib.gg_grain_updates(self.ctx, ctypes.byref(v)))
+        return v.value
+
+    def profile_steps(self, nsteps: int) -> dict:
+        """Runs nsteps stage by stage; returns device ms per stage."""
+        arr = (ctypes.c_double * NSTAGES)()
+        self._check(self.lib.gg_profile_steps(self.ctx, self.loop, nsteps, arr))
+        self.loop += nsteps
+        return dict(zip(STAGE_NAMES, list(arr)))
+
+    def traffic(self) -> tuple[int, int, int]:
+        a, o, n = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int32()
+        self._check(self.lib.gg_traffic(self.ctx, ctypes.byref(a), ctypes.byref(o), ctypes.byref(n)))
+        return a.value, o.value, n.value
 
     def dump(self, path: str, steps_done: int = 0, append: bool = False):
         self._check(self.lib.gg_dump(self.ctx, path.encode(), steps_done, int(append)))

@@ -186,6 +186,23 @@ int gg_dump(gg_ctx* ctx, const char* path, int32_t steps_done, int32_t append);
  * (CUDA events on the context's stream). */
 int gg_last_step_ms(gg_ctx* ctx, double* ms);
 
+/* Sum over completed steps of the grains existing at each step's start
+ * (the grain-updates behind grain-updates/s), counted on the device. */
+int gg_grain_updates(gg_ctx* ctx, int64_t* updates);
+
+/* Runs nsteps whole steps stage by stage with CUDA events between stages
+ * and adds the device milliseconds of each stage to stage_ms[GG_NSTAGES]:
+ * convolution, corrector, second-order lists, comparison, level set,
+ * arena allocation, volume/energy/neighbours, redistancing, end of step
+ * (the reference's stage timers, src/grainhdl.cpp:1146-1154). */
+#define GG_NSTAGES 9
+int gg_profile_steps(gg_ctx* ctx, int32_t loop, int32_t nsteps, double* stage_ms);
+
+/* Algorithmic traffic model of the current network: sum of box areas of
+ * existing grains, sum over grains of the overlap areas with their
+ * comparison-list members, and the number of existing grains. */
+int gg_traffic(gg_ctx* ctx, int64_t* sum_area, int64_t* sum_overlap, int32_t* n_exists);
+
 #ifdef __cplusplus
 }
 #endif

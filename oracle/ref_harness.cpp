@@ -222,10 +222,13 @@ int main(int argc, char** argv) {
     double t_loop = 0.0;
     unsigned long grain_updates = 0;
     int steps = 0;
+    std::vector<double> step_s;
+    std::vector<unsigned> step_grains;
     for (sim->loop = Settings::StartTime; sim->loop <= Settings::StartTime + Settings::NumberOfTimesteps;
          sim->loop++) {
         const double t0 = now_s();
         grain_updates += sim->currentNrGrains;
+        step_grains.push_back(sim->currentNrGrains);
         double overhead = 0;
         sim->gridCoarsement();
         sim->convolution(overhead);
@@ -242,7 +245,8 @@ int main(int argc, char** argv) {
         sim->Realtime += (sim->get_dt() * (Settings::Physical_Domain_Size * Settings::Physical_Domain_Size) /
                           (sim->TimeSlope * Settings::HAGB_Energy * Settings::HAGB_Mobility));
         sim->get_biggestGrainVol();
-        t_loop += now_s() - t0;
+        step_s.push_back(now_s() - t0);
+        t_loop += step_s.back();
         ++steps;
         const bool last = sim->loop == Settings::StartTime + Settings::NumberOfTimesteps;
         const bool brk = sim->currentNrGrains < Settings::BreakupNumber;
@@ -252,7 +256,11 @@ int main(int argc, char** argv) {
     if (w.f) std::fclose(w.f);
     if (quiet) std::cout.rdbuf(saved);
     std::printf("{\"steps\": %d, \"grain_updates\": %lu, \"loop_s\": %.6f, \"init_s\": %.6f, \"threads\": %d, "
-                "\"grains_left\": %u}\n",
+                "\"grains_left\": %u, \"step_s\": [",
                 steps, grain_updates, t_loop, t_init, omp_get_max_threads(), sim->currentNrGrains);
+    for (size_t k = 0; k < step_s.size(); ++k) std::printf("%s%.6f", k ? ", " : "", step_s[k]);
+    std::printf("], \"step_grains\": [");
+    for (size_t k = 0; k < step_grains.size(); ++k) std::printf("%s%u", k ? ", " : "", step_grains[k]);
+    std::printf("]}\n");
     return 0;
 }
