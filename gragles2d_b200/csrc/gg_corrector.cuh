@@ -129,9 +129,26 @@ __device__ __forceinline__ bool within(int left, int right, int totalP, int segm
 }
 
 // ExplicitGrainBoundary::setPointsOnBoundary (src/grainBoundary.cpp:524-559)
+// Iteration bound of a walk along the contour that stops once it has covered
+// `radius`: the reference's loops (which have no bound) end after
+// ceil(radius / perimeter) laps; a zero-length contour would never end.
+__device__ __forceinline__ long lap_guard(const CPoint* P, int size, double h, double radius, uint32_t* status) {
+    double per = 0;
+    for (int i = 0; i < size - 1; ++i) {
+        const double dx = P[i].x - P[i + 1].x, dy = P[i].y - P[i + 1].y;
+        per += sqrt(dx * dx + dy * dy) * h;
+    }
+    if (!(per > 0)) {
+        *status |= S_SECTOR_GUARD;
+        return 2L * size + 8;
+    }
+    const double laps = ceil(radius / per) + 2.0;
+    return (long)(laps * (size + 1)) + 8;
+}
+
 __device__ void set_points_on_boundary(const CPoint* P, int size, const Junction& J0, double h, double csr,
                                        int* left, int* right, uint32_t* status) {
-    const int guard = 4 * size + 8;
+    const long guard = lap_guard(P, size, h, csr, status);
     double dist = 0;
     int l = J0.segment;
     {
@@ -140,12 +157,12 @@ __device__ void set_points_on_boundary(const CPoint* P, int size, const Junction
         dist += sqrt(dx * dx + dy * dy) * h;
     }
     l = periodic(l + 1, size);
-    int it = 0;
+    long it = 0;
     while (dist < csr) {
         dist += seg_len(P, periodic(l + 1, size), l) * h;
         l = periodic(l + 1, size);
         if (++it > guard) {
-            *status |= S_WALK_LIMIT;
+            *status |= S_SECTOR_GUARD;
             break;
         }
     }
@@ -162,7 +179,7 @@ __device__ void set_points_on_boundary(const CPoint* P, int size, const Junction
         dist += seg_len(P, periodic(r - 1, size), r) * h;
         r = periodic(r - 1, size);
         if (++it > guard) {
-            *status |= S_WALK_LIMIT;
+            *status |= S_SECTOR_GUARD;
             break;
         }
     }
@@ -181,7 +198,7 @@ __device__ void build_sectors(const NetConst& C, int g, const CPoint* P, int siz
     if (nj == 0) return;
     const double h = C.h;
     const int real = size - 1;
-    const int guard = 4 * size + 8;
+    const long guard = lap_guard(P, size, h, C.isr > C.csr ? C.isr : C.csr, &S.status);
     auto push_const = [&](int jidx) -> int {
         if (S.nconst >= kMaxConstSectors) {
             S.status |= S_JUNCTION_OVERFLOW;
@@ -251,11 +268,12 @@ __device__ void build_sectors(const NetConst& C, int g, const CPoint* P, int siz
         InterpSector nr;
         {
             double dist = 0;
-            int j = secR.left, it = 0;
+            int j = secR.left;
+            long it = 0;
             for (; dist <= C.isr; j = (j + 1 + real) % real) {
                 dist += seg_len(P, j, (j + 1 + real) % real) * h;
                 if (++it > guard) {
-                    S.status |= S_WALK_LIMIT;
+                    S.status |= S_SECTOR_GUARD;
                     break;
                 }
             }
@@ -269,11 +287,12 @@ __device__ void build_sectors(const NetConst& C, int g, const CPoint* P, int siz
         InterpSector nl;
         {
             double dist = 0;
-            int j = secL.right, it = 0;
+            int j = secL.right;
+            long it = 0;
             for (; dist <= C.isr; j = (j - 1 + real) % real) {
                 dist += seg_len(P, j, (j - 1 + real) % real) * h;
                 if (++it > guard) {
-                    S.status |= S_WALK_LIMIT;
+                    S.status |= S_SECTOR_GUARD;
                     break;
                 }
             }
@@ -288,8 +307,8 @@ __device__ void build_sectors(const NetConst& C, int g, const CPoint* P, int siz
             int it = 0;
             for (int j = nr.right; j != periodic(nr.left + 1, size); j = periodic(j + 1, size)) {
                 if (j == nl.left || j == nl.right) merged = true;
-                if (++it > guard) {
-                    S.status |= S_WALK_LIMIT;
+                if (++it > size + 1) {
+                    S.status |= S_SECTOR_GUARD;
                     break;
                 }
             }
@@ -305,8 +324,8 @@ __device__ void build_sectors(const NetConst& C, int g, const CPoint* P, int siz
             int it = 0;
             for (int j = r.right; j != r.left; j = (j + 1 + real) % real) {
                 dist += seg_len(P, j, (j - 1 + real) % real) * h;
-                if (++it > guard) {
-                    S.status |= S_WALK_LIMIT;
+                if (++it > size + 1) {
+                    S.status |= S_SECTOR_GUARD;
                     break;
                 }
             }

@@ -38,7 +38,9 @@ enum : uint32_t {
     S_TABLE_RANGE = 1u << 5,
     S_NEIGHBOUR_OVERFLOW = 1u << 6,
     S_NAN = 1u << 7,
-    S_INDEX = 1u << 8
+    S_INDEX = 1u << 8,
+    S_SECTOR_GUARD = 1u << 9,   // a sector walk met a zero-length contour
+    S_RETRY_LIMIT = 1u << 10    // more than 64 contour re-extractions
 };
 
 struct Box {

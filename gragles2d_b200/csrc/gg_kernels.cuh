@@ -380,7 +380,7 @@ __global__ void k_levelset(NetConst C, NetState* S) {
                 project_junctions(o.pts, o.n, o.js, o.jn);
                 newVolume = contour_volume(o.pts, o.n, C.h);
                 if (++tries > 64) {
-                    o.status |= S_WALK_LIMIT;
+                    o.status |= S_RETRY_LIMIT;
                     break;
                 }
             } while (!motion_regular(old_len, o.n, C.volume[g], newVolume, C.dt, &irregular));

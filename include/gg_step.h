@@ -54,7 +54,10 @@ enum {
     GG_S_WALK_LIMIT = 1 << 4,
     GG_S_TABLE_RANGE = 1 << 5,
     GG_S_NEIGHBOUR_OVERFLOW = 1 << 6,
-    GG_S_NAN = 1 << 7
+    GG_S_NAN = 1 << 7,
+    GG_S_INDEX = 1 << 8,         /* an access the reference would have faulted on */
+    GG_S_SECTOR_GUARD = 1 << 9,  /* a sector walk met a zero-length contour */
+    GG_S_RETRY_LIMIT = 1 << 10   /* more than 64 contour re-extractions */
 };
 
 /*
