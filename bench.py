@@ -194,7 +194,9 @@ def run_ours(args, rank, world, local_rank):
         stats_bytes += len(st) * 64
     t_e2e = time.perf_counter() - t0
     upd_e2e = hb.grain_updates()
-    areas_b = np.array([s.area if s.state == 1 else np.nan for s in hb.grain_stats()])
+    st_b = hb.grain_stats()
+    areas_b = np.array([s.area if s.state == 1 else np.nan for s in st_b])
+    reg_b = np.array([s.motion_regular for s in st_b])
     h2d = ids.nbytes + euler.nbytes + bbox.nbytes
 
     # ---- device-timed batched steps ----
@@ -219,7 +221,9 @@ def run_ours(args, rank, world, local_rank):
     hp.distanceInitialisation()
     hp.find_neighbors()
     hp.step(W + K)
-    areas_p = np.array([s.area if s.state == 1 else np.nan for s in hp.grain_stats()])
+    st_p = hp.grain_stats()
+    areas_p = np.array([s.area if s.state == 1 else np.nan for s in st_p])
+    reg_p = np.array([s.motion_regular for s in st_p])
     u0p = hp.grain_updates()
     kp = max(1, min(K, args.plain_steps))
     ms_p = hp.step(kp)
@@ -227,7 +231,18 @@ def run_ours(args, rank, world, local_rank):
     hp.close()
 
     both = np.isfinite(areas_b) & np.isfinite(areas_p) & (areas_p > 0)
-    area_err = float(np.max(np.abs(areas_b[both] - areas_p[both]) / areas_p[both])) if both.any() else None
+    rel = np.abs(areas_b - areas_p) / np.where(areas_p > 0, areas_p, 1.0)
+    area_err = float(np.max(rel[both])) if both.any() else None
+    px = 1.0 / (w["grid"] ** 2)  # area of one grid cell in domain units
+    worst = [int(i) for i in np.argsort(np.where(both, rel, -1))[::-1][:5]]
+    area_diag = {"grains_compared": int(both.sum()),
+                 "alive_only_plain": int((np.isfinite(areas_p) & ~np.isfinite(areas_b)).sum()),
+                 "alive_only_batched": int((np.isfinite(areas_b) & ~np.isfinite(areas_p)).sum()),
+                 "p50": float(np.median(rel[both])), "p99": float(np.quantile(rel[both], 0.99)),
+                 "over_1e-3": int((rel[both] > 1e-3).sum()),
+                 "worst": [{"id": i + 1, "area_px_plain": float(areas_p[i] / px),
+                            "area_px_batched": float(areas_b[i] / px), "rel": float(rel[i]),
+                            "regular_plain": int(reg_p[i]), "regular_batched": int(reg_b[i])} for i in worst]}
 
     # ---- max over ranks ----
     t_ms = ms_b
@@ -280,6 +295,7 @@ def run_ours(args, rank, world, local_rank):
         "plain_fp64": {"value": upd_p / (ms_p / 1e3), "ms_per_step": ms_p / kp, "steps": kp},
         "batched_vs_plain": (upd_b / (t_ms / 1e3)) / (upd_p / (ms_p / 1e3)),
         "area_rel_err_max": area_err,
+        "area_err_detail": area_diag,
         "clocks": clk.summary(),
         "gpu_launches": (9 if aniso else 8) * K,
         "status": status_b,

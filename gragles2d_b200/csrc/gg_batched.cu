@@ -7,13 +7,13 @@
 
 namespace gg {
 
-constexpr int kSepSmemMaxN = 110;  // 2 n^2 + n floats of shared memory
+constexpr int kSepSmemMaxN = 64;  // 2 n^2 + n floats of shared memory (larger boxes stage in global scratch)
 
 // Gaussian convolution as a separable circular convolution in real space:
 // out = K X K^T with K[r][r'] = k_n[(r - r') mod n], where k_n is the real
 // kernel whose DFT is the reference's Gaussian multiplier
 // (src/box.cpp:674-687, G(i2, j2) = g(i2) g(j2) / n^2).  One CTA per grain;
-// the box and the intermediate stay in shared memory when n <= 110.
+// the box and the intermediate stay in shared memory when n <= 64.
 __global__ void __launch_bounds__(256) k_conv_sep(NetConst C, NetState* S) {
     extern __shared__ float sm[];
     const int g = blockIdx.x + 1;
@@ -62,6 +62,169 @@ __global__ void __launch_bounds__(256) k_conv_sep(NetConst C, NetState* S) {
     }
 }
 
+// Batched-form corrector: same sectors and weights as k_corrector, with the
+// previous contour staged in shared memory (FP32 coordinates), junction
+// weights computed one thread per junction, and the per-pixel projection in
+// FP32.
+constexpr int kCorrMaxPts = 4096;
+
+__device__ __forceinline__ int project_f(const float2* P, int asize, float px, float py, float* out_lambda) {
+    float minDist = 1e30f;
+    int nearest = -1;
+    for (int k = 0; k < asize - 1; k++) {
+        const float dx = px - P[k].x, dy = py - P[k].y;
+        const float d = dx * dx + dy * dy;
+        if (d < minDist) {
+            nearest = k;
+            minDist = d;
+        }
+    }
+    if (nearest < 0) return 0;
+    float lam_out = 0.f;
+    int seg = nearest;
+    minDist = 1e30f;
+    {
+        const int next = nearest + 1;
+        const float ux = P[next].x - P[nearest].x, uy = P[next].y - P[nearest].y;
+        float lambda = ((px - P[nearest].x) * ux + (py - P[nearest].y) * uy) / (ux * ux + uy * uy);
+        float d;
+        if (lambda < 0) {
+            const float dx = px - P[nearest].x, dy = py - P[nearest].y;
+            d = dx * dx + dy * dy;
+        } else if (lambda > 1) {
+            const float dx = P[next].x - px, dy = P[next].y - py;
+            d = dx * dx + dy * dy;
+        } else {
+            const float dx = px - (P[nearest].x + ux * lambda), dy = py - (P[nearest].y + uy * lambda);
+            d = dx * dx + dy * dy;
+        }
+        if (d < minDist) {
+            seg = nearest;
+            minDist = d;
+            lam_out = lambda;
+        }
+    }
+    int nb = nearest == 0 ? asize - 1 : nearest;
+    {
+        const int prev = nb - 1;
+        const float ux = P[nb].x - P[prev].x, uy = P[nb].y - P[prev].y;
+        float lambda = ((px - P[prev].x) * ux + (py - P[prev].y) * uy) / (ux * ux + uy * uy);
+        float d;
+        if (lambda < 0) {
+            const float dx = px - P[prev].x, dy = py - P[prev].y;
+            d = dx * dx + dy * dy;
+        } else if (lambda > 1) {
+            const float dx = P[nb].x - px, dy = P[nb].y - py;
+            d = dx * dx + dy * dy;
+        } else {
+            const float dx = px - (P[prev].x + ux * lambda), dy = py - (P[prev].y + uy * lambda);
+            d = dx * dx + dy * dy;
+        }
+        if (d < minDist) {
+            seg = prev;
+            lam_out = lambda;
+        }
+    }
+    *out_lambda = fminf(fmaxf(lam_out, 0.f), 1.f);
+    return seg;
+}
+
+__global__ void __launch_bounds__(256) k_corrector_f(NetConst C, NetState* S) {
+    const int g = blockIdx.x + 1;
+    if (g > C.N || C.state[g] != G_EXISTS || C.regular[g] == 0 || S->loop == 0 || halted(S)) return;
+    __shared__ SectorSet sec;
+    __shared__ float2 sp[kCorrMaxPts];
+    __shared__ double jw[64];
+    __shared__ uint32_t s_st;
+    const CPoint* P = S->contPrev + S->coff_prev[g];
+    const int size = S->cn_prev[g];
+    if (size < 2) return;
+    const Box ib = S->box_prev[g];
+    const uint32_t* idl = S->idPrev + S->off_prev[g];
+    const Junction* J = S->jPrev + (int64_t)g * C.jmax;
+    const int nj = min(S->jn_prev[g], 64);
+    const bool staged = size <= kCorrMaxPts;
+    if (threadIdx.x == 0) s_st = 0;
+    __syncthreads();
+    if (staged)
+        for (int k = threadIdx.x; k < size; k += blockDim.x) sp[k] = make_float2((float)P[k].x, (float)P[k].y);
+    if ((int)threadIdx.x < nj) {
+        uint32_t st = 0;
+        jw[threadIdx.x] = junction_weight(C, J[threadIdx.x], g, &st);
+        if (st) atomicOr(&s_st, st);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        build_sectors(C, g, P, size, J, nj, idl, ib, sec, jw);
+        if (sec.status | s_st) set_status(S, sec.status | s_st);
+    }
+    __syncthreads();
+    const Box bo = S->box_cur[g];
+    const int x0 = ib.x0 < bo.x0 ? bo.x0 : ib.x0;
+    const int y0 = ib.y0 < bo.y0 ? bo.y0 : ib.y0;
+    const int x1 = ib.x1 > bo.x1 ? bo.x1 : ib.x1;
+    const int y1 = ib.y1 > bo.y1 ? bo.y1 : ib.y1;
+    if (x1 <= x0 || y1 <= y0) return;
+    const int w = x1 - x0;
+    const int cnt = w * (y1 - y0);
+    const float* in = reinterpret_cast<const float*>(S->phiA) + S->off_cur[g];
+    float* out = reinterpret_cast<float*>(S->phiB) + S->off_cur[g];
+    const int wo = box_w(bo);
+    const float delta = (float)C.delta;
+    const int real = size - 1;
+    uint32_t st = 0;
+    for (int p = threadIdx.x; p < cnt; p += blockDim.x) {
+        const int i = y0 + p / w, j = x0 + p % w;
+        const int k = (i - bo.y0) * wo + (j - bo.x0);
+        const float val = in[k];
+        if (!(val > -delta)) {
+            out[k] = -delta;
+            continue;
+        }
+        float lambda = 0.f;
+        int segment;
+        if (staged) {
+            segment = project_f(sp, size, (float)j, (float)i, &lambda);
+        } else {
+            double dl = 0;
+            segment = project_to_boundary(P, size, (double)j, (double)i, &dl);
+            lambda = (float)dl;
+        }
+        double weight = -1;
+        for (int q = 0; q < sec.nconst && weight < 0; q++)
+            if (within(sec.cs[q].left, sec.cs[q].right, real, segment)) weight = sec.cs[q].weight;
+        for (int q = 0; q < sec.ninterp && weight < 0; q++) {
+            const InterpSector& s = sec.is[q];
+            if (!within(s.left, s.right, real, segment)) continue;
+            double interpolator = 0;
+            int kk = s.right, it = 0;
+            for (; kk != segment; kk = (kk + 1 + real) % real) {
+                interpolator += seg_len(P, kk + 1, kk) * C.h;
+                if (++it > size) break;
+            }
+            const int kn = (kk + 1 + real) % real;
+            const double ax = (P[kn].x - P[kk].x) * lambda, ay = (P[kn].y - P[kk].y) * lambda;
+            interpolator += sqrt(ax * ax + ay * ay);
+            interpolator /= s.length;
+            interpolator = fmin(fmax(interpolator, 0.0), 1.0);
+            if (s.lb >= 0 && s.rb >= 0) {
+                const double isr = C.isr;
+                const double quot = (s.length > 2 * isr ? 2 * isr : s.length);
+                const double amplitude =
+                    (s.boundary_w - (s.left_w + s.right_w) / 2) / (2 * isr) * quot + (s.left_w + s.right_w) / 2;
+                const double a0 = 2 * s.right_w, a1 = -4 * amplitude, a2 = 2 * s.left_w;
+                const double A = a0 + a1 + a2, B = -(a0 * 1.5 + a1 + a2 * 0.5), Cc = a0 * 0.5;
+                weight = A * interpolator * interpolator + B * interpolator + Cc;
+            } else {
+                weight = interpolator * s.left_w + (1 - interpolator) * s.right_w;
+            }
+        }
+        if (weight < 0) weight = gb_weight_at(C, g, idl, ib, i, j, &st);
+        out[k] = val + (out[k] - val) * (float)weight;
+    }
+    if (st) set_status(S, st);
+}
+
 size_t conv_sep_smem(int tmax) {
     const int n = tmax < kSepSmemMaxN ? tmax : kSepSmemMaxN;
     return sizeof(float) * (size_t)(2 * n * n + n);
@@ -87,7 +250,7 @@ cudaError_t batched_stage_kernel(const NetConst& C, NetState* dS, int which, cud
     const int gblocks = (C.N + gt - 1) / gt;
     switch (which) {
         case 0: k_conv_sep<<<C.N, cfg.conv_threads, conv_sep_smem(C.tmax), s>>>(C, dS); break;
-        case 1: if (!C.isotropic) k_corrector<float><<<C.N, 256, 0, s>>>(C, dS); break;
+        case 1: if (!C.isotropic) k_corrector_f<<<C.N, 256, 0, s>>>(C, dS); break;
         case 2: k_second_order<<<gblocks, gt, 0, s>>>(C, dS); break;
         case 3: k_compare<float><<<C.N, cfg.compare_threads, 0, s>>>(C, dS); break;
         case 4: k_levelset<float><<<gblocks, gt, 0, s>>>(C, dS); break;
@@ -105,7 +268,7 @@ cudaError_t batched_stages(const NetConst& C, NetState* dS, int stages, cudaStre
     const int gblocks = (C.N + gt - 1) / gt;
     if (stages & ST_CONV) {
         k_conv_sep<<<C.N, cfg.conv_threads, conv_sep_smem(C.tmax), s>>>(C, dS);
-        if (!C.isotropic) k_corrector<float><<<C.N, 256, 0, s>>>(C, dS);
+        if (!C.isotropic) k_corrector_f<<<C.N, 256, 0, s>>>(C, dS);
     }
     if (stages & ST_SECOND) k_second_order<<<gblocks, gt, 0, s>>>(C, dS);
     if (stages & ST_COMPARE) k_compare<float><<<C.N, cfg.compare_threads, 0, s>>>(C, dS);

@@ -191,7 +191,7 @@ __device__ void set_points_on_boundary(const CPoint* P, int size, const Junction
 // plus the per-sector weights of ContourSector::getWeight
 // (src/contourSector.cpp:200-272) that do not depend on the pixel.
 __device__ void build_sectors(const NetConst& C, int g, const CPoint* P, int size, const Junction* J, int nj,
-                              const uint32_t* idl, const Box& ib, SectorSet& S) {
+                              const uint32_t* idl, const Box& ib, SectorSet& S, const double* jw_in = nullptr) {
     S.nconst = 0;
     S.ninterp = 0;
     S.status = 0;
@@ -251,8 +251,12 @@ __device__ void build_sectors(const NetConst& C, int g, const CPoint* P, int siz
         }
     }
     // constant-sector weights: mean of junction weights in list order
-    double jw[64];
-    for (int q = 0; q < nj && q < 64; ++q) jw[q] = junction_weight(C, J[q], g, &S.status);
+    double jw_local[64];
+    const double* jw = jw_in;
+    if (!jw) {
+        for (int q = 0; q < nj && q < 64; ++q) jw_local[q] = junction_weight(C, J[q], g, &S.status);
+        jw = jw_local;
+    }
     for (int s = 0; s < S.nconst; ++s) {
         double w = 0;
         for (int q = 0; q < S.cs[s].nj; ++q) w += jw[S.cs[s].js[q] < 64 ? S.cs[s].js[q] : 63];
