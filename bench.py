@@ -355,6 +355,26 @@ def run_reference(args, rank, world):
             "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+PROFILE_CASE = dict(name="voronoi_5000g_1800_rs15", grains=5000, grid=1800, seed=4, iso=0, mobility=0, tpd=0.0)
+
+
+def run_profile_case(args, local_rank):
+    """Small case for ncu captures: 5,000 grains on 1800^2 (Read-Shockley),
+    batched form, W graph-captured steps then 2 steps launched stage by stage."""
+    from gragles2d_b200 import gg
+
+    xml, _ = workload_case(PROFILE_CASE)
+    prec = gg.PRECISION_PLAIN if args.profile_plain else gg.PRECISION_BATCHED
+    h = gg.GrainHandler(gg.Settings(xml, precision=prec), device=local_rank)
+    h.load_voxel_files()
+    h.distanceInitialisation()
+    h.find_neighbors()
+    h.step(args.warmup)
+    prof = h.profile_steps(2)
+    print(json.dumps({"profile_case": PROFILE_CASE["name"], "stage_ms": prof, "status": h.status()}), flush=True)
+    h.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -365,11 +385,16 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-max-steps", type=int, default=6)
+    ap.add_argument("--profile-case", action="store_true", help="small stage-by-stage run for ncu captures")
+    ap.add_argument("--profile-plain", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     rank, world, local_rank = rank_info()
     os.makedirs(CACHE, exist_ok=True)
+    if args.profile_case:
+        run_profile_case(args, local_rank)
+        return
     res = run_reference(args, rank, world) if args.impl == "reference" else run_ours(args, rank, world, local_rank)
     if res is not None:
         print(json.dumps(res), flush=True)

@@ -190,10 +190,14 @@ __global__ void __launch_bounds__(256) k_corrector_f(NetConst C, NetState* S) {
             segment = project_to_boundary(P, size, (double)j, (double)i, &dl);
             lambda = (float)dl;
         }
-        double weight = -1;
-        for (int q = 0; q < sec.nconst && weight < 0; q++)
-            if (within(sec.cs[q].left, sec.cs[q].right, real, segment)) weight = sec.cs[q].weight;
-        for (int q = 0; q < sec.ninterp && weight < 0; q++) {
+        double weight = 0;
+        bool found = false;
+        for (int q = 0; q < sec.nconst && !found; q++)
+            if (within(sec.cs[q].left, sec.cs[q].right, real, segment)) {
+                weight = sec.cs[q].weight;
+                found = true;
+            }
+        for (int q = 0; q < sec.ninterp && !found; q++) {
             const InterpSector& s = sec.is[q];
             if (!within(s.left, s.right, real, segment)) continue;
             double interpolator = 0;
@@ -218,8 +222,9 @@ __global__ void __launch_bounds__(256) k_corrector_f(NetConst C, NetState* S) {
             } else {
                 weight = interpolator * s.left_w + (1 - interpolator) * s.right_w;
             }
+            found = true;
         }
-        if (weight < 0) weight = gb_weight_at(C, g, idl, ib, i, j, &st);
+        if (!found) weight = gb_weight_at(C, g, idl, ib, i, j, &st);
         out[k] = val + (out[k] - val) * (float)weight;
     }
     if (st) set_status(S, st);
