@@ -136,29 +136,17 @@ __global__ void __launch_bounds__(256) k_corrector_f(NetConst C, NetState* S) {
     __shared__ float2 sp[kCorrMaxPts];
     __shared__ double jw[64];
     __shared__ uint32_t s_st;
+    __shared__ double s_per;
     const CPoint* P = S->contPrev + S->coff_prev[g];
     const int size = S->cn_prev[g];
     if (size < 2) return;
+    double* seg = S->segPrev + S->coff_prev[g];
     const Box ib = S->box_prev[g];
     const uint32_t* idl = S->idPrev + S->off_prev[g];
-    const Junction* J = S->jPrev + (int64_t)g * C.jmax;
-    const int nj = min(S->jn_prev[g], 64);
     const bool staged = size <= kCorrMaxPts;
-    if (threadIdx.x == 0) s_st = 0;
-    __syncthreads();
     if (staged)
         for (int k = threadIdx.x; k < size; k += blockDim.x) sp[k] = make_float2((float)P[k].x, (float)P[k].y);
-    if ((int)threadIdx.x < nj) {
-        uint32_t st = 0;
-        jw[threadIdx.x] = junction_weight(C, J[threadIdx.x], g, &st);
-        if (st) atomicOr(&s_st, st);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        build_sectors(C, g, P, size, J, nj, idl, ib, sec, jw);
-        if (sec.status | s_st) set_status(S, sec.status | s_st);
-    }
-    __syncthreads();
+    prepare_sectors(C, S, g, P, size, seg, sec, jw, &s_st, &s_per);
     const Box bo = S->box_cur[g];
     const int x0 = ib.x0 < bo.x0 ? bo.x0 : ib.x0;
     const int y0 = ib.y0 < bo.y0 ? bo.y0 : ib.y0;
@@ -203,7 +191,7 @@ __global__ void __launch_bounds__(256) k_corrector_f(NetConst C, NetState* S) {
             double interpolator = 0;
             int kk = s.right, it = 0;
             for (; kk != segment; kk = (kk + 1 + real) % real) {
-                interpolator += seg_len(P, kk + 1, kk) * C.h;
+                interpolator += seg[kk];
                 if (++it > size) break;
             }
             const int kn = (kk + 1 + real) % real;

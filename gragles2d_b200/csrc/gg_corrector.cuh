@@ -128,27 +128,23 @@ __device__ __forceinline__ bool within(int left, int right, int totalP, int segm
     return segment >= right && segment <= left;
 }
 
-// ExplicitGrainBoundary::setPointsOnBoundary (src/grainBoundary.cpp:524-559)
 // Iteration bound of a walk along the contour that stops once it has covered
 // `radius`: the reference's loops (which have no bound) end after
 // ceil(radius / perimeter) laps; a zero-length contour would never end.
-__device__ __forceinline__ long lap_guard(const CPoint* P, int size, double h, double radius, uint32_t* status) {
-    double per = 0;
-    for (int i = 0; i < size - 1; ++i) {
-        const double dx = P[i].x - P[i + 1].x, dy = P[i].y - P[i + 1].y;
-        per += sqrt(dx * dx + dy * dy) * h;
-    }
-    if (!(per > 0)) {
+__device__ __forceinline__ long lap_guard(double perimeter, int size, double radius, uint32_t* status) {
+    if (!(perimeter > 0)) {
         *status |= S_SECTOR_GUARD;
         return 2L * size + 8;
     }
-    const double laps = ceil(radius / per) + 2.0;
+    const double laps = ceil(radius / perimeter) + 2.0;
     return (long)(laps * (size + 1)) + 8;
 }
 
-__device__ void set_points_on_boundary(const CPoint* P, int size, const Junction& J0, double h, double csr,
-                                       int* left, int* right, uint32_t* status) {
-    const long guard = lap_guard(P, size, h, csr, status);
+// ExplicitGrainBoundary::setPointsOnBoundary (src/grainBoundary.cpp:524-559).
+// seg[k] = |P[k+1] - P[k]| h, the term the reference recomputes at every step
+// of its walks (same expression, so the sums are bit-identical).
+__device__ void set_points_on_boundary(const CPoint* P, const double* seg, int size, const Junction& J0, double h,
+                                       double csr, long guard, int* left, int* right, uint32_t* status) {
     double dist = 0;
     int l = J0.segment;
     {
@@ -159,7 +155,7 @@ __device__ void set_points_on_boundary(const CPoint* P, int size, const Junction
     l = periodic(l + 1, size);
     long it = 0;
     while (dist < csr) {
-        dist += seg_len(P, periodic(l + 1, size), l) * h;
+        dist += seg[l];
         l = periodic(l + 1, size);
         if (++it > guard) {
             *status |= S_SECTOR_GUARD;
@@ -176,7 +172,7 @@ __device__ void set_points_on_boundary(const CPoint* P, int size, const Junction
     r = periodic(r, size);
     it = 0;
     while (dist < csr) {
-        dist += seg_len(P, periodic(r - 1, size), r) * h;
+        dist += seg[periodic(r - 1, size)];
         r = periodic(r - 1, size);
         if (++it > guard) {
             *status |= S_SECTOR_GUARD;
@@ -190,15 +186,16 @@ __device__ void set_points_on_boundary(const CPoint* P, int size, const Junction
 // ExplicitGrainBoundary::buildBoundarySectors (src/grainBoundary.cpp:233-342)
 // plus the per-sector weights of ContourSector::getWeight
 // (src/contourSector.cpp:200-272) that do not depend on the pixel.
-__device__ void build_sectors(const NetConst& C, int g, const CPoint* P, int size, const Junction* J, int nj,
-                              const uint32_t* idl, const Box& ib, SectorSet& S, const double* jw_in = nullptr) {
+__device__ void build_sectors(const NetConst& C, int g, const CPoint* P, const double* seg, double perimeter, int size,
+                              const Junction* J, int nj, const uint32_t* idl, const Box& ib, SectorSet& S,
+                              const double* jw) {
     S.nconst = 0;
     S.ninterp = 0;
     S.status = 0;
     if (nj == 0) return;
     const double h = C.h;
     const int real = size - 1;
-    const long guard = lap_guard(P, size, h, C.isr > C.csr ? C.isr : C.csr, &S.status);
+    const long guard = lap_guard(perimeter, size, C.isr > C.csr ? C.isr : C.csr, &S.status);
     auto push_const = [&](int jidx) -> int {
         if (S.nconst >= kMaxConstSectors) {
             S.status |= S_JUNCTION_OVERFLOW;
@@ -207,7 +204,7 @@ __device__ void build_sectors(const NetConst& C, int g, const CPoint* P, int siz
         ConstSector& c = S.cs[S.nconst];
         c.nj = 1;
         c.js[0] = jidx;
-        set_points_on_boundary(P, size, J[jidx], h, C.csr, &c.left, &c.right, &S.status);
+        set_points_on_boundary(P, seg, size, J[jidx], h, C.csr, guard, &c.left, &c.right, &S.status);
         return S.nconst++;
     };
     auto merge = [&](ConstSector& c, int jidx) {
@@ -220,7 +217,7 @@ __device__ void build_sectors(const NetConst& C, int g, const CPoint* P, int siz
     int cb = 0;
     for (int i = 1; i < nj; i++) {
         int cl, cr;  // current sector's contour points
-        set_points_on_boundary(P, size, J[i], h, C.csr, &cl, &cr, &S.status);
+        set_points_on_boundary(P, seg, size, J[i], h, C.csr, guard, &cl, &cr, &S.status);
         if (within(S.cs[cb].left, S.cs[cb].right, real, cr)) {
             merge(S.cs[cb], i);
             S.cs[cb].left = cl;
@@ -251,12 +248,6 @@ __device__ void build_sectors(const NetConst& C, int g, const CPoint* P, int siz
         }
     }
     // constant-sector weights: mean of junction weights in list order
-    double jw_local[64];
-    const double* jw = jw_in;
-    if (!jw) {
-        for (int q = 0; q < nj && q < 64; ++q) jw_local[q] = junction_weight(C, J[q], g, &S.status);
-        jw = jw_local;
-    }
     for (int s = 0; s < S.nconst; ++s) {
         double w = 0;
         for (int q = 0; q < S.cs[s].nj; ++q) w += jw[S.cs[s].js[q] < 64 ? S.cs[s].js[q] : 63];
@@ -275,7 +266,7 @@ __device__ void build_sectors(const NetConst& C, int g, const CPoint* P, int siz
             int j = secR.left;
             long it = 0;
             for (; dist <= C.isr; j = (j + 1 + real) % real) {
-                dist += seg_len(P, j, (j + 1 + real) % real) * h;
+                dist += seg[j];
                 if (++it > guard) {
                     S.status |= S_SECTOR_GUARD;
                     break;
@@ -294,7 +285,7 @@ __device__ void build_sectors(const NetConst& C, int g, const CPoint* P, int siz
             int j = secL.right;
             long it = 0;
             for (; dist <= C.isr; j = (j - 1 + real) % real) {
-                dist += seg_len(P, j, (j - 1 + real) % real) * h;
+                dist += seg[(j - 1 + real) % real];
                 if (++it > guard) {
                     S.status |= S_SECTOR_GUARD;
                     break;
@@ -327,7 +318,7 @@ __device__ void build_sectors(const NetConst& C, int g, const CPoint* P, int siz
             double dist = 0;
             int it = 0;
             for (int j = r.right; j != r.left; j = (j + 1 + real) % real) {
-                dist += seg_len(P, j, (j - 1 + real) % real) * h;
+                dist += seg[(j - 1 + real) % real];
                 if (++it > size + 1) {
                     S.status |= S_SECTOR_GUARD;
                     break;
@@ -368,9 +359,9 @@ __device__ void build_sectors(const NetConst& C, int g, const CPoint* P, int siz
 }
 
 // ExplicitGrainBoundary::getWeight (src/grainBoundary.cpp:344-363) for one pixel.
-__device__ __forceinline__ double pixel_weight(const NetConst& C, int g, const CPoint* P, int size,
-                                               const SectorSet& S, const uint32_t* idl, const Box& ib, int i, int j,
-                                               uint32_t* status) {
+__device__ __forceinline__ double pixel_weight(const NetConst& C, int g, const CPoint* P, const double* seg,
+                                               int size, const SectorSet& S, const uint32_t* idl, const Box& ib,
+                                               int i, int j, uint32_t* status) {
     double lambda = 0.0;
     const int segment = project_to_boundary(P, size, (double)j, (double)i, &lambda);
     const int real = size - 1;
@@ -382,7 +373,7 @@ __device__ __forceinline__ double pixel_weight(const NetConst& C, int g, const C
         double interpolator = 0;
         int k = s.right, it = 0;
         for (; k != segment; k = (k + 1 + real) % real) {
-            interpolator += seg_len(P, k + 1, k) * C.h;
+            interpolator += seg[k];
             if (++it > size) break;
         }
         const int kn = (k + 1 + real) % real;
@@ -409,21 +400,51 @@ __device__ __forceinline__ double pixel_weight(const NetConst& C, int g, const C
     return gb_weight_at(C, g, idl, ib, i, j, status);
 }
 
+// Per-grain preparation shared by both correctors: segment lengths (into
+// the seg scratch, one thread per segment), junction weights (one thread per
+// junction), perimeter, then the sequential sector build by thread 0.
+__device__ void prepare_sectors(const NetConst& C, NetState* S, int g, const CPoint* P, int size, double* seg,
+                                SectorSet& sec, double* jw, uint32_t* s_st, double* s_per) {
+    const Box ib = S->box_prev[g];
+    const uint32_t* idl = S->idPrev + S->off_prev[g];
+    const Junction* J = S->jPrev + (int64_t)g * C.jmax;
+    const int nj = min(S->jn_prev[g], 64);
+    if (threadIdx.x == 0) *s_st = 0;
+    for (int k = threadIdx.x; k < size - 1; k += blockDim.x) {
+        const double dx = P[k + 1].x - P[k].x, dy = P[k + 1].y - P[k].y;
+        seg[k] = sqrt(dx * dx + dy * dy) * C.h;
+    }
+    if ((int)threadIdx.x < nj) {
+        uint32_t st = 0;
+        jw[threadIdx.x] = junction_weight(C, J[threadIdx.x], g, &st);
+        if (st) atomicOr(s_st, st);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double per = 0;
+        for (int k = 0; k < size - 1; ++k) per += seg[k];
+        *s_per = per;
+        build_sectors(C, g, P, seg, per, size, J, nj, idl, ib, sec, jw);
+        if (sec.status | *s_st) set_status(S, sec.status | *s_st);
+    }
+    __syncthreads();
+}
+
 template <typename R>
 __global__ void __launch_bounds__(256) k_corrector(NetConst C, NetState* S) {
     const int g = blockIdx.x + 1;
     if (g > C.N || C.state[g] != G_EXISTS || C.regular[g] == 0 || S->loop == 0 || halted(S)) return;
     __shared__ SectorSet sec;
+    __shared__ double jw[64];
+    __shared__ uint32_t s_st;
+    __shared__ double s_per;
     const CPoint* P = S->contPrev + S->coff_prev[g];
     const int size = S->cn_prev[g];
     if (size < 2) return;
+    double* seg = S->segPrev + S->coff_prev[g];
     const Box ib = S->box_prev[g];
     const uint32_t* idl = S->idPrev + S->off_prev[g];
-    if (threadIdx.x == 0) {
-        build_sectors(C, g, P, size, S->jPrev + (int64_t)g * C.jmax, S->jn_prev[g], idl, ib, sec);
-        if (sec.status) set_status(S, sec.status);
-    }
-    __syncthreads();
+    prepare_sectors(C, S, g, P, size, seg, sec, jw, &s_st, &s_per);
     const Box bo = S->box_cur[g];
     const int x0 = ib.x0 < bo.x0 ? bo.x0 : ib.x0;
     const int y0 = ib.y0 < bo.y0 ? bo.y0 : ib.y0;
@@ -442,7 +463,7 @@ __global__ void __launch_bounds__(256) k_corrector(NetConst C, NetState* S) {
         const int64_t k = (int64_t)(i - bo.y0) * wo + (j - bo.x0);
         const R val = in[k];
         if (val > -delta) {
-            const double weight = pixel_weight(C, g, P, size, sec, idl, ib, i, j, &st);
+            const double weight = pixel_weight(C, g, P, seg, size, sec, idl, ib, i, j, &st);
             out[k] = (R)((double)val + ((double)out[k] - (double)val) * weight * 1.0);
         } else {
             out[k] = -delta;

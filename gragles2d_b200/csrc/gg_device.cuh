@@ -162,6 +162,7 @@ struct NetState {
     int32_t* ccap_new;
     int32_t* cn_prev;
     int32_t* cn_cur;
+    double* segPrev;     // per-contour-point segment lengths (corrector scratch, contPrev offsets)
     Junction* jPrev;
     Junction* jCur;
     int32_t* jn_prev;

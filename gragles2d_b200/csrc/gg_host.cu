@@ -656,6 +656,7 @@ int gg_distance_initialisation(gg_ctx* c) {
     ALLOC(S.idCur, phi_cap);
     ALLOC(S.contPrev, cont_cap);
     ALLOC(S.contCur, cont_cap);
+    ALLOC(S.segPrev, cont_cap);
     ALLOC(S.cn_prev, N + 1);
     ALLOC(S.cn_cur, N + 1);
     ALLOC(S.jPrev, (size_t)C.jmax * (N + 1));
