@@ -4,6 +4,7 @@
 #include "gg_corrector.cuh"
 #include "gg_kernels.cuh"
 #include "gg_launch.cuh"
+#include "gg_warp.cuh"
 
 namespace gg {
 
@@ -66,7 +67,7 @@ __global__ void __launch_bounds__(256) k_conv_sep(NetConst C, NetState* S) {
 // previous contour staged in shared memory (FP32 coordinates), junction
 // weights computed one thread per junction, and the per-pixel projection in
 // FP32.
-constexpr int kCorrMaxPts = 4096;
+constexpr int kCorrMaxPts = 1024;
 
 __device__ __forceinline__ int project_f(const float2* P, int asize, float px, float py, float* out_lambda) {
     float minDist = 1e30f;
@@ -129,7 +130,7 @@ __device__ __forceinline__ int project_f(const float2* P, int asize, float px, f
     return seg;
 }
 
-__global__ void __launch_bounds__(256) k_corrector_f(NetConst C, NetState* S) {
+__global__ void __launch_bounds__(128, 6) k_corrector_f(NetConst C, NetState* S) {
     const int g = blockIdx.x + 1;
     if (g > C.N || C.state[g] != G_EXISTS || C.regular[g] == 0 || S->loop == 0 || halted(S)) return;
     __shared__ SectorSet sec;
@@ -137,6 +138,7 @@ __global__ void __launch_bounds__(256) k_corrector_f(NetConst C, NetState* S) {
     __shared__ double jw[64];
     __shared__ uint32_t s_st;
     __shared__ double s_per;
+    __shared__ NbTable nbt;
     const CPoint* P = S->contPrev + S->coff_prev[g];
     const int size = S->cn_prev[g];
     if (size < 2) return;
@@ -146,7 +148,7 @@ __global__ void __launch_bounds__(256) k_corrector_f(NetConst C, NetState* S) {
     const bool staged = size <= kCorrMaxPts;
     if (staged)
         for (int k = threadIdx.x; k < size; k += blockDim.x) sp[k] = make_float2((float)P[k].x, (float)P[k].y);
-    prepare_sectors(C, S, g, P, size, seg, sec, jw, &s_st, &s_per);
+    prepare_sectors(C, S, g, P, size, seg, sec, jw, &s_st, &s_per, nbt);
     const Box bo = S->box_cur[g];
     const int x0 = ib.x0 < bo.x0 ? bo.x0 : ib.x0;
     const int y0 = ib.y0 < bo.y0 ? bo.y0 : ib.y0;
@@ -212,7 +214,7 @@ __global__ void __launch_bounds__(256) k_corrector_f(NetConst C, NetState* S) {
             }
             found = true;
         }
-        if (!found) weight = gb_weight_at(C, g, idl, ib, i, j, &st);
+        if (!found) weight = table_weight_at(nbt, idl, ib, i, j, &st);
         out[k] = val + (out[k] - val) * (float)weight;
     }
     if (st) set_status(S, st);
@@ -241,14 +243,16 @@ cudaError_t batched_init(const NetConst& C, NetState* dS, const int32_t* d_ids, 
 cudaError_t batched_stage_kernel(const NetConst& C, NetState* dS, int which, cudaStream_t s, const LaunchCfg& cfg) {
     const int gt = cfg.grain_threads;
     const int gblocks = (C.N + gt - 1) / gt;
+    const int wblocks = (C.N + kGrainsPerBlock - 1) / kGrainsPerBlock;
+    (void)gblocks;
     switch (which) {
         case 0: k_conv_sep<<<C.N, cfg.conv_threads, conv_sep_smem(C.tmax), s>>>(C, dS); break;
-        case 1: if (!C.isotropic) k_corrector_f<<<C.N, 256, 0, s>>>(C, dS); break;
-        case 2: k_second_order<<<gblocks, gt, 0, s>>>(C, dS); break;
+        case 1: if (!C.isotropic) k_corrector_f<<<C.N, 128, 0, s>>>(C, dS); break;
+        case 2: k_second_order_w<<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS); break;
         case 3: k_compare<float><<<C.N, cfg.compare_threads, 0, s>>>(C, dS); break;
-        case 4: k_levelset<float><<<gblocks, gt, 0, s>>>(C, dS); break;
+        case 4: k_levelset_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS); break;
         case 5: k_alloc<<<1, 1024, 0, s>>>(C, dS, 1); break;
-        case 6: k_neighbours<float><<<gblocks, gt, 0, s>>>(C, dS); break;
+        case 6: k_neighbours_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS, reinterpret_cast<PointInfo*>(C.ptinfo)); break;
         case 7: k_redistance<float><<<C.N, cfg.redist_threads, 0, s>>>(C, dS); break;
         default: k_finalize<<<1, 1024, 0, s>>>(C, dS, 1); break;
     }
@@ -259,16 +263,18 @@ cudaError_t batched_stages(const NetConst& C, NetState* dS, int stages, cudaStre
     if (C.N <= 0) return cudaSuccess;
     const int gt = cfg.grain_threads;
     const int gblocks = (C.N + gt - 1) / gt;
+    const int wblocks = (C.N + kGrainsPerBlock - 1) / kGrainsPerBlock;
+    (void)gblocks;
     if (stages & ST_CONV) {
         k_conv_sep<<<C.N, cfg.conv_threads, conv_sep_smem(C.tmax), s>>>(C, dS);
-        if (!C.isotropic) k_corrector_f<<<C.N, 256, 0, s>>>(C, dS);
+        if (!C.isotropic) k_corrector_f<<<C.N, 128, 0, s>>>(C, dS);
     }
-    if (stages & ST_SECOND) k_second_order<<<gblocks, gt, 0, s>>>(C, dS);
+    if (stages & ST_SECOND) k_second_order_w<<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS);
     if (stages & ST_COMPARE) k_compare<float><<<C.N, cfg.compare_threads, 0, s>>>(C, dS);
-    if (stages & ST_LEVELSET) k_levelset<float><<<gblocks, gt, 0, s>>>(C, dS);
+    if (stages & ST_LEVELSET) k_levelset_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS);
     if (stages & ST_REDIST) {
         k_alloc<<<1, 1024, 0, s>>>(C, dS, 1);
-        k_neighbours<float><<<gblocks, gt, 0, s>>>(C, dS);
+        k_neighbours_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS, reinterpret_cast<PointInfo*>(C.ptinfo));
         k_redistance<float><<<C.N, cfg.redist_threads, 0, s>>>(C, dS);
         k_finalize<<<1, 1024, 0, s>>>(C, dS, 1);
     }

@@ -13,7 +13,7 @@ namespace {  // internal linkage: each form's translation unit has its own copy
 
 
 constexpr int kMaxConstSectors = 32;
-constexpr int kMaxSectorJunctions = 48;
+constexpr int kMaxSectorJunctions = 24;
 constexpr int kMaxInterpSectors = 2 * kMaxConstSectors;
 
 struct ConstSector {
@@ -70,6 +70,43 @@ __device__ __forceinline__ double gb_weight_at(const NetConst& C, int owner, con
     const uint32_t id = idl[k];
     if (id > (uint32_t)C.N) return gb_weight_for(C, owner, -1);
     return gb_weight_for(C, owner, (int)id);
+}
+
+// The owner's direct-neighbour weights (energy x mobility floored at 0.01)
+// for the per-pixel default weight; entries of removed grains are dropped
+// because a removed grain matches no characteristic.
+struct NbTable {
+    int n;
+    int id[48];
+    double w[48];
+};
+
+__device__ void build_nb_table(const NetConst& C, int owner, NbTable& T) {
+    const Neighbour* nb = C.nb + (int64_t)owner * C.nbmax;
+    const int n = min(C.nb_n[owner], 48);
+    if (threadIdx.x == 0) T.n = n;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        const int id = nb[e].id;
+        const bool gone = id < 0 || id > C.N || (id != 0 && C.state[id] == G_GONE);
+        T.id[e] = gone ? -2 : id;
+        const double v = nb[e].energy * nb[e].mobility;
+        T.w[e] = v > 0.01 ? v : 0.01;
+    }
+}
+
+// getGBEnergyTimesGBMobility(i, j) through the table (first match, as the
+// reference's linear search).
+__device__ __forceinline__ double table_weight_at(const NbTable& T, const uint32_t* idl, const Box& ib, int row,
+                                                  int col, uint32_t* status) {
+    uint32_t k;
+    if (!buf_index(ib, row, col, &k)) {
+        *status |= S_INDEX;
+        return 1.0;
+    }
+    const int id = (int)idl[k];
+    for (int e = 0; e < T.n; ++e)
+        if (T.id[e] == id) return T.w[e];
+    return 1.0;
 }
 
 // GrainJunction::getWeight (src/junction.cpp:23-192), mode 4, ResearchMode 0,
@@ -359,9 +396,9 @@ __device__ void build_sectors(const NetConst& C, int g, const CPoint* P, const d
 }
 
 // ExplicitGrainBoundary::getWeight (src/grainBoundary.cpp:344-363) for one pixel.
-__device__ __forceinline__ double pixel_weight(const NetConst& C, int g, const CPoint* P, const double* seg,
-                                               int size, const SectorSet& S, const uint32_t* idl, const Box& ib,
-                                               int i, int j, uint32_t* status) {
+__device__ __forceinline__ double pixel_weight(const NetConst& C, const NbTable& T, const CPoint* P,
+                                               const double* seg, int size, const SectorSet& S, const uint32_t* idl,
+                                               const Box& ib, int i, int j, uint32_t* status) {
     double lambda = 0.0;
     const int segment = project_to_boundary(P, size, (double)j, (double)i, &lambda);
     const int real = size - 1;
@@ -397,14 +434,14 @@ __device__ __forceinline__ double pixel_weight(const NetConst& C, int g, const C
         }
         return interpolator * s.left_w + (1 - interpolator) * s.right_w;
     }
-    return gb_weight_at(C, g, idl, ib, i, j, status);
+    return table_weight_at(T, idl, ib, i, j, status);
 }
 
 // Per-grain preparation shared by both correctors: segment lengths (into
 // the seg scratch, one thread per segment), junction weights (one thread per
 // junction), perimeter, then the sequential sector build by thread 0.
 __device__ void prepare_sectors(const NetConst& C, NetState* S, int g, const CPoint* P, int size, double* seg,
-                                SectorSet& sec, double* jw, uint32_t* s_st, double* s_per) {
+                                SectorSet& sec, double* jw, uint32_t* s_st, double* s_per, NbTable& T) {
     const Box ib = S->box_prev[g];
     const uint32_t* idl = S->idPrev + S->off_prev[g];
     const Junction* J = S->jPrev + (int64_t)g * C.jmax;
@@ -419,6 +456,7 @@ __device__ void prepare_sectors(const NetConst& C, NetState* S, int g, const CPo
         jw[threadIdx.x] = junction_weight(C, J[threadIdx.x], g, &st);
         if (st) atomicOr(s_st, st);
     }
+    build_nb_table(C, g, T);
     __syncthreads();
     if (threadIdx.x == 0) {
         double per = 0;
@@ -431,20 +469,21 @@ __device__ void prepare_sectors(const NetConst& C, NetState* S, int g, const CPo
 }
 
 template <typename R>
-__global__ void __launch_bounds__(256) k_corrector(NetConst C, NetState* S) {
+__global__ void __launch_bounds__(128) k_corrector(NetConst C, NetState* S) {
     const int g = blockIdx.x + 1;
     if (g > C.N || C.state[g] != G_EXISTS || C.regular[g] == 0 || S->loop == 0 || halted(S)) return;
     __shared__ SectorSet sec;
     __shared__ double jw[64];
     __shared__ uint32_t s_st;
     __shared__ double s_per;
+    __shared__ NbTable nbt;
     const CPoint* P = S->contPrev + S->coff_prev[g];
     const int size = S->cn_prev[g];
     if (size < 2) return;
     double* seg = S->segPrev + S->coff_prev[g];
     const Box ib = S->box_prev[g];
     const uint32_t* idl = S->idPrev + S->off_prev[g];
-    prepare_sectors(C, S, g, P, size, seg, sec, jw, &s_st, &s_per);
+    prepare_sectors(C, S, g, P, size, seg, sec, jw, &s_st, &s_per, nbt);
     const Box bo = S->box_cur[g];
     const int x0 = ib.x0 < bo.x0 ? bo.x0 : ib.x0;
     const int y0 = ib.y0 < bo.y0 ? bo.y0 : ib.y0;
@@ -463,7 +502,7 @@ __global__ void __launch_bounds__(256) k_corrector(NetConst C, NetState* S) {
         const int64_t k = (int64_t)(i - bo.y0) * wo + (j - bo.x0);
         const R val = in[k];
         if (val > -delta) {
-            const double weight = pixel_weight(C, g, P, seg, size, sec, idl, ib, i, j, &st);
+            const double weight = pixel_weight(C, nbt, P, seg, size, sec, idl, ib, i, j, &st);
             out[k] = (R)((double)val + ((double)out[k] - (double)val) * weight * 1.0);
         } else {
             out[k] = -delta;

@@ -134,6 +134,7 @@ struct NetConst {
     const int64_t* gk_off;   // [tmax+1]
     const float* ck;         // separable real-space kernel per n at ck_off[n] (batched form)
     const int64_t* ck_off;
+    void* ptinfo;            // per-contour-point probe scratch (contCur offsets), 32 bytes each
 };
 
 // Per-step rotating state, resident in device memory (kernels read it

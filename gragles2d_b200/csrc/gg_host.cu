@@ -657,6 +657,11 @@ int gg_distance_initialisation(gg_ctx* c) {
     ALLOC(S.contPrev, cont_cap);
     ALLOC(S.contCur, cont_cap);
     ALLOC(S.segPrev, cont_cap);
+    {
+        double* pt;
+        ALLOC(pt, 4 * (size_t)cont_cap);  // PointInfo: 32 bytes per contour point
+        C.ptinfo = pt;
+    }
     ALLOC(S.cn_prev, N + 1);
     ALLOC(S.cn_cur, N + 1);
     ALLOC(S.jPrev, (size_t)C.jmax * (N + 1));

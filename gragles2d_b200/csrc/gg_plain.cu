@@ -4,6 +4,7 @@
 #include "gg_corrector.cuh"
 #include "gg_kernels.cuh"
 #include "gg_launch.cuh"
+#include "gg_warp.cuh"
 
 namespace gg {
 
@@ -48,14 +49,16 @@ cudaError_t traffic_launch(const NetConst& C, NetState* dS, cudaStream_t s) {
 cudaError_t plain_stage_kernel(const NetConst& C, NetState* dS, int which, cudaStream_t s, const LaunchCfg& cfg) {
     const int gt = cfg.grain_threads;
     const int gblocks = (C.N + gt - 1) / gt;
+    const int wblocks = (C.N + kGrainsPerBlock - 1) / kGrainsPerBlock;
+    (void)gblocks;
     switch (which) {
         case 0: k_conv_dft<double><<<C.N, cfg.conv_threads, 0, s>>>(C, dS); break;
-        case 1: if (!C.isotropic) k_corrector<double><<<C.N, 256, 0, s>>>(C, dS); break;
-        case 2: k_second_order<<<gblocks, gt, 0, s>>>(C, dS); break;
+        case 1: if (!C.isotropic) k_corrector<double><<<C.N, 128, 0, s>>>(C, dS); break;
+        case 2: k_second_order_w<<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS); break;
         case 3: k_compare<double><<<C.N, cfg.compare_threads, 0, s>>>(C, dS); break;
-        case 4: k_levelset<double><<<gblocks, gt, 0, s>>>(C, dS); break;
+        case 4: k_levelset_w<double><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS); break;
         case 5: k_alloc<<<1, 1024, 0, s>>>(C, dS, 2); break;
-        case 6: k_neighbours<double><<<gblocks, gt, 0, s>>>(C, dS); break;
+        case 6: k_neighbours_w<double><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS, reinterpret_cast<PointInfo*>(C.ptinfo)); break;
         case 7: k_redistance<double><<<C.N, cfg.redist_threads, 0, s>>>(C, dS); break;
         default: k_finalize<<<1, 1024, 0, s>>>(C, dS, 1); break;
     }
@@ -63,7 +66,7 @@ cudaError_t plain_stage_kernel(const NetConst& C, NetState* dS, int which, cudaS
 }
 
 cudaError_t plain_corrector(const NetConst& C, NetState* dS, cudaStream_t s) {
-    k_corrector<double><<<C.N, 256, 0, s>>>(C, dS);
+    k_corrector<double><<<C.N, 128, 0, s>>>(C, dS);
     return cudaGetLastError();
 }
 
@@ -71,6 +74,8 @@ cudaError_t plain_stages(const NetConst& C, NetState* dS, int stages, cudaStream
     if (C.N <= 0) return cudaSuccess;
     const int gt = cfg.grain_threads;
     const int gblocks = (C.N + gt - 1) / gt;
+    const int wblocks = (C.N + kGrainsPerBlock - 1) / kGrainsPerBlock;
+    (void)gblocks;
     if (stages & ST_CONV) {
         k_conv_dft<double><<<C.N, cfg.conv_threads, 0, s>>>(C, dS);
         if (!C.isotropic) {
@@ -78,12 +83,12 @@ cudaError_t plain_stages(const NetConst& C, NetState* dS, int stages, cudaStream
             if (e != cudaSuccess) return e;
         }
     }
-    if (stages & ST_SECOND) k_second_order<<<gblocks, gt, 0, s>>>(C, dS);
+    if (stages & ST_SECOND) k_second_order_w<<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS);
     if (stages & ST_COMPARE) k_compare<double><<<C.N, cfg.compare_threads, 0, s>>>(C, dS);
-    if (stages & ST_LEVELSET) k_levelset<double><<<gblocks, gt, 0, s>>>(C, dS);
+    if (stages & ST_LEVELSET) k_levelset_w<double><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS);
     if (stages & ST_REDIST) {
         k_alloc<<<1, 1024, 0, s>>>(C, dS, 2);
-        k_neighbours<double><<<gblocks, gt, 0, s>>>(C, dS);
+        k_neighbours_w<double><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS, reinterpret_cast<PointInfo*>(C.ptinfo));
         k_redistance<double><<<C.N, cfg.redist_threads, 0, s>>>(C, dS);
         k_finalize<<<1, 1024, 0, s>>>(C, dS, 1);
     }
