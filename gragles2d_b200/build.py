@@ -27,6 +27,7 @@ UNITS = {
     "gg_plain": ["--fmad=false"],
     "gg_batched": [],
     "gg_host": ["--fmad=false"],
+    "gg_static": ["--fmad=false"],
 }
 
 

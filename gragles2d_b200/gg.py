@@ -28,8 +28,9 @@ EXPORTS = (
     "gg_load_voxel_files", "gg_distance_initialisation", "gg_find_neighbors", "gg_set_neighbours",
     "gg_convolution", "gg_update_second_order_neighbors", "gg_comparison", "gg_level_set", "gg_redistancing",
     "gg_grain_count", "gg_step", "gg_status", "gg_read_grain_stats", "gg_dims", "gg_dump", "gg_last_step_ms",
-    "gg_grain_updates", "gg_profile_steps", "gg_traffic",
+    "gg_grain_updates", "gg_profile_steps", "gg_traffic", "gg_convolve_box_static",
 )
+STATIC_CONV_MAX_N = 128
 NSTAGES = 9
 STAGE_NAMES = ("convolution", "corrector", "second_order", "comparison", "level_set", "alloc",
                "volume_energy_neighbours", "redistancing", "end_of_step")
@@ -110,6 +111,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "gg_grain_updates": (I, [V, P(ctypes.c_int64)]),
         "gg_profile_steps": (I, [V, I, I, P(D)]),
         "gg_traffic": (I, [V, P(ctypes.c_int64), P(ctypes.c_int64), P(I)]),
+        "gg_convolve_box_static": (I, [V, V, I, D, I, V]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -117,6 +119,16 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         fn.argtypes = args
     _lib = lib
     return lib
+
+
+def convolve_box_static(d_in: int, d_out: int, n: int, dt: float, real_domain_size: int, stream: int = 0) -> None:
+    """Allocation-free convolution of one n x n FP64 box (device pointers),
+    bit-identical to the plain convolution stage; see gg_convolve_box_static."""
+    lib = load_library()
+    rc = lib.gg_convolve_box_static(ctypes.c_void_p(d_in), ctypes.c_void_p(d_out), n, dt, real_domain_size,
+                                    ctypes.c_void_p(stream))
+    if rc != GG_OK:
+        raise GGError(rc, f"gg_convolve_box_static(n={n})")
 
 
 class Settings:

@@ -206,6 +206,31 @@ int gg_profile_steps(gg_ctx* ctx, int32_t loop, int32_t nsteps, double* stage_ms
  * comparison-list members, and the number of existing grains. */
 int gg_traffic(gg_ctx* ctx, int64_t* sum_area, int64_t* sum_overlap, int32_t* n_exists);
 
+/*
+ * Allocation-free box convolution.  No counterpart in the reference: the
+ * reference allocates its FFT scratch per thread.  For callers that cannot
+ * allocate device memory (an application that passes this library buffers
+ * from its own device memory pool and does not allow plug-ins to allocate),
+ * this convolves one n x n box with the Gaussian kernel of the convolution
+ * stage (src/box.cpp:622-695), with the plain form's arithmetic, so the
+ * result is bit-identical to that stage.
+ *  - d_in, d_out: caller-owned device buffers of n*n doubles, row-major.
+ *  - dt, real_domain_size: the timestep and grid edge the kernel depends on.
+ *  - stream: a cudaStream_t (NULL for the default stream); the call returns
+ *    after the work on that stream has finished.
+ * It calls no cudaMalloc, cudaFree or allocating library routine: its scratch
+ * is a fixed array of about 300 KB compiled into the library, which every GPU
+ * that loads the library holds until the process exits.  n must be in
+ * 1..GG_STATIC_CONV_MAX_N, else GG_E_INVALID is returned.  The first call on
+ * a device looks up the scratch's device address (once per device); make
+ * that first call before capturing any stream.  All calls on a device share
+ * the one scratch array, so calls that overlap on the GPU (from several host
+ * threads or streams) race; serialise them.
+ */
+#define GG_STATIC_CONV_MAX_N 128
+int gg_convolve_box_static(const double* d_in, double* d_out, int32_t n, double dt, int32_t real_domain_size,
+                           void* stream);
+
 #ifdef __cplusplus
 }
 #endif
