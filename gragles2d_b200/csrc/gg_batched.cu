@@ -8,14 +8,80 @@
 
 namespace gg {
 
-constexpr int kSepSmemMaxN = 64;  // 2 n^2 + n floats of shared memory (larger boxes stage in global scratch)
+constexpr int kSepSmemMaxN = 64;  // box + intermediate in shared memory up to this edge
+constexpr int kSepStrip = 4;       // outputs per thread along the convolution axis
 
 // Gaussian convolution as a separable circular convolution in real space:
 // out = K X K^T with K[r][r'] = k_n[(r - r') mod n], where k_n is the real
 // kernel whose DFT is the reference's Gaussian multiplier
-// (src/box.cpp:674-687, G(i2, j2) = g(i2) g(j2) / n^2).  One CTA per grain;
-// the box and the intermediate stay in shared memory when n <= 64.
-__global__ void __launch_bounds__(256) k_conv_sep(NetConst C, NetState* S) {
+// (src/box.cpp:674-687, G(i2, j2) = g(i2) g(j2) / n^2).  One CTA per grain.
+// The kernel is laid out once as kx[j] = k_n[(j - (n-1)) mod n], j < 2n-1
+// (zero-padded), so output c of a row is sum_c' X[c'] kx[c - c' + n - 1]:
+// each thread accumulates a strip of 4 consecutive outputs while a 4-entry
+// register window slides down kx (one shared-memory load per 4 FMAs).
+__device__ __forceinline__ void sep_pass_rows(const float* __restrict__ X, float* __restrict__ T,
+                                              const float* __restrict__ kx, int n) {
+    const int nb = (n + kSepStrip - 1) / kSepStrip;
+    for (int t = threadIdx.x; t < n * nb; t += blockDim.x) {
+        const int r = t / nb, c0 = (t - r * nb) * kSepStrip;
+        const float* xr = X + r * n;
+        int base = c0 + n - 1;  // kx index of (c0 - c') at c' = 0
+        float w0 = kx[base], w1 = kx[base + 1], w2 = kx[base + 2], w3 = kx[base + 3];
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+#pragma unroll 4
+        for (int cp = 0; cp < n; ++cp) {
+            const float x = xr[cp];
+            a0 = fmaf(x, w0, a0);
+            a1 = fmaf(x, w1, a1);
+            a2 = fmaf(x, w2, a2);
+            a3 = fmaf(x, w3, a3);
+            --base;
+            w3 = w2;
+            w2 = w1;
+            w1 = w0;
+            w0 = kx[base];
+        }
+        float* tr = T + r * n + c0;
+        tr[0] = a0;
+        if (c0 + 1 < n) tr[1] = a1;
+        if (c0 + 2 < n) tr[2] = a2;
+        if (c0 + 3 < n) tr[3] = a3;
+    }
+}
+
+__device__ __forceinline__ void sep_pass_cols(const float* __restrict__ T, float* __restrict__ out,
+                                              const float* __restrict__ kx, int n) {
+    const int nb = (n + kSepStrip - 1) / kSepStrip;
+    for (int t = threadIdx.x; t < n * nb; t += blockDim.x) {
+        const int rb = t / n, c = t - rb * n, r0 = rb * kSepStrip;
+        int base = r0 + n - 1;
+        float w0 = kx[base], w1 = kx[base + 1], w2 = kx[base + 2], w3 = kx[base + 3];
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+#pragma unroll 4
+        for (int rp = 0; rp < n; ++rp) {
+            const float x = T[rp * n + c];
+            a0 = fmaf(w0, x, a0);
+            a1 = fmaf(w1, x, a1);
+            a2 = fmaf(w2, x, a2);
+            a3 = fmaf(w3, x, a3);
+            --base;
+            w3 = w2;
+            w2 = w1;
+            w1 = w0;
+            w0 = kx[base];
+        }
+        out[r0 * n + c] = a0;
+        if (r0 + 1 < n) out[(r0 + 1) * n + c] = a1;
+        if (r0 + 2 < n) out[(r0 + 2) * n + c] = a2;
+        if (r0 + 3 < n) out[(r0 + 3) * n + c] = a3;
+    }
+}
+
+// Extended kernel length: 2n-1 entries plus the window's look-ahead, and one
+// guard entry below index 0 (the window reads kx[-1] after its last step).
+__device__ __forceinline__ int kx_len(int n) { return 2 * n + kSepStrip + 1; }
+
+__global__ void __launch_bounds__(128) k_conv_sep(NetConst C, NetState* S) {
     extern __shared__ float sm[];
     const int g = blockIdx.x + 1;
     if (g > C.N || C.state[g] != G_EXISTS || halted(S)) return;
@@ -31,36 +97,28 @@ __global__ void __launch_bounds__(256) k_conv_sep(NetConst C, NetState* S) {
     const float* kg = C.ck + C.ck_off[n];
     const int nn2 = n * n;
     const bool fits = n <= kSepSmemMaxN;
-    float* kk = sm;
-    float* X = sm + n;
+    float* kx = sm + 1;  // sm[0] is the guard entry kx[-1]
+    const int kl = kx_len(n);
+    float* X = sm + 1 + kl;
     float* T = fits ? X + nn2 : reinterpret_cast<float*>(S->spec) + S->soff_cur[g];
-    const float* Xr = fits ? X : in;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) kk[i] = kg[i];
+    for (int j = threadIdx.x; j < kl; j += blockDim.x) {
+        int m = j - (n - 1);
+        m %= n;
+        if (m < 0) m += n;
+        kx[j] = j < 2 * n - 1 ? kg[m] : 0.f;
+    }
+    if (threadIdx.x == 0) sm[0] = 0.f;
     if (fits)
         for (int i = threadIdx.x; i < nn2; i += blockDim.x) X[i] = in[i];
     __syncthreads();
-    for (int idx = threadIdx.x; idx < nn2; idx += blockDim.x) {
-        const int r = idx / n, c = idx - r * n;
-        const float* xr = Xr + r * n;
-        float acc = 0.f;
-        int m = c;  // (c - c') mod n, c' = 0
-        for (int cp = 0; cp < n; ++cp) {
-            acc = fmaf(xr[cp], kk[m], acc);
-            m = (m == 0) ? n - 1 : m - 1;
-        }
-        T[idx] = acc;
-    }
+    sep_pass_rows(fits ? X : in, T, kx, n);
     __syncthreads();
-    for (int idx = threadIdx.x; idx < nn2; idx += blockDim.x) {
-        const int r = idx / n, c = idx - r * n;
-        float acc = 0.f;
-        int m = r;
-        for (int rp = 0; rp < n; ++rp) {
-            acc = fmaf(kk[m], T[rp * n + c], acc);
-            m = (m == 0) ? n - 1 : m - 1;
-        }
-        out[idx] = acc;
-    }
+    sep_pass_cols(T, out, kx, n);
+}
+
+size_t conv_sep_smem(int tmax) {
+    const int n = tmax < kSepSmemMaxN ? tmax : kSepSmemMaxN;
+    return sizeof(float) * (size_t)(2 * n * n + 2 * kSepSmemMaxN + kSepStrip + 2);
 }
 
 // Batched-form corrector: same sectors and weights as k_corrector, with the
@@ -68,16 +126,33 @@ __global__ void __launch_bounds__(256) k_conv_sep(NetConst C, NetState* S) {
 // weights computed one thread per junction, and the per-pixel projection in
 // FP32.
 constexpr int kCorrMaxPts = 1024;
+constexpr int kCorrMaxPix = 4096;  // compacted pixel list (boxes up to 64 x 64)
 
-__device__ __forceinline__ int project_f(const float2* P, int asize, float px, float py, float* out_lambda) {
-    float minDist = 1e30f;
+constexpr int kChunk = 8;  // contour points per bounding box of the nearest-vertex search
+
+// projectToGrainBondary (src/grainBoundary.cpp:365-447) in FP32 over the
+// staged contour.  The nearest-vertex scan skips every run of 8 consecutive
+// points whose bounding box is farther than the best point found so far
+// (runs are visited in index order, so ties still go to the first point).
+__device__ __forceinline__ int project_f(const float2* P, const float4* cbb, int asize, float px, float py,
+                                         float* out_lambda) {
+    float minDist = 3.0e38f;
     int nearest = -1;
-    for (int k = 0; k < asize - 1; k++) {
-        const float dx = px - P[k].x, dy = py - P[k].y;
-        const float d = dx * dx + dy * dy;
-        if (d < minDist) {
-            nearest = k;
-            minDist = d;
+    const int npts = asize - 1;
+    const int nch = (npts + kChunk - 1) / kChunk;
+    for (int ch = 0; ch < nch; ++ch) {
+        const float4 b = cbb[ch];
+        const float bx = fmaxf(fmaxf(b.x - px, px - b.y), 0.f);
+        const float by = fmaxf(fmaxf(b.z - py, py - b.w), 0.f);
+        if (bx * bx + by * by > minDist) continue;
+        const int k1 = min(ch * kChunk + kChunk, npts);
+        for (int k = ch * kChunk; k < k1; k++) {
+            const float dx = px - P[k].x, dy = py - P[k].y;
+            const float d = dx * dx + dy * dy;
+            if (d < minDist) {
+                nearest = k;
+                minDist = d;
+            }
         }
     }
     if (nearest < 0) return 0;
@@ -139,6 +214,9 @@ __global__ void __launch_bounds__(128, 6) k_corrector_f(NetConst C, NetState* S)
     __shared__ uint32_t s_st;
     __shared__ double s_per;
     __shared__ NbTable nbt;
+    __shared__ float4 cbb[kCorrMaxPts / kChunk];
+    __shared__ unsigned short plist[kCorrMaxPix];
+    __shared__ int pcount;
     const CPoint* P = S->contPrev + S->coff_prev[g];
     const int size = S->cn_prev[g];
     if (size < 2) return;
@@ -148,6 +226,21 @@ __global__ void __launch_bounds__(128, 6) k_corrector_f(NetConst C, NetState* S)
     const bool staged = size <= kCorrMaxPts;
     if (staged)
         for (int k = threadIdx.x; k < size; k += blockDim.x) sp[k] = make_float2((float)P[k].x, (float)P[k].y);
+    if (threadIdx.x == 0) pcount = 0;
+    __syncthreads();
+    if (staged) {
+        const int npts = size - 1, nch = (npts + kChunk - 1) / kChunk;
+        for (int ch = threadIdx.x; ch < nch; ch += blockDim.x) {
+            float4 b = make_float4(3.0e38f, -3.0e38f, 3.0e38f, -3.0e38f);
+            for (int k = ch * kChunk; k < min(ch * kChunk + kChunk, npts); ++k) {
+                b.x = fminf(b.x, sp[k].x);
+                b.y = fmaxf(b.y, sp[k].x);
+                b.z = fminf(b.z, sp[k].y);
+                b.w = fmaxf(b.w, sp[k].y);
+            }
+            cbb[ch] = b;
+        }
+    }
     prepare_sectors(C, S, g, P, size, seg, sec, jw, &s_st, &s_per, nbt);
     const Box bo = S->box_cur[g];
     const int x0 = ib.x0 < bo.x0 ? bo.x0 : ib.x0;
@@ -163,18 +256,39 @@ __global__ void __launch_bounds__(128, 6) k_corrector_f(NetConst C, NetState* S)
     const float delta = (float)C.delta;
     const int real = size - 1;
     uint32_t st = 0;
-    for (int p = threadIdx.x; p < cnt; p += blockDim.x) {
+    // pixels at or below -delta are set to -delta; the others are compacted
+    // into a list so every lane of a warp projects a pixel
+    const bool compact = cnt <= kCorrMaxPix;
+    for (int p0 = 0; p0 < cnt; p0 += blockDim.x) {
+        const int p = p0 + threadIdx.x;
+        bool active = false;
+        if (p < cnt) {
+            const int i = y0 + p / w, j = x0 + p % w;
+            const int k = (i - bo.y0) * wo + (j - bo.x0);
+            active = in[k] > -delta;
+            if (!active) out[k] = -delta;
+        }
+        if (compact) {
+            const int lane = threadIdx.x & 31;
+            const unsigned bal = __ballot_sync(0xffffffffu, active);
+            int base = 0;
+            if (lane == 0 && bal) base = atomicAdd(&pcount, __popc(bal));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (active) plist[base + __popc(bal & ((1u << lane) - 1u))] = (unsigned short)p;
+        }
+    }
+    __syncthreads();
+    const int total = compact ? pcount : cnt;
+    for (int q = threadIdx.x; q < total; q += blockDim.x) {
+        const int p = compact ? (int)plist[q] : q;
         const int i = y0 + p / w, j = x0 + p % w;
         const int k = (i - bo.y0) * wo + (j - bo.x0);
         const float val = in[k];
-        if (!(val > -delta)) {
-            out[k] = -delta;
-            continue;
-        }
+        if (!compact && !(val > -delta)) continue;
         float lambda = 0.f;
         int segment;
         if (staged) {
-            segment = project_f(sp, size, (float)j, (float)i, &lambda);
+            segment = project_f(sp, cbb, size, (float)j, (float)i, &lambda);
         } else {
             double dl = 0;
             segment = project_to_boundary(P, size, (double)j, (double)i, &dl);
@@ -220,10 +334,6 @@ __global__ void __launch_bounds__(128, 6) k_corrector_f(NetConst C, NetState* S)
     if (st) set_status(S, st);
 }
 
-size_t conv_sep_smem(int tmax) {
-    const int n = tmax < kSepSmemMaxN ? tmax : kSepSmemMaxN;
-    return sizeof(float) * (size_t)(2 * n * n + n);
-}
 
 cudaError_t batched_prepare(int tmax) {
     return cudaFuncSetAttribute(k_conv_sep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conv_sep_smem(tmax));
@@ -246,14 +356,14 @@ cudaError_t batched_stage_kernel(const NetConst& C, NetState* dS, int which, cud
     const int wblocks = (C.N + kGrainsPerBlock - 1) / kGrainsPerBlock;
     (void)gblocks;
     switch (which) {
-        case 0: k_conv_sep<<<C.N, cfg.conv_threads, conv_sep_smem(C.tmax), s>>>(C, dS); break;
+        case 0: k_conv_sep<<<C.N, 128, conv_sep_smem(C.tmax), s>>>(C, dS); break;
         case 1: if (!C.isotropic) k_corrector_f<<<C.N, 128, 0, s>>>(C, dS); break;
         case 2: k_second_order_w<<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS); break;
         case 3: k_compare<float><<<C.N, cfg.compare_threads, 0, s>>>(C, dS); break;
         case 4: k_levelset_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS); break;
         case 5: k_alloc<<<1, 1024, 0, s>>>(C, dS, 1); break;
         case 6: k_neighbours_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS, reinterpret_cast<PointInfo*>(C.ptinfo)); break;
-        case 7: k_redistance<float><<<C.N, cfg.redist_threads, 0, s>>>(C, dS); break;
+        case 7: k_redistance_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS); break;
         default: k_finalize<<<1, 1024, 0, s>>>(C, dS, 1); break;
     }
     return cudaGetLastError();
@@ -266,7 +376,7 @@ cudaError_t batched_stages(const NetConst& C, NetState* dS, int stages, cudaStre
     const int wblocks = (C.N + kGrainsPerBlock - 1) / kGrainsPerBlock;
     (void)gblocks;
     if (stages & ST_CONV) {
-        k_conv_sep<<<C.N, cfg.conv_threads, conv_sep_smem(C.tmax), s>>>(C, dS);
+        k_conv_sep<<<C.N, 128, conv_sep_smem(C.tmax), s>>>(C, dS);
         if (!C.isotropic) k_corrector_f<<<C.N, 128, 0, s>>>(C, dS);
     }
     if (stages & ST_SECOND) k_second_order_w<<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS);
@@ -275,7 +385,7 @@ cudaError_t batched_stages(const NetConst& C, NetState* dS, int stages, cudaStre
     if (stages & ST_REDIST) {
         k_alloc<<<1, 1024, 0, s>>>(C, dS, 1);
         k_neighbours_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS, reinterpret_cast<PointInfo*>(C.ptinfo));
-        k_redistance<float><<<C.N, cfg.redist_threads, 0, s>>>(C, dS);
+        k_redistance_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS);
         k_finalize<<<1, 1024, 0, s>>>(C, dS, 1);
     }
     return cudaGetLastError();

@@ -38,21 +38,39 @@ __device__ int first_inside_warp(const Field<R>& f, int lane) {
 }
 
 // Marching-squares walk from a known start pixel (src/marchingSquares.cpp:44-187).
+// The four corner values of the current square are kept in registers and
+// only the two corners a move uncovers are loaded; the last emitted point
+// is kept in registers for insertPoint's duplicate test; junction corners
+// are only read where a junction is possible (at most two inside corners).
 template <typename R>
 __device__ void ms_walk(const Field<R>& f, const uint32_t* idl, uint32_t own, int startX, int startY,
                         ContourOut& o) {
     o.n = 0;
     o.jn = 0;
+    const Box b = f.b;
+    const int w = b.x1 - b.x0;
+    auto val = [&](int row, int col, double* v) -> bool {  // value and isInside
+        if (row < b.y0 || row >= b.y1 || col < b.x0 || col >= b.x1) {
+            *v = -1.0;
+            return false;
+        }
+        *v = (double)f.v[(row - b.y0) * w + (col - b.x0)];
+        return *v >= 0;
+    };
     int left = startX - 1, right = startX, top = startY - 1, bottom = startY;
+    double vTL, vTR, vBL, vBR;
+    bool iTL = val(top, left, &vTL), iTR = val(top, right, &vTR);
+    bool iBL = val(bottom, left, &vBL), iBR = val(bottom, right, &vBR);
     int next = MS_NONE, prev = MS_NONE;
-    const long limit = 4L * (box_w(f.b) + 2) * (box_h(f.b) + 2) + 16;
+    double lastx = 0, lasty = 0, firstx = 0, firsty = 0;
+    const long limit = 4L * (w + 2) * (box_h(b) + 2) + 16;
     long it = 0;
     do {
         int mask = 0;
-        if (f.inside(top, left)) mask |= C_TL;
-        if (f.inside(top, right)) mask |= C_TR;
-        if (f.inside(bottom, left)) mask |= C_BL;
-        if (f.inside(bottom, right)) mask |= C_BR;
+        if (iTL) mask |= C_TL;
+        if (iTR) mask |= C_TR;
+        if (iBL) mask |= C_BL;
+        if (iBR) mask |= C_BR;
         bool emit = true;
         switch (mask) {
             case C_TL: next = MS_UP; break;
@@ -77,17 +95,111 @@ __device__ void ms_walk(const Field<R>& f, const uint32_t* idl, uint32_t own, in
             case C_BR | C_BL | C_TR: next = MS_LEFT; break;
             default: emit = false; break;
         }
-        if (emit) {
-            double px, py;
-            ms_point(f, next, top, bottom, left, right, &px, &py);
-            ms_insert(o, px, py);
+        if (emit) {  // generatePoint (src/marchingSquares.cpp:204-265) on the cached corners
+            double px, py, delta, position;
+            switch (next) {
+                case MS_LEFT:
+                    px = left;
+                    if (top < b.y0) {
+                        py = bottom;
+                    } else {
+                        delta = vBL - vTL;
+                        position = bottom - vBL / delta;
+                        py = position;
+                    }
+                    break;
+                case MS_RIGHT:
+                    px = right;
+                    if (bottom >= b.y1) {
+                        py = top;
+                    } else {
+                        delta = vTR - vBR;
+                        position = top + vTR / delta;
+                        py = position;
+                    }
+                    break;
+                case MS_UP:
+                    py = top;
+                    if (right >= b.x1) {
+                        px = left;
+                    } else {
+                        delta = vTL - vTR;
+                        position = left + vTL / delta;
+                        px = position;
+                    }
+                    break;
+                default:
+                    py = bottom;
+                    if (left < b.x0) {
+                        px = right;
+                    } else {
+                        delta = vBR - vBL;
+                        position = right - vBR / delta;
+                        px = position;
+                    }
+                    break;
+            }
+            if (o.n == 0 || px != lastx || py != lasty) {  // insertPoint
+                if (o.n >= o.cap) {
+                    o.status |= S_CONTOUR_OVERFLOW;
+                } else {
+                    CPoint& q = o.pts[o.n];
+                    q.x = px;
+                    q.y = py;
+                    q.energy = -1.0;
+                    q.mob = -1.0;
+                    if (o.n == 0) {
+                        firstx = px;
+                        firsty = py;
+                    }
+                    o.n++;
+                    lastx = px;
+                    lasty = py;
+                }
+            }
         }
-        ms_junction(f, idl, own, mask, top, bottom, left, right, o);
+        if (__popc(mask) < 3) ms_junction(f, idl, own, mask, top, bottom, left, right, o);
         switch (next) {
-            case MS_UP: top--; bottom--; break;
-            case MS_DOWN: top++; bottom++; break;
-            case MS_LEFT: left--; right--; break;
-            case MS_RIGHT: left++; right++; break;
+            case MS_UP:
+                top--;
+                bottom--;
+                vBL = vTL;
+                vBR = vTR;
+                iBL = iTL;
+                iBR = iTR;
+                iTL = val(top, left, &vTL);
+                iTR = val(top, right, &vTR);
+                break;
+            case MS_DOWN:
+                top++;
+                bottom++;
+                vTL = vBL;
+                vTR = vBR;
+                iTL = iBL;
+                iTR = iBR;
+                iBL = val(bottom, left, &vBL);
+                iBR = val(bottom, right, &vBR);
+                break;
+            case MS_LEFT:
+                left--;
+                right--;
+                vTR = vTL;
+                vBR = vBL;
+                iTR = iTL;
+                iBR = iBL;
+                iTL = val(top, left, &vTL);
+                iBL = val(bottom, left, &vBL);
+                break;
+            case MS_RIGHT:
+                left++;
+                right++;
+                vTL = vTR;
+                vBL = vBR;
+                iTL = iTR;
+                iBL = iBR;
+                iTR = val(top, right, &vTR);
+                iBR = val(bottom, right, &vBR);
+                break;
             default: break;
         }
         prev = next;
@@ -96,7 +208,7 @@ __device__ void ms_walk(const Field<R>& f, const uint32_t* idl, uint32_t own, in
             break;
         }
     } while (left != startX - 1 || bottom != startY);
-    if (o.n > 0 && (o.pts[0].x != o.pts[o.n - 1].x || o.pts[0].y != o.pts[o.n - 1].y)) {
+    if (o.n > 0 && (firstx != lastx || firsty != lasty)) {
         if (o.n >= o.cap) {
             o.status |= S_CONTOUR_OVERFLOW;
         } else {
@@ -383,6 +495,91 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_second_order_w(NetCons
     if (lane == 0) {
         C.cmp_n[g] = nc;
         if (overflow) set_status(S, S_LIST_OVERFLOW);
+    }
+}
+
+// LSbox::executeRedistancing (src/box.cpp:1259-1399), one warp per grain:
+// lanes take columns for the two y sweeps, then rows for the two x sweeps
+// (each column / row is a sequential recurrence, as in the reference).
+template <typename R>
+__global__ void __launch_bounds__(32 * kGrainsPerBlock) k_redistance_w(NetConst C, NetState* S) {
+    const int lane = threadIdx.x & 31;
+    const int g = blockIdx.x * kGrainsPerBlock + (threadIdx.x >> 5) + 1;
+    if (g > C.N || C.state[g] != G_EXISTS || halted(S)) return;
+    const R* __restrict__ in = phiA_of<R>(S) + S->off_cur[g];
+    R* __restrict__ out = phiB_of<R>(S) + S->off_new[g];
+    const Box bi = S->box_cur[g], bo = S->box_new[g];
+    const R h = (R)C.h, delta = (R)C.delta;
+    const int wi = box_w(bi), wo = box_w(bo);
+    const int64_t ao = box_area(bo);
+    for (int64_t p = lane; p < ao; p += 32) out[p] = (R)-1.0;
+    __syncwarp();
+    const int ixmin = (bi.x0 < bo.x0) ? bo.x0 : bi.x0;
+    const int iymin = (bi.y0 < bo.y0) ? bo.y0 : bi.y0;
+    const int ixmax = (bi.x1 < bo.x1) ? bi.x1 : bo.x1;
+    const int iymax = (bi.y1 < bo.y1) ? bi.y1 : bo.y1;
+#define GG_IN(i, j) in[(int64_t)((i) - bi.y0) * wi + ((j) - bi.x0)]
+#define GG_OUT(i, j) out[(int64_t)((i) - bo.y0) * wo + ((j) - bo.x0)]
+    for (int j = ixmin + lane; j < bo.x1; j += 32) {
+        for (int i = iymin; i < bo.y1 - 1; i++) {  // y forward
+            R cand;
+            if (j < ixmax && i < iymax - 1) {
+                const R a = GG_IN(i, j), c = GG_IN(i + 1, j);
+                if (a * c <= (R)0.0) {
+                    const R slope = (c - a) / h;
+                    const R dz = -a / slope;
+                    if (fabs(GG_OUT(i, j)) > fabs(dz)) GG_OUT(i, j) = -dz * (R)sgn(slope);
+                }
+                cand = GG_OUT(i, j) + ((R)sgn(c) * h);
+            } else {
+                cand = GG_OUT(i, j) + ((R)sgn(GG_OUT(i + 1, j)) * h);
+            }
+            if (fabs(cand) < fabs(GG_OUT(i + 1, j))) GG_OUT(i + 1, j) = cand;
+        }
+        for (int i = iymax - 1; i > bo.y0; i--) {  // y backward
+            R cand;
+            if (j < ixmax && i > iymin)
+                cand = GG_OUT(i, j) + ((R)sgn(GG_IN(i - 1, j)) * h);
+            else
+                cand = GG_OUT(i, j) + ((R)sgn(GG_OUT(i - 1, j)) * h);
+            if (fabs(cand) < fabs(GG_OUT(i - 1, j))) GG_OUT(i - 1, j) = cand;
+        }
+    }
+    __syncwarp();
+    for (int i = iymin + lane; i < bo.y1; i += 32) {
+        for (int j = ixmin; j < bo.x1 - 1; j++) {  // x forward
+            R cand;
+            if (j < ixmax - 1 && i < iymax) {
+                const R a = GG_IN(i, j), c = GG_IN(i, j + 1);
+                if (a * c <= (R)0.0) {
+                    const R slope = (c - a) / h;
+                    const R dz = -a / slope;
+                    if (fabs(GG_OUT(i, j)) > fabs(dz)) GG_OUT(i, j) = -dz * (R)sgn(slope);
+                }
+                cand = GG_OUT(i, j) + ((R)sgn(c) * h);
+            } else {
+                cand = GG_OUT(i, j) + ((R)sgn(GG_OUT(i, j + 1)) * h);
+            }
+            if (fabs(cand) < fabs(GG_OUT(i, j + 1))) GG_OUT(i, j + 1) = cand;
+        }
+        for (int j = ixmax - 1; j > bo.x0; j--) {  // x backward
+            R cand;
+            if (j > ixmin && i < iymax)
+                cand = GG_OUT(i, j) + ((R)sgn(GG_IN(i, j - 1)) * h);
+            else
+                cand = GG_OUT(i, j) + (R)sgn(GG_OUT(i, j - 1)) * h;
+            if (fabs(cand) < fabs(GG_OUT(i, j - 1))) GG_OUT(i, j - 1) = cand;
+        }
+    }
+#undef GG_IN
+#undef GG_OUT
+    __syncwarp();
+    for (int64_t p = lane; p < ao; p += 32) {  // clampValues(-delta, delta)
+        const R v = out[p];
+        if (v < -delta)
+            out[p] = -delta;
+        else if (v > delta)
+            out[p] = delta;
     }
 }
 
