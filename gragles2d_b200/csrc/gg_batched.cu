@@ -217,10 +217,11 @@ __global__ void __launch_bounds__(128, 6) k_corrector_f(NetConst C, NetState* S)
     __shared__ float4 cbb[kCorrMaxPts / kChunk];
     __shared__ unsigned short plist[kCorrMaxPix];
     __shared__ int pcount;
+    __shared__ double s_seg[kSegShared];
     const CPoint* P = S->contPrev + S->coff_prev[g];
     const int size = S->cn_prev[g];
     if (size < 2) return;
-    double* seg = S->segPrev + S->coff_prev[g];
+    double* seg = size - 1 <= kSegShared ? s_seg : S->segPrev + S->coff_prev[g];
     const Box ib = S->box_prev[g];
     const uint32_t* idl = S->idPrev + S->off_prev[g];
     const bool staged = size <= kCorrMaxPts;

@@ -15,6 +15,7 @@ namespace {  // internal linkage: each form's translation unit has its own copy
 constexpr int kMaxConstSectors = 32;
 constexpr int kMaxSectorJunctions = 24;
 constexpr int kMaxInterpSectors = 2 * kMaxConstSectors;
+constexpr int kSegShared = 1024;  // contours up to this length keep their segment lengths in shared memory
 
 struct ConstSector {
     int left, right;  // contour point IDs (-1, -1: whole contour)
@@ -477,10 +478,11 @@ __global__ void __launch_bounds__(128) k_corrector(NetConst C, NetState* S) {
     __shared__ uint32_t s_st;
     __shared__ double s_per;
     __shared__ NbTable nbt;
+    __shared__ double s_seg[kSegShared];
     const CPoint* P = S->contPrev + S->coff_prev[g];
     const int size = S->cn_prev[g];
     if (size < 2) return;
-    double* seg = S->segPrev + S->coff_prev[g];
+    double* seg = size - 1 <= kSegShared ? s_seg : S->segPrev + S->coff_prev[g];
     const Box ib = S->box_prev[g];
     const uint32_t* idl = S->idPrev + S->off_prev[g];
     prepare_sectors(C, S, g, P, size, seg, sec, jw, &s_st, &s_per, nbt);

@@ -44,7 +44,7 @@ __device__ int first_inside_warp(const Field<R>& f, int lane) {
 // are only read where a junction is possible (at most two inside corners).
 template <typename R>
 __device__ void ms_walk(const Field<R>& f, const uint32_t* idl, uint32_t own, int startX, int startY,
-                        ContourOut& o) {
+                        ContourOut& o, double2* xy) {
     o.n = 0;
     o.jn = 0;
     const Box b = f.b;
@@ -143,11 +143,15 @@ __device__ void ms_walk(const Field<R>& f, const uint32_t* idl, uint32_t own, in
                 if (o.n >= o.cap) {
                     o.status |= S_CONTOUR_OVERFLOW;
                 } else {
-                    CPoint& q = o.pts[o.n];
-                    q.x = px;
-                    q.y = py;
-                    q.energy = -1.0;
-                    q.mob = -1.0;
+                    if (xy) {
+                        xy[o.n] = make_double2(px, py);
+                    } else {
+                        CPoint& q = o.pts[o.n];
+                        q.x = px;
+                        q.y = py;
+                        q.energy = -1.0;
+                        q.mob = -1.0;
+                    }
                     if (o.n == 0) {
                         firstx = px;
                         firsty = py;
@@ -212,16 +216,121 @@ __device__ void ms_walk(const Field<R>& f, const uint32_t* idl, uint32_t own, in
         if (o.n >= o.cap) {
             o.status |= S_CONTOUR_OVERFLOW;
         } else {
-            o.pts[o.n] = o.pts[0];
+            if (xy)
+                xy[o.n] = make_double2(firstx, firsty);
+            else
+                o.pts[o.n] = o.pts[0];
             o.n++;
         }
     }
 }
 
-// Contour + junctions of one grain by one warp; returns false if no pixel
-// has phi >= 0.  Junctions are projected one lane per junction.
+// Contour routines over a shared-memory (x, y) buffer: the same operations
+// as project_to_boundary, contour_volume, contour_perimeter and
+// clear_contour_area on CPoint arrays (src/grainBoundary.cpp:201-231, 365-447,
+// src/box.cpp:1888-1906).
+__device__ int project_xy(const double2* P, int asize, double px, double py, double* out_lambda) {
+    double minDist = 1000000.0;
+    int minimal_segment = 0;
+    double dist = 0;
+    int nearest = -1;
+    for (int k = 0; k < asize - 1; k++) {
+        dist = len_sqr(px - P[k].x, py - P[k].y);
+        if (dist < minDist) {
+            nearest = k;
+            minDist = dist;
+            minimal_segment = k;
+        }
+    }
+    double lam_out = *out_lambda;
+    if (nearest < 0) return 0;
+    minDist = 1000000.0;
+    int next = nearest + 1;
+    double ux = P[next].x - P[nearest].x, uy = P[next].y - P[nearest].y;
+    double lambda = (px - P[nearest].x) * ux + (py - P[nearest].y) * uy;
+    lambda /= (ux * ux + uy * uy);
+    if (lambda < 0)
+        dist = len_sqr(px - P[nearest].x, py - P[nearest].y);
+    else if (lambda > 1)
+        dist = len_sqr(P[next].x - px, P[next].y - py);
+    else
+        dist = len_sqr(px - (P[nearest].x + ux * lambda), py - (P[nearest].y + uy * lambda));
+    if (dist < minDist) {
+        minimal_segment = nearest;
+        minDist = dist;
+        lam_out = lambda;
+    }
+    if (nearest == 0) nearest = asize - 1;
+    int previous = nearest - 1;
+    ux = P[nearest].x - P[previous].x;
+    uy = P[nearest].y - P[previous].y;
+    lambda = (px - P[previous].x) * ux + (py - P[previous].y) * uy;
+    lambda /= (ux * ux + uy * uy);
+    if (lambda < 0)
+        dist = len_sqr(px - P[previous].x, py - P[previous].y);
+    else if (lambda > 1)
+        dist = len_sqr(P[nearest].x - px, P[nearest].y - py);
+    else
+        dist = len_sqr(px - (P[previous].x + ux * lambda), py - (P[previous].y + uy * lambda));
+    if (dist < minDist) {
+        minimal_segment = previous;
+        minDist = dist;
+        lam_out = lambda;
+    }
+    if (lam_out > 1) lam_out = 1;
+    if (lam_out < 0) lam_out = 0;
+    *out_lambda = lam_out;
+    return minimal_segment;
+}
+
+__device__ __forceinline__ double volume_xy(const double2* P, int n, double h) {
+    double v = 0;
+    for (int i = 0; i < n - 1; i++) v += (P[i].y + P[i + 1].y) * (P[i].x - P[i + 1].x);
+    return fabs(v) * h * h * 0.5;
+}
+
+__device__ __forceinline__ double perimeter_xy(const double2* P, int n, double h) {
+    double p = 0;
+    for (int i = 0; i < n - 1; i++) {
+        const double dx = P[i].x - P[i + 1].x, dy = P[i].y - P[i + 1].y;
+        p += sqrt(dx * dx + dy * dy) * h;
+    }
+    return p;
+}
+
 template <typename R>
-__device__ bool extract_warp(const Field<R>& f, const uint32_t* idl, uint32_t own, ContourOut& o, int lane) {
+__device__ bool clear_area_xy(R* phi, const Box& b, const double2* P, int n, double h) {
+    if (n == 0) return true;
+    double minx = P[0].x, maxx = P[0].x, miny = P[0].y, maxy = P[0].y;
+    for (int i = 0; i < n; i++) {
+        minx = fmin(minx, P[i].x);
+        maxx = fmax(maxx, P[i].x);
+        miny = fmin(miny, P[i].y);
+        maxy = fmax(maxy, P[i].y);
+    }
+    bool ok = true;
+    for (int i = (int)(miny - 1); i < maxy + 1; i++)
+        for (int j = (int)(minx - 1); j < maxx + 1; j++) {
+            uint32_t k;
+            if (!buf_index(b, i, j, &k)) {
+                ok = false;
+                continue;
+            }
+            if ((double)phi[k] >= 0) phi[k] = (R)(-h);
+        }
+    return ok;
+}
+
+constexpr int kWalkPts = 512;  // shared-memory contour buffer per warp
+
+// Contour + junctions of one grain by one warp; returns false if no pixel
+// has phi >= 0.  The walk writes into the warp's shared buffer xy (or, for a
+// contour longer than the buffer, directly into the global contour);
+// junctions are projected one lane per junction.  On return *in_shared says
+// where the points are.
+template <typename R>
+__device__ bool extract_warp(const Field<R>& f, const uint32_t* idl, uint32_t own, ContourOut& o, int lane,
+                             double2* xy, bool* in_shared) {
     const int start = first_inside_warp(f, lane);
     if (start < 0) {
         o.n = 0;
@@ -229,7 +338,20 @@ __device__ bool extract_warp(const Field<R>& f, const uint32_t* idl, uint32_t ow
         return false;
     }
     const int w = box_w(f.b);
-    if (lane == 0) ms_walk(f, idl, own, f.b.x0 + start % w, f.b.y0 + start / w, o);
+    const int gcap = o.cap;
+    bool shared = true;
+    if (lane == 0) {
+        o.cap = gcap < kWalkPts ? gcap : kWalkPts;
+        ms_walk(f, idl, own, f.b.x0 + start % w, f.b.y0 + start / w, o, xy);
+        if ((o.status & S_CONTOUR_OVERFLOW) && gcap > kWalkPts) {  // long contour: walk again into global memory
+            o.status &= ~S_CONTOUR_OVERFLOW;
+            o.cap = gcap;
+            ms_walk(f, idl, own, f.b.x0 + start % w, f.b.y0 + start / w, o, (double2*)nullptr);
+            shared = false;
+        }
+        o.cap = gcap;
+    }
+    shared = __shfl_sync(0xffffffffu, shared, 0);
     o.n = __shfl_sync(0xffffffffu, o.n, 0);
     o.jn = __shfl_sync(0xffffffffu, o.jn, 0);
     o.status = __shfl_sync(0xffffffffu, o.status, 0);
@@ -237,15 +359,32 @@ __device__ bool extract_warp(const Field<R>& f, const uint32_t* idl, uint32_t ow
     if (o.n >= 2) {
         for (int j = lane; j < o.jn; j += 32) {
             double lambda = 0.0;
-            const int seg = project_to_boundary(o.pts, o.n, o.js[j].x, o.js[j].y, &lambda);
-            const int nx = periodic(seg + 1, o.n);
-            o.js[j].x = o.pts[seg].x + (o.pts[nx].x - o.pts[seg].x) * lambda;
-            o.js[j].y = o.pts[seg].y + (o.pts[nx].y - o.pts[seg].y) * lambda;
+            const int nx_n = o.n;
+            int seg;
+            double sx, sy, tx, ty;
+            if (shared) {
+                seg = project_xy(xy, o.n, o.js[j].x, o.js[j].y, &lambda);
+                const int nx = periodic(seg + 1, nx_n);
+                sx = xy[seg].x;
+                sy = xy[seg].y;
+                tx = xy[nx].x;
+                ty = xy[nx].y;
+            } else {
+                seg = project_to_boundary(o.pts, o.n, o.js[j].x, o.js[j].y, &lambda);
+                const int nx = periodic(seg + 1, nx_n);
+                sx = o.pts[seg].x;
+                sy = o.pts[seg].y;
+                tx = o.pts[nx].x;
+                ty = o.pts[nx].y;
+            }
+            o.js[j].x = sx + (tx - sx) * lambda;
+            o.js[j].y = sy + (ty - sy) * lambda;
             o.js[j].segment = seg;
             o.js[j].lambda = lambda;
         }
     }
     __syncwarp();
+    *in_shared = shared;
     return true;
 }
 
@@ -253,8 +392,10 @@ __device__ bool extract_warp(const Field<R>& f, const uint32_t* idl, uint32_t ow
 // src/box.cpp:1089-1153), one warp per grain.
 template <typename R>
 __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_levelset_w(NetConst C, NetState* S) {
+    __shared__ double2 s_xy[kGrainsPerBlock][kWalkPts];
     const int lane = threadIdx.x & 31;
-    const int g = blockIdx.x * kGrainsPerBlock + (threadIdx.x >> 5) + 1;
+    const int wid = threadIdx.x >> 5;
+    const int g = blockIdx.x * kGrainsPerBlock + wid + 1;
     if (g > C.N || halted(S)) return;
     const int st = C.state[g];
     const Box bc = S->box_cur[g];
@@ -267,29 +408,35 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_levelset_w(NetConst C,
         }
         return;
     }
+    double2* xy = s_xy[wid];
     const int old_len = S->cn_prev[g];
     R* phi = phiA_of<R>(S) + S->off_cur[g];
     Field<R> f{phi, bc};
     const uint32_t* idl = S->idCur + S->off_cur[g];
     ContourOut o{S->contCur + S->coff_cur[g], S->ccap_cur[g], 0, S->jCur + (int64_t)g * C.jmax, C.jmax, 0, 0};
-    bool ok = extract_warp(f, idl, (uint32_t)g, o, lane);
+    bool shared = true;
+    bool ok = extract_warp(f, idl, (uint32_t)g, o, lane, xy, &shared);
     int irregular = 0;
     if (ok) {
         double newVolume = 0;
         bool regular_motion = true;
         if (lane == 0) {
-            newVolume = contour_volume(o.pts, o.n, C.h);
+            newVolume = shared ? volume_xy(xy, o.n, C.h) : contour_volume(o.pts, o.n, C.h);
             regular_motion = motion_regular(old_len, o.n, C.volume[g], newVolume, C.dt, &irregular);
         }
         regular_motion = __shfl_sync(0xffffffffu, regular_motion, 0);
         int tries = 0;
         while (!regular_motion) {  // clear the grain area and extract again (src/box.cpp:1099-1114)
-            if (lane == 0 && !clear_contour_area(phi, bc, o.pts, o.n, C.h)) o.status |= S_INDEX;
+            if (lane == 0) {
+                const bool in_range = shared ? clear_area_xy(phi, bc, xy, o.n, C.h)
+                                             : clear_contour_area(phi, bc, o.pts, o.n, C.h);
+                if (!in_range) o.status |= S_INDEX;
+            }
             __syncwarp();
-            ok = extract_warp(f, idl, (uint32_t)g, o, lane);
+            ok = extract_warp(f, idl, (uint32_t)g, o, lane, xy, &shared);
             if (!ok) break;
             if (lane == 0) {
-                newVolume = contour_volume(o.pts, o.n, C.h);
+                newVolume = shared ? volume_xy(xy, o.n, C.h) : contour_volume(o.pts, o.n, C.h);
                 regular_motion = motion_regular(old_len, o.n, C.volume[g], newVolume, C.dt, &irregular);
                 if (++tries > 64) {
                     o.status |= S_RETRY_LIMIT;
@@ -299,6 +446,18 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_levelset_w(NetConst C,
             regular_motion = __shfl_sync(0xffffffffu, regular_motion, 0);
         }
     }
+    if (ok && shared) {  // publish the contour (energy and mobility still unset, as generatePoint leaves them)
+        for (int i = lane; i < o.n; i += 32) {
+            CPoint q;
+            q.x = xy[i].x;
+            q.y = xy[i].y;
+            q.energy = -1.0;
+            q.mob = -1.0;
+            o.pts[i] = q;
+        }
+    }
+    double perim = 0;
+    if (ok && lane == 0) perim = shared ? perimeter_xy(xy, o.n, C.h) : contour_perimeter(o.pts, o.n, C.h);
     if (lane != 0) return;
     if (o.status) set_status(S, o.status);
     C.regular[g] = 1;
@@ -320,7 +479,7 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_levelset_w(NetConst C,
         nbx = resize_to_square(Box{nb[0], nb[1], nb[2], nb[3]}, C.m);
     }
     S->box_new[g] = nbx;
-    C.perimeter[g] = contour_perimeter(o.pts, o.n, C.h);
+    C.perimeter[g] = perim;
     S->cn_cur[g] = o.n;
     S->jn_cur[g] = o.jn;
 }
@@ -333,14 +492,21 @@ struct PointInfo {
     double len;
 };
 
+constexpr int kNbPts = 512;  // per-warp shared buffers of the neighbour build
+
 // LSbox::computeVolumeAndEnergy + ExplicitGrainBoundary::buildDirectNeighbours
 // (src/box.cpp:1201-1228, src/grainBoundary.cpp:85-199), one warp per grain:
-// lanes probe contour points and evaluate the per-pair physics, lane 0 builds
-// the neighbour list and the sums in contour order.
+// lanes probe contour points, evaluate the per-pair physics and the terms of
+// the area and energy sums into shared memory; lane 0 builds the neighbour
+// list and adds the terms in contour order (the reference's order).
 template <typename R>
 __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_neighbours_w(NetConst C, NetState* S, PointInfo* scratch) {
+    __shared__ int s_cid[kGrainsPerBlock][kNbPts];
+    __shared__ double s_len[kGrainsPerBlock][kNbPts];
+    __shared__ double s_term[kGrainsPerBlock][kNbPts];
     const int lane = threadIdx.x & 31;
-    const int g = blockIdx.x * kGrainsPerBlock + (threadIdx.x >> 5) + 1;
+    const int wid = threadIdx.x >> 5;
+    const int g = blockIdx.x * kGrainsPerBlock + wid + 1;
     if (g > C.N || C.state[g] != G_EXISTS || C.regular[g] == 0 || halted(S)) return;
     const int loop = S->loop;
     CPoint* P = S->contCur + S->coff_cur[g];
@@ -351,7 +517,21 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_neighbours_w(NetConst 
     const R* phi = phiA_of<R>(S) + S->off_cur[g];
     const uint32_t* idl = S->idCur + S->off_cur[g];
     const double* qg = C.quat + 4 * (int64_t)g;
-    // probes, in parallel; the first failing point ends the reference's loop
+    const bool sh = n - 1 <= kNbPts;
+    auto CID = [&](int q) -> int& { return sh ? s_cid[wid][q] : info[q].cid; };
+    auto LEN = [&](int q) -> double& { return sh ? s_len[wid][q] : info[q].len; };
+    auto TERM = [&](int q) -> double& { return sh ? s_term[wid][q] : info[q].theta; };
+    // area terms (computeVolume, src/grainBoundary.cpp:201-213)
+    for (int i = lane; i < n - 1; i += 32) TERM(i) = (P[i].y + P[i + 1].y) * (P[i].x - P[i + 1].x);
+    __syncwarp();
+    double newVolume = 0;
+    if (lane == 0) {
+        double v = 0;
+        for (int i = 0; i < n - 1; i++) v += TERM(i);
+        newVolume = fabs(fabs(v) * h * h * 0.5);
+    }
+    __syncwarp();
+    // probes; the first failing point ends the reference's loop
     int first_bad = 0x7fffffff;
     for (int i = lane; i < n - 1; i += 32) {
         const double px = P[i].x, py = P[i].y;
@@ -375,33 +555,33 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_neighbours_w(NetConst 
             cid = idl[k];
             if (cid != 0 && (cid > (uint32_t)C.N || C.state[cid] == G_GONE)) bad = true;
         }
-        if (bad) {
-            first_bad = min(first_bad, i);
-            info[i].cid = -1;
-            continue;
-        }
-        info[i].cid = (int)cid;
-        const double theta = grain_misorientation(qg, C.quat + 4 * (int64_t)cid);
-        info[i].theta = theta;
-        const double dx = P[i].x - P[i + 1].x, dy = P[i].y - P[i + 1].y;
-        info[i].len = sqrt(dx * dx + dy * dy) * h;
+        CID(i) = bad ? -1 : (int)cid;
+        if (bad) first_bad = min(first_bad, i);
     }
     first_bad = warp_min_i(first_bad);
     const int upto = first_bad < n - 1 ? first_bad : n - 1;
     __syncwarp();
-    for (int i = lane; i < upto; i += 32) {  // points before the first failure get their physics
-        const double theta = info[i].theta;
-        P[i].mob = mobility_model(theta, C);
-        P[i].energy = read_shockley(theta, C);
+    // physics of the points before the first failure; energy terms of all points
+    for (int i = lane; i < n - 1; i += 32) {
+        const double dx = P[i].x - P[i + 1].x, dy = P[i].y - P[i + 1].y;
+        const double len = sqrt(dx * dx + dy * dy);
+        double energy = -1.0;  // generatePoint's value, kept where the loop never reached
+        if (i < upto) {
+            const double theta = grain_misorientation(qg, C.quat + 4 * (int64_t)CID(i));
+            P[i].mob = mobility_model(theta, C);
+            energy = read_shockley(theta, C);
+            P[i].energy = energy;
+            LEN(i) = len * h;
+        }
+        TERM(i) = len * energy * h;
     }
     __syncwarp();
     if (lane != 0) return;
-    const double newVolume = fabs(contour_volume(P, n, h));
     Neighbour* nb = C.nb + (int64_t)g * C.nbmax;
     int nn = 0;
     bool overflow = false;
     for (int i = 0; i < upto; i++) {
-        const int cid = info[i].cid;
+        const int cid = CID(i);
         int e = 0;
         for (; e < nn; ++e)
             if (nb[e].id == cid) break;
@@ -410,14 +590,15 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_neighbours_w(NetConst 
                 overflow = true;
                 continue;
             }
+            const double theta = grain_misorientation(qg, C.quat + 4 * (int64_t)cid);
             nb[nn].id = cid;
             nb[nn].length = 0;
-            nb[nn].energy = P[i].energy;
-            nb[nn].misori = info[i].theta;
-            nb[nn].mobility = P[i].mob;
+            nb[nn].energy = read_shockley(theta, C);
+            nb[nn].misori = theta;
+            nb[nn].mobility = mobility_model(theta, C);
             nn++;
         }
-        nb[e].length += info[i].len;
+        nb[e].length += LEN(i);
     }
     C.nb_n[g] = nn;
     if (overflow) set_status(S, S_NEIGHBOUR_OVERFLOW);
@@ -427,7 +608,9 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_neighbours_w(NetConst 
         P[n - 1].energy = P[0].energy;
         P[n - 1].mob = P[0].mob;
     }
-    C.energy[g] = contour_energy(P, n, h);
+    double energy = 0;
+    for (int i = 0; i < n - 1; i++) energy += TERM(i);
+    C.energy[g] = energy;
     double dA = newVolume - C.volume[g];
     dA = dA / C.dt;
     dA = dA * (3 / kPi);
@@ -520,55 +703,95 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_redistance_w(NetConst 
     const int iymax = (bi.y1 < bo.y1) ? bi.y1 : bo.y1;
 #define GG_IN(i, j) in[(int64_t)((i) - bi.y0) * wi + ((j) - bi.x0)]
 #define GG_OUT(i, j) out[(int64_t)((i) - bo.y0) * wo + ((j) - bo.x0)]
+    // Each sweep is a recurrence along a column or row; the running value is
+    // carried in a register instead of being re-read right after its store.
     for (int j = ixmin + lane; j < bo.x1; j += 32) {
-        for (int i = iymin; i < bo.y1 - 1; i++) {  // y forward
-            R cand;
-            if (j < ixmax && i < iymax - 1) {
-                const R a = GG_IN(i, j), c = GG_IN(i + 1, j);
-                if (a * c <= (R)0.0) {
-                    const R slope = (c - a) / h;
-                    const R dz = -a / slope;
-                    if (fabs(GG_OUT(i, j)) > fabs(dz)) GG_OUT(i, j) = -dz * (R)sgn(slope);
+        if (iymin < bo.y1 - 1) {  // y forward
+            R cur = GG_OUT(iymin, j);
+            for (int i = iymin; i < bo.y1 - 1; i++) {
+                R nxt = GG_OUT(i + 1, j);
+                R cand;
+                if (j < ixmax && i < iymax - 1) {
+                    const R a = GG_IN(i, j), c = GG_IN(i + 1, j);
+                    if (a * c <= (R)0.0) {
+                        const R slope = (c - a) / h;
+                        const R dz = -a / slope;
+                        if (fabs(cur) > fabs(dz)) {
+                            cur = -dz * (R)sgn(slope);
+                            GG_OUT(i, j) = cur;
+                        }
+                    }
+                    cand = cur + ((R)sgn(c) * h);
+                } else {
+                    cand = cur + ((R)sgn(nxt) * h);
                 }
-                cand = GG_OUT(i, j) + ((R)sgn(c) * h);
-            } else {
-                cand = GG_OUT(i, j) + ((R)sgn(GG_OUT(i + 1, j)) * h);
+                if (fabs(cand) < fabs(nxt)) {
+                    nxt = cand;
+                    GG_OUT(i + 1, j) = nxt;
+                }
+                cur = nxt;
             }
-            if (fabs(cand) < fabs(GG_OUT(i + 1, j))) GG_OUT(i + 1, j) = cand;
         }
-        for (int i = iymax - 1; i > bo.y0; i--) {  // y backward
-            R cand;
-            if (j < ixmax && i > iymin)
-                cand = GG_OUT(i, j) + ((R)sgn(GG_IN(i - 1, j)) * h);
-            else
-                cand = GG_OUT(i, j) + ((R)sgn(GG_OUT(i - 1, j)) * h);
-            if (fabs(cand) < fabs(GG_OUT(i - 1, j))) GG_OUT(i - 1, j) = cand;
+        if (iymax - 1 > bo.y0) {  // y backward
+            R cur = GG_OUT(iymax - 1, j);
+            for (int i = iymax - 1; i > bo.y0; i--) {
+                R prv = GG_OUT(i - 1, j);
+                R cand;
+                if (j < ixmax && i > iymin)
+                    cand = cur + ((R)sgn(GG_IN(i - 1, j)) * h);
+                else
+                    cand = cur + ((R)sgn(prv) * h);
+                if (fabs(cand) < fabs(prv)) {
+                    prv = cand;
+                    GG_OUT(i - 1, j) = prv;
+                }
+                cur = prv;
+            }
         }
     }
     __syncwarp();
     for (int i = iymin + lane; i < bo.y1; i += 32) {
-        for (int j = ixmin; j < bo.x1 - 1; j++) {  // x forward
-            R cand;
-            if (j < ixmax - 1 && i < iymax) {
-                const R a = GG_IN(i, j), c = GG_IN(i, j + 1);
-                if (a * c <= (R)0.0) {
-                    const R slope = (c - a) / h;
-                    const R dz = -a / slope;
-                    if (fabs(GG_OUT(i, j)) > fabs(dz)) GG_OUT(i, j) = -dz * (R)sgn(slope);
+        if (ixmin < bo.x1 - 1) {  // x forward
+            R cur = GG_OUT(i, ixmin);
+            for (int j = ixmin; j < bo.x1 - 1; j++) {
+                R nxt = GG_OUT(i, j + 1);
+                R cand;
+                if (j < ixmax - 1 && i < iymax) {
+                    const R a = GG_IN(i, j), c = GG_IN(i, j + 1);
+                    if (a * c <= (R)0.0) {
+                        const R slope = (c - a) / h;
+                        const R dz = -a / slope;
+                        if (fabs(cur) > fabs(dz)) {
+                            cur = -dz * (R)sgn(slope);
+                            GG_OUT(i, j) = cur;
+                        }
+                    }
+                    cand = cur + ((R)sgn(c) * h);
+                } else {
+                    cand = cur + ((R)sgn(nxt) * h);
                 }
-                cand = GG_OUT(i, j) + ((R)sgn(c) * h);
-            } else {
-                cand = GG_OUT(i, j) + ((R)sgn(GG_OUT(i, j + 1)) * h);
+                if (fabs(cand) < fabs(nxt)) {
+                    nxt = cand;
+                    GG_OUT(i, j + 1) = nxt;
+                }
+                cur = nxt;
             }
-            if (fabs(cand) < fabs(GG_OUT(i, j + 1))) GG_OUT(i, j + 1) = cand;
         }
-        for (int j = ixmax - 1; j > bo.x0; j--) {  // x backward
-            R cand;
-            if (j > ixmin && i < iymax)
-                cand = GG_OUT(i, j) + ((R)sgn(GG_IN(i, j - 1)) * h);
-            else
-                cand = GG_OUT(i, j) + (R)sgn(GG_OUT(i, j - 1)) * h;
-            if (fabs(cand) < fabs(GG_OUT(i, j - 1))) GG_OUT(i, j - 1) = cand;
+        if (ixmax - 1 > bo.x0) {  // x backward
+            R cur = GG_OUT(i, ixmax - 1);
+            for (int j = ixmax - 1; j > bo.x0; j--) {
+                R prv = GG_OUT(i, j - 1);
+                R cand;
+                if (j > ixmin && i < iymax)
+                    cand = cur + ((R)sgn(GG_IN(i, j - 1)) * h);
+                else
+                    cand = cur + (R)sgn(prv) * h;
+                if (fabs(cand) < fabs(prv)) {
+                    prv = cand;
+                    GG_OUT(i, j - 1) = prv;
+                }
+                cur = prv;
+            }
         }
     }
 #undef GG_IN
