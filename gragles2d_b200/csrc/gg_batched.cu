@@ -364,7 +364,7 @@ cudaError_t batched_stage_kernel(const NetConst& C, NetState* dS, int which, cud
         case 4: k_levelset_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS); break;
         case 5: k_alloc<<<1, 1024, 0, s>>>(C, dS, 1); break;
         case 6: k_neighbours_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS, reinterpret_cast<PointInfo*>(C.ptinfo)); break;
-        case 7: k_redistance_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS); break;
+        case 7: k_redistance_s<float><<<C.N, kRedistThreads, kRedistSmemBytes, s>>>(C, dS); break;
         default: k_finalize<<<1, 1024, 0, s>>>(C, dS, 1); break;
     }
     return cudaGetLastError();
@@ -386,7 +386,7 @@ cudaError_t batched_stages(const NetConst& C, NetState* dS, int stages, cudaStre
     if (stages & ST_REDIST) {
         k_alloc<<<1, 1024, 0, s>>>(C, dS, 1);
         k_neighbours_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS, reinterpret_cast<PointInfo*>(C.ptinfo));
-        k_redistance_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS);
+        k_redistance_s<float><<<C.N, kRedistThreads, kRedistSmemBytes, s>>>(C, dS);
         k_finalize<<<1, 1024, 0, s>>>(C, dS, 1);
     }
     return cudaGetLastError();

@@ -59,7 +59,7 @@ cudaError_t plain_stage_kernel(const NetConst& C, NetState* dS, int which, cudaS
         case 4: k_levelset_w<double><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS); break;
         case 5: k_alloc<<<1, 1024, 0, s>>>(C, dS, 2); break;
         case 6: k_neighbours_w<double><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS, reinterpret_cast<PointInfo*>(C.ptinfo)); break;
-        case 7: k_redistance_w<double><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS); break;
+        case 7: k_redistance_s<double><<<C.N, kRedistThreads, kRedistSmemBytes, s>>>(C, dS); break;
         default: k_finalize<<<1, 1024, 0, s>>>(C, dS, 1); break;
     }
     return cudaGetLastError();
@@ -89,7 +89,7 @@ cudaError_t plain_stages(const NetConst& C, NetState* dS, int stages, cudaStream
     if (stages & ST_REDIST) {
         k_alloc<<<1, 1024, 0, s>>>(C, dS, 2);
         k_neighbours_w<double><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS, reinterpret_cast<PointInfo*>(C.ptinfo));
-        k_redistance_w<double><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS);
+        k_redistance_s<double><<<C.N, kRedistThreads, kRedistSmemBytes, s>>>(C, dS);
         k_finalize<<<1, 1024, 0, s>>>(C, dS, 1);
     }
     return cudaGetLastError();

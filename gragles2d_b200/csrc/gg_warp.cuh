@@ -576,30 +576,46 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_neighbours_w(NetConst 
         TERM(i) = len * energy * h;
     }
     __syncwarp();
-    if (lane != 0) return;
-    Neighbour* nb = C.nb + (int64_t)g * C.nbmax;
+    // the list is built in shared memory (one entry per distinct neighbour)
+    // and written out once, so lane 0 never re-reads its own global stores
+    __shared__ int s_nid[kGrainsPerBlock][48];
+    __shared__ double s_nlen[kGrainsPerBlock][48];
+    __shared__ int s_first[kGrainsPerBlock][48];
+    const int cap = C.nbmax < 48 ? C.nbmax : 48;
     int nn = 0;
     bool overflow = false;
-    for (int i = 0; i < upto; i++) {
-        const int cid = CID(i);
-        int e = 0;
-        for (; e < nn; ++e)
-            if (nb[e].id == cid) break;
-        if (e == nn) {
-            if (nn >= C.nbmax) {
-                overflow = true;
-                continue;
+    if (lane == 0) {
+        for (int i = 0; i < upto; i++) {
+            const int cid = CID(i);
+            int e = 0;
+            for (; e < nn; ++e)
+                if (s_nid[wid][e] == cid) break;
+            if (e == nn) {
+                if (nn >= cap) {
+                    overflow = true;
+                    continue;
+                }
+                s_nid[wid][nn] = cid;
+                s_nlen[wid][nn] = 0;
+                s_first[wid][nn] = i;
+                nn++;
             }
-            const double theta = grain_misorientation(qg, C.quat + 4 * (int64_t)cid);
-            nb[nn].id = cid;
-            nb[nn].length = 0;
-            nb[nn].energy = read_shockley(theta, C);
-            nb[nn].misori = theta;
-            nb[nn].mobility = mobility_model(theta, C);
-            nn++;
+            s_nlen[wid][e] += LEN(i);
         }
-        nb[e].length += LEN(i);
     }
+    nn = __shfl_sync(0xffffffffu, nn, 0);
+    __syncwarp();
+    Neighbour* nb = C.nb + (int64_t)g * C.nbmax;
+    for (int e = lane; e < nn; e += 32) {
+        const int cid = s_nid[wid][e];
+        const double theta = grain_misorientation(qg, C.quat + 4 * (int64_t)cid);
+        nb[e].id = cid;
+        nb[e].length = s_nlen[wid][e];
+        nb[e].energy = read_shockley(theta, C);
+        nb[e].misori = theta;
+        nb[e].mobility = mobility_model(theta, C);
+    }
+    if (lane != 0) return;
     C.nb_n[g] = nn;
     if (overflow) set_status(S, S_NEIGHBOUR_OVERFLOW);
     if (first_bad < n - 1) {
@@ -624,13 +640,16 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_neighbours_w(NetConst 
 // grain: candidates of each member's list are tested across lanes and the
 // accepted ones appended in list order.
 __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_second_order_w(NetConst C, NetState* S) {
+    constexpr int kL = 128;
+    __shared__ int s_list[kGrainsPerBlock][kL];
     const int lane = threadIdx.x & 31;
-    const int g = blockIdx.x * kGrainsPerBlock + (threadIdx.x >> 5) + 1;
+    const int wid = threadIdx.x >> 5;
+    const int g = blockIdx.x * kGrainsPerBlock + wid + 1;
     if (g > C.N || C.state[g] != G_EXISTS) return;
-    const int K = C.kmax;
-    const int* sec = C.sec_ids + (int64_t)g * K;
+    const int K = C.kmax < kL ? C.kmax : kL;
+    const int* sec = C.sec_ids + (int64_t)g * C.kmax;
     const int ns = C.sec_n[g];
-    int* cmp = C.cmp_ids + (int64_t)g * K;
+    int* list = s_list[wid];
     const unsigned lt = (1u << lane) - 1u;
     int nc = 0;
     bool overflow = false;
@@ -640,16 +659,16 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_second_order_w(NetCons
         const unsigned bal = __ballot_sync(0xffffffffu, take);
         if (take) {
             const int pos = nc + __popc(bal & lt);
-            if (pos < K) cmp[pos] = sec[a]; else overflow = true;
+            if (pos < K) list[pos] = sec[a]; else overflow = true;
         }
         nc += __popc(bal);
+        if (nc > K) nc = K;
     }
-    if (nc > K) nc = K;
     __syncwarp();
     const Box mine = S->box_cur[g];
     for (int a = 0; a < ns; ++a) {
         const int id = sec[a];
-        const int* s2 = C.sec_ids + (int64_t)id * K;
+        const int* s2 = C.sec_ids + (int64_t)id * C.kmax;
         const int n2 = C.sec_n[id];
         for (int q0 = 0; q0 < n2; q0 += 32) {
             const int q = q0 + lane;
@@ -657,10 +676,10 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_second_order_w(NetCons
             int c = 0;
             if (q < n2) {
                 c = s2[q];
-                take = C.state[c] == G_EXISTS && boxes_intersect(mine, S->box_cur[c]) && c != g && c != 0;
+                take = C.state[c] == G_EXISTS && c != g && c != 0 && boxes_intersect(mine, S->box_cur[c]);
                 if (take)
                     for (int e = 0; e < nc; ++e)
-                        if (cmp[e] == c) {
+                        if (list[e] == c) {
                             take = false;
                             break;
                         }
@@ -668,44 +687,40 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_second_order_w(NetCons
             const unsigned bal = __ballot_sync(0xffffffffu, take);
             if (take) {
                 const int pos = nc + __popc(bal & lt);
-                if (pos < K) cmp[pos] = c; else overflow = true;
+                if (pos < K) list[pos] = c; else overflow = true;
             }
             nc += __popc(bal);
             if (nc > K) nc = K;
             __syncwarp();
         }
     }
+    int* cmp = C.cmp_ids + (int64_t)g * C.kmax;
+    for (int e = lane; e < nc; e += 32) cmp[e] = list[e];
     if (lane == 0) {
         C.cmp_n[g] = nc;
-        if (overflow) set_status(S, S_LIST_OVERFLOW);
+        if (overflow || C.kmax > kL) set_status(S, overflow ? S_LIST_OVERFLOW : 0u);
     }
 }
 
-// LSbox::executeRedistancing (src/box.cpp:1259-1399), one warp per grain:
-// lanes take columns for the two y sweeps, then rows for the two x sweeps
-// (each column / row is a sequential recurrence, as in the reference).
+// LSbox::executeRedistancing (src/box.cpp:1259-1399): one CTA of 64 threads
+// per grain.  Both boxes are staged in shared memory when they fit (48 KB),
+// so the four sweeps (threads over columns for y, over rows for x; each
+// column / row a sequential recurrence with the running value carried in a
+// register) never wait on global memory; the result is clamped to +-delta
+// and written back coalesced.
+constexpr int kRedistThreads = 64;
+constexpr int kRedistSmemBytes = 48 * 1024;
+
 template <typename R>
-__global__ void __launch_bounds__(32 * kGrainsPerBlock) k_redistance_w(NetConst C, NetState* S) {
-    const int lane = threadIdx.x & 31;
-    const int g = blockIdx.x * kGrainsPerBlock + (threadIdx.x >> 5) + 1;
-    if (g > C.N || C.state[g] != G_EXISTS || halted(S)) return;
-    const R* __restrict__ in = phiA_of<R>(S) + S->off_cur[g];
-    R* __restrict__ out = phiB_of<R>(S) + S->off_new[g];
-    const Box bi = S->box_cur[g], bo = S->box_new[g];
-    const R h = (R)C.h, delta = (R)C.delta;
+__device__ void redistance_sweeps(const R* __restrict__ in, const Box bi, R* __restrict__ out, const Box bo, R h) {
     const int wi = box_w(bi), wo = box_w(bo);
-    const int64_t ao = box_area(bo);
-    for (int64_t p = lane; p < ao; p += 32) out[p] = (R)-1.0;
-    __syncwarp();
     const int ixmin = (bi.x0 < bo.x0) ? bo.x0 : bi.x0;
     const int iymin = (bi.y0 < bo.y0) ? bo.y0 : bi.y0;
     const int ixmax = (bi.x1 < bo.x1) ? bi.x1 : bo.x1;
     const int iymax = (bi.y1 < bo.y1) ? bi.y1 : bo.y1;
 #define GG_IN(i, j) in[(int64_t)((i) - bi.y0) * wi + ((j) - bi.x0)]
 #define GG_OUT(i, j) out[(int64_t)((i) - bo.y0) * wo + ((j) - bo.x0)]
-    // Each sweep is a recurrence along a column or row; the running value is
-    // carried in a register instead of being re-read right after its store.
-    for (int j = ixmin + lane; j < bo.x1; j += 32) {
+    for (int j = ixmin + (int)threadIdx.x; j < bo.x1; j += blockDim.x) {
         if (iymin < bo.y1 - 1) {  // y forward
             R cur = GG_OUT(iymin, j);
             for (int i = iymin; i < bo.y1 - 1; i++) {
@@ -749,8 +764,8 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_redistance_w(NetConst 
             }
         }
     }
-    __syncwarp();
-    for (int i = iymin + lane; i < bo.y1; i += 32) {
+    __syncthreads();
+    for (int i = iymin + (int)threadIdx.x; i < bo.y1; i += blockDim.x) {
         if (ixmin < bo.x1 - 1) {  // x forward
             R cur = GG_OUT(i, ixmin);
             for (int j = ixmin; j < bo.x1 - 1; j++) {
@@ -796,13 +811,35 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_redistance_w(NetConst 
     }
 #undef GG_IN
 #undef GG_OUT
-    __syncwarp();
-    for (int64_t p = lane; p < ao; p += 32) {  // clampValues(-delta, delta)
-        const R v = out[p];
+    __syncthreads();
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kRedistThreads) k_redistance_s(NetConst C, NetState* S) {
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    const int g = blockIdx.x + 1;
+    if (g > C.N || C.state[g] != G_EXISTS || halted(S)) return;
+    const R* in_g = phiA_of<R>(S) + S->off_cur[g];
+    R* out_g = phiB_of<R>(S) + S->off_new[g];
+    const Box bi = S->box_cur[g], bo = S->box_new[g];
+    const R h = (R)C.h, delta = (R)C.delta;
+    const int64_t ai = box_area(bi), ao = box_area(bo);
+    const bool fits = (ai + ao) * (int64_t)sizeof(R) <= kRedistSmemBytes;
+    R* sm = reinterpret_cast<R*>(s_raw);
+    const R* in = fits ? sm : in_g;
+    R* out = fits ? sm + ai : out_g;
+    if (fits)
+        for (int64_t p = threadIdx.x; p < ai; p += blockDim.x) sm[p] = in_g[p];
+    for (int64_t p = threadIdx.x; p < ao; p += blockDim.x) out[p] = (R)-1.0;  // clearValues(-1)
+    __syncthreads();
+    redistance_sweeps<R>(in, bi, out, bo, h);
+    for (int64_t p = threadIdx.x; p < ao; p += blockDim.x) {  // clampValues(-delta, delta)
+        R v = out[p];
         if (v < -delta)
-            out[p] = -delta;
+            v = -delta;
         else if (v > delta)
-            out[p] = delta;
+            v = delta;
+        out_g[p] = v;
     }
 }
 
