@@ -218,6 +218,7 @@ __global__ void __launch_bounds__(128, 6) k_corrector_f(NetConst C, NetState* S)
     __shared__ unsigned short plist[kCorrMaxPix];
     __shared__ int pcount;
     __shared__ double s_seg[kSegShared];
+    __shared__ SegTable stab;
     const CPoint* P = S->contPrev + S->coff_prev[g];
     const int size = S->cn_prev[g];
     if (size < 2) return;
@@ -243,6 +244,9 @@ __global__ void __launch_bounds__(128, 6) k_corrector_f(NetConst C, NetState* S)
         }
     }
     prepare_sectors(C, S, g, P, size, seg, sec, jw, &s_st, &s_per, nbt);
+    const bool tabled = size - 1 <= kSegTable;
+    if (tabled) build_seg_table(sec, seg, size, stab);
+    __syncthreads();
     const Box bo = S->box_cur[g];
     const int x0 = ib.x0 < bo.x0 ? bo.x0 : ib.x0;
     const int y0 = ib.y0 < bo.y0 ? bo.y0 : ib.y0;
@@ -295,24 +299,33 @@ __global__ void __launch_bounds__(128, 6) k_corrector_f(NetConst C, NetState* S)
             segment = project_to_boundary(P, size, (double)j, (double)i, &dl);
             lambda = (float)dl;
         }
-        double weight = 0;
-        bool found = false;
-        for (int q = 0; q < sec.nconst && !found; q++)
-            if (within(sec.cs[q].left, sec.cs[q].right, real, segment)) {
-                weight = sec.cs[q].weight;
-                found = true;
+        int sid = -1;
+        double interpolator = 0;
+        if (tabled) {
+            sid = stab.sector[segment];
+            if (sid <= -2) interpolator = stab.acc[segment];
+        } else {
+            for (int q = 0; q < sec.nconst && sid == -1; q++)
+                if (within(sec.cs[q].left, sec.cs[q].right, real, segment)) sid = q;
+            for (int q = 0; q < sec.ninterp && sid == -1; q++)
+                if (within(sec.is[q].left, sec.is[q].right, real, segment)) sid = -2 - q;
+            if (sid <= -2) {
+                int it = 0;
+                for (int kk = sec.is[-2 - sid].right; kk != segment; kk = wrap_next(kk, real)) {
+                    interpolator += seg[kk];
+                    if (++it > size) break;
+                }
             }
-        for (int q = 0; q < sec.ninterp && !found; q++) {
-            const InterpSector& s = sec.is[q];
-            if (!within(s.left, s.right, real, segment)) continue;
-            double interpolator = 0;
-            int kk = s.right, it = 0;
-            for (; kk != segment; kk = (kk + 1 + real) % real) {
-                interpolator += seg[kk];
-                if (++it > size) break;
-            }
-            const int kn = (kk + 1 + real) % real;
-            const double ax = (P[kn].x - P[kk].x) * lambda, ay = (P[kn].y - P[kk].y) * lambda;
+        }
+        double weight;
+        if (sid >= 0) {
+            weight = sec.cs[sid].weight;
+        } else if (sid == -1) {
+            weight = table_weight_at(nbt, idl, ib, i, j, &st);
+        } else {
+            const InterpSector& s = sec.is[-2 - sid];
+            const int kn = wrap_next(segment, real);
+            const double ax = (P[kn].x - P[segment].x) * lambda, ay = (P[kn].y - P[segment].y) * lambda;
             interpolator += sqrt(ax * ax + ay * ay);
             interpolator /= s.length;
             interpolator = fmin(fmax(interpolator, 0.0), 1.0);
@@ -327,9 +340,7 @@ __global__ void __launch_bounds__(128, 6) k_corrector_f(NetConst C, NetState* S)
             } else {
                 weight = interpolator * s.left_w + (1 - interpolator) * s.right_w;
             }
-            found = true;
         }
-        if (!found) weight = table_weight_at(nbt, idl, ib, i, j, &st);
         out[k] = val + (out[k] - val) * (float)weight;
     }
     if (st) set_status(S, st);

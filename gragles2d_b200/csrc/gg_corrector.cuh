@@ -38,6 +38,17 @@ struct SectorSet {
     InterpSector is[kMaxInterpSectors];
 };
 
+// Per contour segment: the sector getWeight would pick (first constant
+// sector containing it, else first interpolating sector, else none) and, for
+// an interpolating sector, the partial sum of segment lengths from the
+// sector's right point up to the segment, accumulated in the same order as
+// ContourSector::getWeight (src/contourSector.cpp:242-246).
+constexpr int kSegTable = 1024;
+struct SegTable {
+    short sector[kSegTable];  // >= 0 constant, <= -2 interpolating (-2 - q), -1 none
+    double acc[kSegTable];
+};
+
 // characteristics lookup of ExplicitGrainBoundary::getDirectNeighbourCaracteristic
 // (src/grainBoundary.cpp:561-571): by grain ID; a removed grain matches
 // nothing; absent -> default (energy 1, mobility 1).
@@ -303,14 +314,14 @@ __device__ void build_sectors(const NetConst& C, int g, const CPoint* P, const d
             double dist = 0;
             int j = secR.left;
             long it = 0;
-            for (; dist <= C.isr; j = (j + 1 + real) % real) {
+            for (; dist <= C.isr; j = wrap_next(j, real)) {
                 dist += seg[j];
                 if (++it > guard) {
                     S.status |= S_SECTOR_GUARD;
                     break;
                 }
             }
-            nr.left = (j + 1 + real) % real;
+            nr.left = wrap_next(j, real);
             nr.right = secR.left;
             nr.lb = -1;
             nr.rb = iR;
@@ -322,15 +333,15 @@ __device__ void build_sectors(const NetConst& C, int g, const CPoint* P, const d
             double dist = 0;
             int j = secL.right;
             long it = 0;
-            for (; dist <= C.isr; j = (j - 1 + real) % real) {
-                dist += seg[(j - 1 + real) % real];
+            for (; dist <= C.isr; j = wrap_prev(j, real)) {
+                dist += seg[wrap_prev(j, real)];
                 if (++it > guard) {
                     S.status |= S_SECTOR_GUARD;
                     break;
                 }
             }
             nl.left = secL.right;
-            nl.right = (j - 1 + real) % real;
+            nl.right = wrap_prev(j, real);
             nl.lb = iL;
             nl.rb = -1;
             nl.length = dist;
@@ -355,8 +366,8 @@ __device__ void build_sectors(const NetConst& C, int g, const CPoint* P, const d
             r.rb = iR;
             double dist = 0;
             int it = 0;
-            for (int j = r.right; j != r.left; j = (j + 1 + real) % real) {
-                dist += seg[(j - 1 + real) % real];
+            for (int j = r.right; j != r.left; j = wrap_next(j, real)) {
+                dist += seg[wrap_prev(j, real)];
                 if (++it > size + 1) {
                     S.status |= S_SECTOR_GUARD;
                     break;
@@ -396,46 +407,85 @@ __device__ void build_sectors(const NetConst& C, int g, const CPoint* P, const d
     }
 }
 
+__device__ void build_seg_table(const SectorSet& S, const double* seg, int size, SegTable& T) {
+    const int real = size - 1;
+    for (int q = threadIdx.x; q < real; q += blockDim.x) {
+        int sid = -1;
+        for (int c = 0; c < S.nconst; c++)
+            if (within(S.cs[c].left, S.cs[c].right, real, q)) {
+                sid = c;
+                break;
+            }
+        if (sid < 0)
+            for (int c = 0; c < S.ninterp; c++)
+                if (within(S.is[c].left, S.is[c].right, real, q)) {
+                    sid = -2 - c;
+                    break;
+                }
+        T.sector[q] = (short)sid;
+        double acc = 0;
+        if (sid <= -2) {
+            const int k0 = S.is[-2 - sid].right;
+            int it = 0;
+            for (int k = k0; k != q; k = wrap_next(k, real)) {
+                acc += seg[k];
+                if (++it > size) break;
+            }
+        }
+        T.acc[q] = acc;
+    }
+}
+
 // ExplicitGrainBoundary::getWeight (src/grainBoundary.cpp:344-363) for one pixel.
 __device__ __forceinline__ double pixel_weight(const NetConst& C, const NbTable& T, const CPoint* P,
-                                               const double* seg, int size, const SectorSet& S, const uint32_t* idl,
-                                               const Box& ib, int i, int j, uint32_t* status) {
+                                               const double* seg, int size, const SectorSet& S,
+                                               const SegTable* ST, const uint32_t* idl, const Box& ib, int i, int j,
+                                               uint32_t* status) {
     double lambda = 0.0;
     const int segment = project_to_boundary(P, size, (double)j, (double)i, &lambda);
     const int real = size - 1;
-    for (int q = 0; q < S.nconst; q++)
-        if (within(S.cs[q].left, S.cs[q].right, real, segment)) return S.cs[q].weight;
-    for (int q = 0; q < S.ninterp; q++) {
-        const InterpSector& s = S.is[q];
-        if (!within(s.left, s.right, real, segment)) continue;
-        double interpolator = 0;
-        int k = s.right, it = 0;
-        for (; k != segment; k = (k + 1 + real) % real) {
-            interpolator += seg[k];
-            if (++it > size) break;
+    int sid = -1;
+    double interpolator = 0;
+    if (ST) {
+        sid = ST->sector[segment];
+        if (sid <= -2) interpolator = ST->acc[segment];
+    } else {
+        for (int q = 0; q < S.nconst && sid == -1; q++)
+            if (within(S.cs[q].left, S.cs[q].right, real, segment)) sid = q;
+        for (int q = 0; q < S.ninterp && sid == -1; q++)
+            if (within(S.is[q].left, S.is[q].right, real, segment)) sid = -2 - q;
+        if (sid <= -2) {
+            int it = 0;
+            for (int k = S.is[-2 - sid].right; k != segment; k = wrap_next(k, real)) {
+                interpolator += seg[k];
+                if (++it > size) break;
+            }
         }
-        const int kn = (k + 1 + real) % real;
-        const double ax = (P[kn].x - P[k].x) * lambda, ay = (P[kn].y - P[k].y) * lambda;
-        interpolator += sqrt(ax * ax + ay * ay);
-        interpolator /= s.length;
-        if (interpolator < 0) interpolator = 0;
-        if (interpolator > 1) interpolator = 1;
-        if (s.lb >= 0 && s.rb >= 0) {
-            const double isr = C.isr;
-            const double quot = (s.length > 2 * isr ? 2 * isr : s.length);
-            const double amplitude =
-                (s.boundary_w - (s.left_w + s.right_w) / 2) / (2 * isr) * quot + (s.left_w + s.right_w) / 2;
-            const double a0 = 2 * s.right_w;
-            const double a1 = -4 * amplitude;
-            const double a2 = 2 * s.left_w;
-            const double A = a0 + a1 + a2;
-            const double B = -(a0 * 1.5 + a1 + a2 * 0.5);
-            const double Cc = a0 * 0.5;
-            return A * interpolator * interpolator + B * interpolator + Cc;
-        }
-        return interpolator * s.left_w + (1 - interpolator) * s.right_w;
     }
-    return table_weight_at(T, idl, ib, i, j, status);
+    if (sid >= 0) return S.cs[sid].weight;
+    if (sid == -1) return table_weight_at(T, idl, ib, i, j, status);
+    const InterpSector& s = S.is[-2 - sid];
+    const int k = segment;
+    const int kn = wrap_next(k, real);
+    const double ax = (P[kn].x - P[k].x) * lambda, ay = (P[kn].y - P[k].y) * lambda;
+    interpolator += sqrt(ax * ax + ay * ay);
+    interpolator /= s.length;
+    if (interpolator < 0) interpolator = 0;
+    if (interpolator > 1) interpolator = 1;
+    if (s.lb >= 0 && s.rb >= 0) {
+        const double isr = C.isr;
+        const double quot = (s.length > 2 * isr ? 2 * isr : s.length);
+        const double amplitude =
+            (s.boundary_w - (s.left_w + s.right_w) / 2) / (2 * isr) * quot + (s.left_w + s.right_w) / 2;
+        const double a0 = 2 * s.right_w;
+        const double a1 = -4 * amplitude;
+        const double a2 = 2 * s.left_w;
+        const double A = a0 + a1 + a2;
+        const double B = -(a0 * 1.5 + a1 + a2 * 0.5);
+        const double Cc = a0 * 0.5;
+        return A * interpolator * interpolator + B * interpolator + Cc;
+    }
+    return interpolator * s.left_w + (1 - interpolator) * s.right_w;
 }
 
 // Per-grain preparation shared by both correctors: segment lengths (into
@@ -479,6 +529,7 @@ __global__ void __launch_bounds__(128) k_corrector(NetConst C, NetState* S) {
     __shared__ double s_per;
     __shared__ NbTable nbt;
     __shared__ double s_seg[kSegShared];
+    __shared__ SegTable stab;
     const CPoint* P = S->contPrev + S->coff_prev[g];
     const int size = S->cn_prev[g];
     if (size < 2) return;
@@ -486,6 +537,9 @@ __global__ void __launch_bounds__(128) k_corrector(NetConst C, NetState* S) {
     const Box ib = S->box_prev[g];
     const uint32_t* idl = S->idPrev + S->off_prev[g];
     prepare_sectors(C, S, g, P, size, seg, sec, jw, &s_st, &s_per, nbt);
+    const bool tabled = size - 1 <= kSegTable;
+    if (tabled) build_seg_table(sec, seg, size, stab);
+    __syncthreads();
     const Box bo = S->box_cur[g];
     const int x0 = ib.x0 < bo.x0 ? bo.x0 : ib.x0;
     const int y0 = ib.y0 < bo.y0 ? bo.y0 : ib.y0;
@@ -504,7 +558,7 @@ __global__ void __launch_bounds__(128) k_corrector(NetConst C, NetState* S) {
         const int64_t k = (int64_t)(i - bo.y0) * wo + (j - bo.x0);
         const R val = in[k];
         if (val > -delta) {
-            const double weight = pixel_weight(C, nbt, P, seg, size, sec, idl, ib, i, j, &st);
+            const double weight = pixel_weight(C, nbt, P, seg, size, sec, tabled ? &stab : nullptr, idl, ib, i, j, &st);
             out[k] = (R)((double)val + ((double)out[k] - (double)val) * weight * 1.0);
         } else {
             out[k] = -delta;

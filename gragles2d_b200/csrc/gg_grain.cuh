@@ -245,10 +245,22 @@ __device__ bool ms_contour(const Field<R>& f, const uint32_t* idl, uint32_t own,
 __device__ __forceinline__ double len_sqr(double x, double y) { return x * x + y * y; }
 
 // PERIODIC(x) of src/grainBoundary.cpp:26 (size_t arithmetic modulo size-1).
+// The walks only pass x in [-(size-1), 2(size-1)), where a conditional add or
+// subtract gives the same value as the unsigned 64-bit remainder.
 __device__ __forceinline__ int periodic(int x, int size) {
-    const unsigned long long m = (unsigned long long)(size - 1);
-    return (int)(((unsigned long long)(long long)x + m) % m);
+    const int m = size - 1;
+    if (x >= -m && x < 2 * m) {
+        if (x < 0) return x + m;
+        if (x >= m) return x - m;
+        return x;
+    }
+    const unsigned long long mm = (unsigned long long)m;
+    return (int)(((unsigned long long)(long long)x + mm) % mm);
 }
+
+// (j + 1 + real) % real and (j - 1 + real) % real for j in [0, real).
+__device__ __forceinline__ int wrap_next(int j, int real) { return j + 1 >= real ? j + 1 - real : j + 1; }
+__device__ __forceinline__ int wrap_prev(int j, int real) { return j - 1 < 0 ? j - 1 + real : j - 1; }
 
 // ExplicitGrainBoundary::projectToGrainBondary (src/grainBoundary.cpp:365-447)
 __device__ int project_to_boundary(const CPoint* P, int asize, double px, double py, double* out_lambda) {

@@ -321,7 +321,11 @@ __device__ bool clear_area_xy(R* phi, const Box& b, const double2* P, int n, dou
     return ok;
 }
 
-constexpr int kWalkPts = 512;  // shared-memory contour buffer per warp
+constexpr int kWalkPts = 448;  // shared-memory contour buffer per warp
+struct WalkShared;
+template <typename R>
+__device__ int extract_bitmap_warp(const Field<R>& f, const uint32_t* idl, uint32_t own, ContourOut& o, int lane,
+                                   double2* xy, WalkShared& ws);
 
 // Contour + junctions of one grain by one warp; returns false if no pixel
 // has phi >= 0.  The walk writes into the warp's shared buffer xy (or, for a
@@ -330,7 +334,17 @@ constexpr int kWalkPts = 512;  // shared-memory contour buffer per warp
 // where the points are.
 template <typename R>
 __device__ bool extract_warp(const Field<R>& f, const uint32_t* idl, uint32_t own, ContourOut& o, int lane,
-                             double2* xy, bool* in_shared) {
+                             double2* xy, bool* in_shared, WalkShared* ws) {
+    if (ws) {
+        const uint32_t st0 = o.status;
+        const int r = extract_bitmap_warp(f, idl, own, o, lane, xy, *ws);
+        if (r >= 0) {
+            *in_shared = true;
+            return r == 1;
+        }
+        o.status = st0;  // does not fit the shared buffers: walk in global memory
+        o.jn = 0;
+    }
     const int start = first_inside_warp(f, lane);
     if (start < 0) {
         o.n = 0;
@@ -388,11 +402,230 @@ __device__ bool extract_warp(const Field<R>& f, const uint32_t* idl, uint32_t ow
     return true;
 }
 
+constexpr int kBitmapRows = 96;  // bitmap walk for boxes up to 96 x 96
+constexpr int kBitmapWords = 4;
+constexpr int kTrace = 640;  // walk steps recorded per warp
+
+struct WalkShared {
+    uint32_t bm[kBitmapRows * kBitmapWords];
+    uint32_t trace[kTrace];
+};
+
+// Marching squares with the inside/outside decisions taken from a bitmap of
+// the box in shared memory (built with one ballot per 32 pixels), the walk
+// recorded as a trace by lane 0, and the points, junctions and duplicate
+// removal evaluated across the lanes in walk order.  Returns 0 if no pixel
+// is inside, 1 on success, -1 if the box or the walk does not fit the
+// shared buffers (the caller then walks in global memory).
+template <typename R>
+__device__ int extract_bitmap_warp(const Field<R>& f, const uint32_t* idl, uint32_t own, ContourOut& o, int lane,
+                                   double2* xy, WalkShared& ws) {
+    const Box b = f.b;
+    const int w = box_w(b), hgt = box_h(b);
+    if (w > kBitmapWords * 32 || hgt > kBitmapRows) return -1;
+    const int wpr = (w + 31) >> 5;
+    for (int r = 0; r < hgt; ++r)
+        for (int q = 0; q < wpr; ++q) {
+            const int c = q * 32 + lane;
+            const bool in = c < w && (double)f.v[r * w + c] >= 0;
+            const uint32_t word = __ballot_sync(0xffffffffu, in);
+            if (lane == 0) ws.bm[r * wpr + q] = word;
+        }
+    __syncwarp();
+    auto inside = [&](int row, int col) -> bool {
+        if (row < b.y0 || row >= b.y1 || col < b.x0 || col >= b.x1) return false;
+        const int rc = col - b.x0;
+        return (ws.bm[(row - b.y0) * wpr + (rc >> 5)] >> (rc & 31)) & 1u;
+    };
+    // first inside pixel in row-major order
+    int start = -1;
+    for (int q0 = 0; q0 < hgt * wpr; q0 += 32) {
+        const int q = q0 + lane;
+        const uint32_t word = q < hgt * wpr ? ws.bm[q] : 0u;
+        const uint32_t any = __ballot_sync(0xffffffffu, word != 0u);
+        if (any) {
+            const int src = __ffs(any) - 1;
+            const uint32_t wd = __shfl_sync(0xffffffffu, word, src);
+            const int qq = q0 + src;
+            start = (qq / wpr) * w + (qq % wpr) * 32 + (__ffs(wd) - 1);
+            break;
+        }
+    }
+    if (start < 0) {
+        o.n = 0;
+        o.jn = 0;
+        return 0;
+    }
+    const int startX = b.x0 + start % w, startY = b.y0 + start / w;
+    // lane 0: the walk of generateContour (src/marchingSquares.cpp:44-187) on the bitmap
+    int nsteps = 0;
+    uint32_t st = 0;
+    if (lane == 0) {
+        int left = startX - 1, right = startX, top = startY - 1, bottom = startY;
+        int next = MS_NONE, prev = MS_NONE;
+        const long limit = 4L * (w + 2) * (hgt + 2) + 16;
+        long it = 0;
+        do {
+            int mask = 0;
+            if (inside(top, left)) mask |= C_TL;
+            if (inside(top, right)) mask |= C_TR;
+            if (inside(bottom, left)) mask |= C_BL;
+            if (inside(bottom, right)) mask |= C_BR;
+            int emit = 1;
+            switch (mask) {
+                case C_TL: next = MS_UP; break;
+                case C_TR: next = MS_RIGHT; break;
+                case C_TL | C_TR: next = MS_RIGHT; break;
+                case C_BL: next = MS_LEFT; break;
+                case C_BL | C_TL: next = MS_UP; break;
+                case C_BL | C_TR:
+                    next = (prev == MS_UP) ? MS_RIGHT : MS_LEFT;
+                    emit = 0;
+                    break;
+                case C_BL | C_TR | C_TL: next = MS_RIGHT; break;
+                case C_BR: next = MS_DOWN; break;
+                case C_BR | C_TL:
+                    next = (prev == MS_RIGHT) ? MS_DOWN : MS_UP;
+                    emit = 0;
+                    break;
+                case C_BR | C_TR: next = MS_DOWN; break;
+                case C_BR | C_TR | C_TL: next = MS_DOWN; break;
+                case C_BR | C_BL: next = MS_LEFT; break;
+                case C_BR | C_BL | C_TL: next = MS_UP; break;
+                case C_BR | C_BL | C_TR: next = MS_LEFT; break;
+                default: emit = 0; break;
+            }
+            if (nsteps >= kTrace) {
+                nsteps = -1;
+                break;
+            }
+            ws.trace[nsteps++] = (uint32_t)(left - b.x0 + 1) | ((uint32_t)(top - b.y0 + 1) << 10) |
+                                 ((uint32_t)mask << 20) | ((uint32_t)next << 24) | ((uint32_t)emit << 27);
+            switch (next) {
+                case MS_UP: top--; bottom--; break;
+                case MS_DOWN: top++; bottom++; break;
+                case MS_LEFT: left--; right--; break;
+                case MS_RIGHT: left++; right++; break;
+                default: break;
+            }
+            prev = next;
+            if (++it > limit) {
+                st |= S_WALK_LIMIT;
+                break;
+            }
+        } while (left != startX - 1 || bottom != startY);
+    }
+    nsteps = __shfl_sync(0xffffffffu, nsteps, 0);
+    if (nsteps < 0) return -1;
+    o.status |= __shfl_sync(0xffffffffu, st, 0);
+    __syncwarp();
+    // points and junctions of every step, in walk order
+    const unsigned lt = (1u << lane) - 1u;
+    int ne = 0;
+    int jn = 0;
+    bool point_overflow = false;
+    for (int t0 = 0; t0 < nsteps; t0 += 32) {
+        const int t = t0 + lane;
+        bool emit = false, junc = false;
+        double px = 0, py = 0;
+        uint32_t boxes[4] = {0xFFFFFFu, 0xFFFFFFu, 0xFFFFFFu, 0xFFFFFFu};
+        int order = 0, left = 0, top = 0;
+        if (t < nsteps) {
+            const uint32_t e = ws.trace[t];
+            left = (int)(e & 1023u) - 1 + b.x0;
+            top = (int)((e >> 10) & 1023u) - 1 + b.y0;
+            const int mask = (int)((e >> 20) & 15u);
+            const int next = (int)((e >> 24) & 7u);
+            emit = (e >> 27) & 1u;
+            const int right = left + 1, bottom = top + 1;
+            if (emit) ms_point(f, next, top, bottom, left, right, &px, &py);
+            if (__popc(mask) < 3 && bottom >= b.y0 && bottom < b.y1 && top >= b.y0 && top < b.y1 &&
+                left >= b.x0 && left < b.x1 && right >= b.x0 && right < b.x1) {  // generateJunction
+                insert_distinct((mask & C_BL) ? own : idl[(bottom - b.y0) * w + (left - b.x0)], boxes, order);
+                insert_distinct((mask & C_TL) ? own : idl[(top - b.y0) * w + (left - b.x0)], boxes, order);
+                insert_distinct((mask & C_BR) ? own : idl[(bottom - b.y0) * w + (right - b.x0)], boxes, order);
+                insert_distinct((mask & C_TR) ? own : idl[(top - b.y0) * w + (right - b.x0)], boxes, order);
+                junc = order > 2;
+            }
+        }
+        const uint32_t eb = __ballot_sync(0xffffffffu, emit);
+        if (emit) {
+            const int pos = ne + __popc(eb & lt);
+            if (pos < kWalkPts)
+                xy[pos] = make_double2(px, py);
+            else
+                point_overflow = true;
+        }
+        ne += __popc(eb);
+        const uint32_t jb = __ballot_sync(0xffffffffu, junc);
+        if (junc) {
+            const int pos = jn + __popc(jb & lt);
+            if (pos < o.jcap) {
+                Junction& j = o.js[pos];
+                j.type = order;
+                for (int q = 0; q < 4; ++q) j.grains[q] = q < order ? boxes[q] : 0xFFFFFFFFu;
+                j.segment = -1;
+                j.lambda = 0;
+                j.x = left + 0.5;
+                j.y = top + 0.5;
+            } else {
+                o.status |= S_JUNCTION_OVERFLOW;
+            }
+        }
+        jn += __popc(jb);
+    }
+    if (__any_sync(0xffffffffu, point_overflow)) return -1;
+    o.jn = jn < o.jcap ? jn : o.jcap;
+    __syncwarp();
+    // insertPoint's duplicate test: a candidate equal to its predecessor is dropped
+    int n = 0;
+    for (int i0 = 0; i0 < ne; i0 += 32) {
+        const int i = i0 + lane;
+        double2 pnt = make_double2(0, 0);
+        bool keep = false;
+        if (i < ne) {
+            pnt = xy[i];
+            keep = i == 0 || pnt.x != xy[i - 1].x || pnt.y != xy[i - 1].y;
+        }
+        __syncwarp();
+        const uint32_t kb = __ballot_sync(0xffffffffu, keep);
+        if (keep) xy[n + __popc(kb & lt)] = pnt;
+        n += __popc(kb);
+        __syncwarp();
+    }
+    const int cap = o.cap < kWalkPts ? o.cap : kWalkPts;
+    if (n > 0 && (xy[0].x != xy[n - 1].x || xy[0].y != xy[n - 1].y)) {  // close the loop
+        if (lane == 0 && n < kWalkPts) xy[n] = xy[0];
+        n++;
+    }
+    if (n > cap) {
+        o.status |= S_CONTOUR_OVERFLOW;
+        n = cap;
+    }
+    o.n = n;
+    __syncwarp();
+    // junctions projected onto the contour (extractBoundaryAndJunctions, src/grainBoundary.cpp:51-61)
+    if (n >= 2) {
+        for (int j = lane; j < o.jn; j += 32) {
+            double lambda = 0.0;
+            const int seg = project_xy(xy, n, o.js[j].x, o.js[j].y, &lambda);
+            const int nx = periodic(seg + 1, n);
+            o.js[j].x = xy[seg].x + (xy[nx].x - xy[seg].x) * lambda;
+            o.js[j].y = xy[seg].y + (xy[nx].y - xy[seg].y) * lambda;
+            o.js[j].segment = seg;
+            o.js[j].lambda = lambda;
+        }
+    }
+    __syncwarp();
+    return 1;
+}
+
 // grainhdl::level_set -> LSbox::extractContour (src/grainhdl.cpp:830-848,
 // src/box.cpp:1089-1153), one warp per grain.
 template <typename R>
 __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_levelset_w(NetConst C, NetState* S) {
     __shared__ double2 s_xy[kGrainsPerBlock][kWalkPts];
+    __shared__ WalkShared s_walk[kGrainsPerBlock];
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;
     const int g = blockIdx.x * kGrainsPerBlock + wid + 1;
@@ -415,7 +648,7 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_levelset_w(NetConst C,
     const uint32_t* idl = S->idCur + S->off_cur[g];
     ContourOut o{S->contCur + S->coff_cur[g], S->ccap_cur[g], 0, S->jCur + (int64_t)g * C.jmax, C.jmax, 0, 0};
     bool shared = true;
-    bool ok = extract_warp(f, idl, (uint32_t)g, o, lane, xy, &shared);
+    bool ok = extract_warp(f, idl, (uint32_t)g, o, lane, xy, &shared, &s_walk[wid]);
     int irregular = 0;
     if (ok) {
         double newVolume = 0;
@@ -433,7 +666,7 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_levelset_w(NetConst C,
                 if (!in_range) o.status |= S_INDEX;
             }
             __syncwarp();
-            ok = extract_warp(f, idl, (uint32_t)g, o, lane, xy, &shared);
+            ok = extract_warp(f, idl, (uint32_t)g, o, lane, xy, &shared, &s_walk[wid]);
             if (!ok) break;
             if (lane == 0) {
                 newVolume = shared ? volume_xy(xy, o.n, C.h) : contour_volume(o.pts, o.n, C.h);
@@ -703,13 +936,14 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_second_order_w(NetCons
 }
 
 // LSbox::executeRedistancing (src/box.cpp:1259-1399): one CTA of 64 threads
-// per grain.  Both boxes are staged in shared memory when they fit (48 KB),
-// so the four sweeps (threads over columns for y, over rows for x; each
-// column / row a sequential recurrence with the running value carried in a
-// register) never wait on global memory; the result is clamped to +-delta
-// and written back coalesced.
+// per grain.  The output box is built in shared memory when it fits (16 KB,
+// small enough for many grains per SM), so the four sweeps (threads over
+// columns for y, over rows for x; each column / row a sequential recurrence
+// with the running value carried in a register) never re-read global stores;
+// the input box is read through L1; the result is clamped to +-delta and
+// written back coalesced.
 constexpr int kRedistThreads = 64;
-constexpr int kRedistSmemBytes = 48 * 1024;
+constexpr int kRedistSmemBytes = 16 * 1024;
 
 template <typename R>
 __device__ void redistance_sweeps(const R* __restrict__ in, const Box bi, R* __restrict__ out, const Box bo, R h) {
@@ -823,16 +1057,12 @@ __global__ void __launch_bounds__(kRedistThreads) k_redistance_s(NetConst C, Net
     R* out_g = phiB_of<R>(S) + S->off_new[g];
     const Box bi = S->box_cur[g], bo = S->box_new[g];
     const R h = (R)C.h, delta = (R)C.delta;
-    const int64_t ai = box_area(bi), ao = box_area(bo);
-    const bool fits = (ai + ao) * (int64_t)sizeof(R) <= kRedistSmemBytes;
-    R* sm = reinterpret_cast<R*>(s_raw);
-    const R* in = fits ? sm : in_g;
-    R* out = fits ? sm + ai : out_g;
-    if (fits)
-        for (int64_t p = threadIdx.x; p < ai; p += blockDim.x) sm[p] = in_g[p];
+    const int64_t ao = box_area(bo);
+    const bool fits = ao * (int64_t)sizeof(R) <= kRedistSmemBytes;
+    R* out = fits ? reinterpret_cast<R*>(s_raw) : out_g;
     for (int64_t p = threadIdx.x; p < ao; p += blockDim.x) out[p] = (R)-1.0;  // clearValues(-1)
     __syncthreads();
-    redistance_sweeps<R>(in, bi, out, bo, h);
+    redistance_sweeps<R>(in_g, bi, out, bo, h);
     for (int64_t p = threadIdx.x; p < ao; p += blockDim.x) {  // clampValues(-delta, delta)
         R v = out[p];
         if (v < -delta)
