@@ -6,7 +6,7 @@ C++ (``oracle/_ref/gg_ref``, built by ``make -C oracle ref`` from the
 reference sources) after initialisation and after selected steps, gzipped.
 
 Run from the repository root in the build container (it needs the reference
-tree to build the oracle):  python tests/golden/make_golden.py
+tree to build the oracle):  python tests/golden/make_golden.py [case ...]
 """
 from __future__ import annotations
 
@@ -32,6 +32,9 @@ CASES = {
     "rs_v30": ("voronoi", 30, 120, 2, 20, 5, {"IsIsotropicNetwork": 0}),
     "mob_v30": ("voronoi", 30, 120, 3, 20, 5,
                 {"IsIsotropicNetwork": 0, "UseMobilityModel": 1, "TriplePointDrag": 5.0}),
+    # every step dumped: the per-routine restatement in oracle/gg_oracle.c is
+    # checked on each consecutive pair of records
+    "seq_v24": ("voronoi", 24, 100, 5, 6, 1, {"IsIsotropicNetwork": 1}),
 }
 
 
@@ -59,8 +62,9 @@ def make_case(name: str, spec) -> dict:
 def main():
     if not os.path.exists(GG_REF):
         subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
-    for name, spec in CASES.items():
-        info = make_case(name, spec)
+    names = sys.argv[1:] or list(CASES)
+    for name in names:
+        info = make_case(name, CASES[name])
         print(name, info)
 
 
