@@ -121,57 +121,130 @@ size_t conv_sep_smem(int tmax) {
     return sizeof(float) * (size_t)(2 * n * n + 2 * kSepSmemMaxN + kSepStrip + 2);
 }
 
-// Batched-form corrector: same sectors and weights as k_corrector, with the
-// previous contour staged in shared memory (FP32 coordinates), junction
-// weights computed one thread per junction, and the per-pixel projection in
-// FP32.
+// Batched-form corrector: same sectors as k_corrector (built by one warp),
+// with the previous contour staged in shared memory (FP32 coordinates) and
+// the per-pixel work in FP32.  Each warp takes one 8 x 4 tile of the box at a
+// time, so its 32 pixels lie close together and the warp prunes the
+// nearest-vertex search as one: chunks of 8 contour points whose bounding box
+// is farther from the tile than every lane's best point so far are skipped
+// by all lanes together.
 constexpr int kCorrMaxPts = 1024;
-constexpr int kCorrMaxPix = 4096;  // compacted pixel list (boxes up to 64 x 64)
 
 constexpr int kChunk = 8;  // contour points per bounding box of the nearest-vertex search
 
-// projectToGrainBondary (src/grainBoundary.cpp:365-447) in FP32 over the
-// staged contour.  The nearest-vertex scan skips every run of 8 consecutive
-// points whose bounding box is farther than the best point found so far
-// (runs are visited in index order, so ties still go to the first point).
-__device__ __forceinline__ int project_f(const float2* P, const float4* cbb, int asize, float px, float py,
-                                         float* out_lambda) {
-    float minDist = 3.0e38f;
-    int nearest = -1;
+// Slack on the chunk bound so that a box distance which rounds a little
+// above an equal point distance does not drop the chunk (ties matter).
+constexpr float kBoundSlack = 1.0000005f;
+
+// Packed FP32 pairs (sm_100 f32x2 arithmetic): two contour points per
+// instruction in the nearest-vertex scan.
+__device__ __forceinline__ unsigned long long f2_pack(float a, float b) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void f2_unpack(unsigned long long v, float& a, float& b) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long f2_sub(unsigned long long a, unsigned long long b) {
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ unsigned long long f2_mul(unsigned long long a, unsigned long long b) {
+    unsigned long long r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ unsigned long long f2_fma(unsigned long long a, unsigned long long b,
+                                                     unsigned long long c) {
+    unsigned long long r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+
+// projectToGrainBondary (src/grainBoundary.cpp:365-447) in FP32 for the
+// pixels (px, py) of the 32 lanes of a warp (all lanes call it; `valid` lanes
+// are the warp's real pixels, the others only follow along).  The nearest
+// vertex of each lane is the first one at the smallest distance: chunks are
+// visited out of index order (first the chunk `*wseed` that held the nearest
+// vertex of the warp's previous tile, then the others that the bound does
+// not rule out), comparing (distance, index) pairs.  P holds the contour with
+// a 16-byte aligned start, two points per float4.
+__device__ __forceinline__ int project_warp(const float2* P, const float4* cbb, int asize, int px, int py,
+                                            bool valid, float* out_lambda, int* wseed) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const float fx = (float)px, fy = (float)py;
+    const unsigned long long FX = f2_pack(fx, fx), FY = f2_pack(fy, fy);
     const int npts = asize - 1;
     const int nch = (npts + kChunk - 1) / kChunk;
-    for (int ch = 0; ch < nch; ++ch) {
-        const float4 b = cbb[ch];
-        const float bx = fmaxf(fmaxf(b.x - px, px - b.y), 0.f);
-        const float by = fmaxf(fmaxf(b.z - py, py - b.w), 0.f);
-        if (bx * bx + by * by > minDist) continue;
-        const int k1 = min(ch * kChunk + kChunk, npts);
-        for (int k = ch * kChunk; k < k1; k++) {
-            const float dx = px - P[k].x, dy = py - P[k].y;
-            const float d = dx * dx + dy * dy;
-            if (d < minDist) {
-                nearest = k;
-                minDist = d;
-            }
+    const float4* P2 = reinterpret_cast<const float4*>(P);
+    float best = 3.0e38f;
+    int nearest = -1;
+    auto take = [&](float d, int k) {
+        if (d < best || (d == best && k < nearest)) {
+            nearest = k;
+            best = d;
         }
+    };
+    auto scan = [&](int ch) {
+        const int k0 = ch * kChunk, k1 = min(k0 + kChunk, npts);
+        for (int k = k0; k < k1; k += 2) {
+            const float4 v = P2[k >> 1];
+            const unsigned long long DX = f2_sub(FX, f2_pack(v.x, v.z)), DY = f2_sub(FY, f2_pack(v.y, v.w));
+            float d0, d1;
+            f2_unpack(f2_fma(DY, DY, f2_mul(DX, DX)), d0, d1);
+            take(d0, k);
+            if (k + 1 < k1) take(d1, k + 1);
+        }
+    };
+    const int sc = *wseed < nch ? *wseed : 0;
+    scan(sc);
+    const int bx0 = __reduce_min_sync(FULL, valid ? px : INT_MAX), bx1 = __reduce_max_sync(FULL, valid ? px : INT_MIN);
+    const int by0 = __reduce_min_sync(FULL, valid ? py : INT_MAX), by1 = __reduce_max_sync(FULL, valid ? py : INT_MIN);
+    float U = __uint_as_float(__reduce_max_sync(FULL, valid ? __float_as_uint(best) : 0u));
+    for (int c0 = 0; c0 < nch; c0 += 32) {
+        const int ch = c0 + lane;
+        float lb = 3.0e38f;
+        if (ch < nch) {
+            const float4 b = cbb[ch];
+            const float gx = fmaxf(fmaxf(b.x - (float)bx1, (float)bx0 - b.y), 0.f);
+            const float gy = fmaxf(fmaxf(b.z - (float)by1, (float)by0 - b.w), 0.f);
+            lb = gx * gx + gy * gy;
+        }
+        unsigned mask = __ballot_sync(FULL, ch < nch && ch != sc && lb <= U * kBoundSlack);
+        while (mask) {
+            const int bit = __ffs(mask) - 1;
+            mask &= mask - 1;
+            const float lbc = __shfl_sync(FULL, lb, bit);
+            if (lbc > U * kBoundSlack) continue;
+            scan(c0 + bit);
+            U = __uint_as_float(__reduce_max_sync(FULL, valid ? __float_as_uint(best) : 0u));
+        }
+    }
+    {
+        const int src = __ffs(__ballot_sync(FULL, valid)) - 1;
+        const int sn = __shfl_sync(FULL, nearest, src < 0 ? 0 : src);
+        if (sn >= 0) *wseed = sn / kChunk;
     }
     if (nearest < 0) return 0;
     float lam_out = 0.f;
     int seg = nearest;
-    minDist = 1e30f;
+    float minDist = 1e30f;
     {
         const int next = nearest + 1;
         const float ux = P[next].x - P[nearest].x, uy = P[next].y - P[nearest].y;
-        float lambda = ((px - P[nearest].x) * ux + (py - P[nearest].y) * uy) / (ux * ux + uy * uy);
+        float lambda = ((fx - P[nearest].x) * ux + (fy - P[nearest].y) * uy) / (ux * ux + uy * uy);
         float d;
         if (lambda < 0) {
-            const float dx = px - P[nearest].x, dy = py - P[nearest].y;
+            const float dx = fx - P[nearest].x, dy = fy - P[nearest].y;
             d = dx * dx + dy * dy;
         } else if (lambda > 1) {
-            const float dx = P[next].x - px, dy = P[next].y - py;
+            const float dx = P[next].x - fx, dy = P[next].y - fy;
             d = dx * dx + dy * dy;
         } else {
-            const float dx = px - (P[nearest].x + ux * lambda), dy = py - (P[nearest].y + uy * lambda);
+            const float dx = fx - (P[nearest].x + ux * lambda), dy = fy - (P[nearest].y + uy * lambda);
             d = dx * dx + dy * dy;
         }
         if (d < minDist) {
@@ -180,20 +253,20 @@ __device__ __forceinline__ int project_f(const float2* P, const float4* cbb, int
             lam_out = lambda;
         }
     }
-    int nb = nearest == 0 ? asize - 1 : nearest;
+    const int nb = nearest == 0 ? asize - 1 : nearest;
     {
         const int prev = nb - 1;
         const float ux = P[nb].x - P[prev].x, uy = P[nb].y - P[prev].y;
-        float lambda = ((px - P[prev].x) * ux + (py - P[prev].y) * uy) / (ux * ux + uy * uy);
+        float lambda = ((fx - P[prev].x) * ux + (fy - P[prev].y) * uy) / (ux * ux + uy * uy);
         float d;
         if (lambda < 0) {
-            const float dx = px - P[prev].x, dy = py - P[prev].y;
+            const float dx = fx - P[prev].x, dy = fy - P[prev].y;
             d = dx * dx + dy * dy;
         } else if (lambda > 1) {
-            const float dx = P[nb].x - px, dy = P[nb].y - py;
+            const float dx = P[nb].x - fx, dy = P[nb].y - fy;
             d = dx * dx + dy * dy;
         } else {
-            const float dx = px - (P[prev].x + ux * lambda), dy = py - (P[prev].y + uy * lambda);
+            const float dx = fx - (P[prev].x + ux * lambda), dy = fy - (P[prev].y + uy * lambda);
             d = dx * dx + dy * dy;
         }
         if (d < minDist) {
@@ -209,16 +282,15 @@ __global__ void __launch_bounds__(128, 6) k_corrector_f(NetConst C, NetState* S)
     const int g = blockIdx.x + 1;
     if (g > C.N || C.state[g] != G_EXISTS || C.regular[g] == 0 || S->loop == 0 || halted(S)) return;
     __shared__ SectorSet sec;
-    __shared__ float2 sp[kCorrMaxPts];
+    __shared__ __align__(16) float2 sp[kCorrMaxPts];
     __shared__ double jw[64];
     __shared__ uint32_t s_st;
     __shared__ double s_per;
     __shared__ NbTable nbt;
     __shared__ float4 cbb[kCorrMaxPts / kChunk];
-    __shared__ unsigned short plist[kCorrMaxPix];
-    __shared__ int pcount;
     __shared__ double s_seg[kSegShared];
     __shared__ SegTable stab;
+    __shared__ int jl[64], jr[64];
     const CPoint* P = S->contPrev + S->coff_prev[g];
     const int size = S->cn_prev[g];
     if (size < 2) return;
@@ -228,7 +300,6 @@ __global__ void __launch_bounds__(128, 6) k_corrector_f(NetConst C, NetState* S)
     const bool staged = size <= kCorrMaxPts;
     if (staged)
         for (int k = threadIdx.x; k < size; k += blockDim.x) sp[k] = make_float2((float)P[k].x, (float)P[k].y);
-    if (threadIdx.x == 0) pcount = 0;
     __syncthreads();
     if (staged) {
         const int npts = size - 1, nch = (npts + kChunk - 1) / kChunk;
@@ -243,7 +314,7 @@ __global__ void __launch_bounds__(128, 6) k_corrector_f(NetConst C, NetState* S)
             cbb[ch] = b;
         }
     }
-    prepare_sectors(C, S, g, P, size, seg, sec, jw, &s_st, &s_per, nbt);
+    prepare_sectors(C, S, g, P, size, seg, sec, jw, &s_st, &s_per, nbt, jl, jr);
     const bool tabled = size - 1 <= kSegTable;
     if (tabled) build_seg_table(sec, seg, size, stab);
     __syncthreads();
@@ -253,95 +324,98 @@ __global__ void __launch_bounds__(128, 6) k_corrector_f(NetConst C, NetState* S)
     const int x1 = ib.x1 > bo.x1 ? bo.x1 : ib.x1;
     const int y1 = ib.y1 > bo.y1 ? bo.y1 : ib.y1;
     if (x1 <= x0 || y1 <= y0) return;
-    const int w = x1 - x0;
-    const int cnt = w * (y1 - y0);
+    const int w = x1 - x0, hgt = y1 - y0;
     const float* in = reinterpret_cast<const float*>(S->phiA) + S->off_cur[g];
     float* out = reinterpret_cast<float*>(S->phiB) + S->off_cur[g];
-    const int wo = box_w(bo);
+    const int wo = box_w(bo), wi = box_w(ib);
     const float delta = (float)C.delta;
     const int real = size - 1;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int ntx = (w + 7) >> 3, ntiles = ntx * ((hgt + 3) >> 2);
     uint32_t st = 0;
-    // pixels at or below -delta are set to -delta; the others are compacted
-    // into a list so every lane of a warp projects a pixel
-    const bool compact = cnt <= kCorrMaxPix;
-    for (int p0 = 0; p0 < cnt; p0 += blockDim.x) {
-        const int p = p0 + threadIdx.x;
-        bool active = false;
-        if (p < cnt) {
-            const int i = y0 + p / w, j = x0 + p % w;
-            const int k = (i - bo.y0) * wo + (j - bo.x0);
-            active = in[k] > -delta;
-            if (!active) out[k] = -delta;
-        }
-        if (compact) {
-            const int lane = threadIdx.x & 31;
-            const unsigned bal = __ballot_sync(0xffffffffu, active);
-            int base = 0;
-            if (lane == 0 && bal) base = atomicAdd(&pcount, __popc(bal));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (active) plist[base + __popc(bal & ((1u << lane) - 1u))] = (unsigned short)p;
-        }
-    }
-    __syncthreads();
-    const int total = compact ? pcount : cnt;
-    for (int q = threadIdx.x; q < total; q += blockDim.x) {
-        const int p = compact ? (int)plist[q] : q;
-        const int i = y0 + p / w, j = x0 + p % w;
+    int wseed = 0;
+    // one warp per 8 x 4 tile; pixels at or below -delta are set to -delta
+    for (int t = warp; t < ntiles; t += nwarps) {
+        const int x = (t % ntx) * 8 + (lane & 7), y = (t / ntx) * 4 + (lane >> 3);
+        const bool inside = x < w && y < hgt;
+        const int i = y0 + y, j = x0 + x;
         const int k = (i - bo.y0) * wo + (j - bo.x0);
-        const float val = in[k];
-        if (!compact && !(val > -delta)) continue;
+        float val = 0.f, conv = 0.f;
+        uint32_t id = 0;
+        if (inside) {
+            val = __ldg(in + k);
+            conv = out[k];
+            id = idl[(i - ib.y0) * wi + (j - ib.x0)];
+        }
+        const bool valid = inside && val > -delta;
+        if (inside && !valid) out[k] = -delta;
+        if (__ballot_sync(0xffffffffu, valid) == 0u) continue;
         float lambda = 0.f;
         int segment;
         if (staged) {
-            segment = project_f(sp, cbb, size, (float)j, (float)i, &lambda);
+            segment = project_warp(sp, cbb, size, j, i, valid, &lambda, &wseed);
         } else {
             double dl = 0;
             segment = project_to_boundary(P, size, (double)j, (double)i, &dl);
             lambda = (float)dl;
         }
+        if (!valid) continue;
         int sid = -1;
-        double interpolator = 0;
+        float interpolator = 0.f;
         if (tabled) {
             sid = stab.sector[segment];
-            if (sid <= -2) interpolator = stab.acc[segment];
+            if (sid <= -2) interpolator = (float)stab.acc[segment];
         } else {
-            for (int q = 0; q < sec.nconst && sid == -1; q++)
-                if (within(sec.cs[q].left, sec.cs[q].right, real, segment)) sid = q;
-            for (int q = 0; q < sec.ninterp && sid == -1; q++)
-                if (within(sec.is[q].left, sec.is[q].right, real, segment)) sid = -2 - q;
+            for (int c = 0; c < sec.nconst && sid == -1; c++)
+                if (within(sec.cs[c].left, sec.cs[c].right, real, segment)) sid = c;
+            for (int c = 0; c < sec.ninterp && sid == -1; c++)
+                if (within(sec.is[c].left, sec.is[c].right, real, segment)) sid = -2 - c;
             if (sid <= -2) {
                 int it = 0;
                 for (int kk = sec.is[-2 - sid].right; kk != segment; kk = wrap_next(kk, real)) {
-                    interpolator += seg[kk];
+                    interpolator += (float)seg[kk];
                     if (++it > size) break;
                 }
             }
         }
-        double weight;
+        float weight;
         if (sid >= 0) {
-            weight = sec.cs[sid].weight;
+            weight = (float)sec.cs[sid].weight;
         } else if (sid == -1) {
-            weight = table_weight_at(nbt, idl, ib, i, j, &st);
+            // getGBEnergyTimesGBMobility(i, j) through the neighbour table
+            weight = 1.f;
+            for (int e = 0; e < nbt.n; ++e)
+                if (nbt.id[e] == (int)id) {
+                    weight = (float)nbt.w[e];
+                    break;
+                }
         } else {
             const InterpSector& s = sec.is[-2 - sid];
             const int kn = wrap_next(segment, real);
-            const double ax = (P[kn].x - P[segment].x) * lambda, ay = (P[kn].y - P[segment].y) * lambda;
-            interpolator += sqrt(ax * ax + ay * ay);
-            interpolator /= s.length;
-            interpolator = fmin(fmax(interpolator, 0.0), 1.0);
+            float ax, ay;
+            if (staged) {
+                ax = (sp[kn].x - sp[segment].x) * lambda;
+                ay = (sp[kn].y - sp[segment].y) * lambda;
+            } else {
+                ax = (float)((P[kn].x - P[segment].x) * lambda);
+                ay = (float)((P[kn].y - P[segment].y) * lambda);
+            }
+            interpolator += sqrtf(ax * ax + ay * ay);
+            interpolator /= (float)s.length;
+            interpolator = fminf(fmaxf(interpolator, 0.f), 1.f);
+            const float lw = (float)s.left_w, rw = (float)s.right_w;
             if (s.lb >= 0 && s.rb >= 0) {
-                const double isr = C.isr;
-                const double quot = (s.length > 2 * isr ? 2 * isr : s.length);
-                const double amplitude =
-                    (s.boundary_w - (s.left_w + s.right_w) / 2) / (2 * isr) * quot + (s.left_w + s.right_w) / 2;
-                const double a0 = 2 * s.right_w, a1 = -4 * amplitude, a2 = 2 * s.left_w;
-                const double A = a0 + a1 + a2, B = -(a0 * 1.5 + a1 + a2 * 0.5), Cc = a0 * 0.5;
+                const float isr = (float)C.isr, len = (float)s.length;
+                const float quot = (len > 2 * isr ? 2 * isr : len);
+                const float amplitude = ((float)s.boundary_w - (lw + rw) / 2) / (2 * isr) * quot + (lw + rw) / 2;
+                const float a0 = 2 * rw, a1 = -4 * amplitude, a2 = 2 * lw;
+                const float A = a0 + a1 + a2, B = -(a0 * 1.5f + a1 + a2 * 0.5f), Cc = a0 * 0.5f;
                 weight = A * interpolator * interpolator + B * interpolator + Cc;
             } else {
-                weight = interpolator * s.left_w + (1 - interpolator) * s.right_w;
+                weight = interpolator * lw + (1 - interpolator) * rw;
             }
         }
-        out[k] = val + (out[k] - val) * (float)weight;
+        out[k] = val + (conv - val) * weight;
     }
     if (st) set_status(S, st);
 }

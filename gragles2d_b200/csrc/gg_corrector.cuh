@@ -1,6 +1,6 @@
 // Anisotropic velocity corrector of the convolution stage
 // (LSbox::executeConvolution, src/box.cpp:428-531): per grain, contour
-// sectors around the previous step's junctions are built by one thread into
+// sectors around the previous step's junctions are built by one warp into
 // shared memory, then every pixel projects onto the previous contour and
 // blends its convolved value with the sector / junction / boundary weight.
 #pragma once
@@ -70,20 +70,6 @@ __device__ __forceinline__ double gb_weight_for(const NetConst& C, int owner, in
     return 0.01;
 }
 
-// LSbox::getGBEnergyTimesGBMobility(int i, int j) (src/box.cpp:543-553): the
-// IDLocal entry at (row, col) of the previous step's box.
-__device__ __forceinline__ double gb_weight_at(const NetConst& C, int owner, const uint32_t* idl, const Box& ib,
-                                               int row, int col, uint32_t* status) {
-    uint32_t k;
-    if (!buf_index(ib, row, col, &k)) {
-        *status |= S_INDEX;
-        return 1.0;
-    }
-    const uint32_t id = idl[k];
-    if (id > (uint32_t)C.N) return gb_weight_for(C, owner, -1);
-    return gb_weight_for(C, owner, (int)id);
-}
-
 // The owner's direct-neighbour weights (energy x mobility floored at 0.01)
 // for the per-pixel default weight; entries of removed grains are dropped
 // because a removed grain matches no characteristic.
@@ -122,47 +108,79 @@ __device__ __forceinline__ double table_weight_at(const NbTable& T, const uint32
 }
 
 // GrainJunction::getWeight (src/junction.cpp:23-192), mode 4, ResearchMode 0,
-// ResearchProject 0, no twin identification.
-__device__ double junction_weight(const NetConst& C, const Junction& J, int me, uint32_t* status) {
-    uint32_t nbr[4] = {0xFFFFFFu, 0xFFFFFFu, 0xFFFFFFu, 0xFFFFFFu};
-    for (int i = 0, j = 0; i < J.type && i < 4; i++) {
-        if ((uint32_t)me != J.grains[i]) {
-            nbr[j] = J.grains[i];
-            j++;
+// ResearchProject 0, no twin identification, for every junction of grain
+// `me`: one warp per junction.  Lanes 0-2 evaluate the three grain pairs
+// (me-n0, n0-n1, me-n1) side by side and the warp scans n0's characteristics
+// for n1 together; lane 0 then combines the terms in the reference's order,
+// so each weight is the value the sequential routine computes.
+__device__ void junction_weights(const NetConst& C, const Junction* J, int nj, int me, double* jw,
+                                 uint32_t* s_status) {
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int q = threadIdx.x >> 5; q < nj; q += nw) {
+        const int type = J[q].type;
+        uint32_t nbr[4] = {0xFFFFFFu, 0xFFFFFFu, 0xFFFFFFu, 0xFFFFFFu};
+        for (int i = 0, j = 0; i < type && i < 4; i++) {
+            const uint32_t gi = J[q].grains[i];
+            if ((uint32_t)me != gi) {
+                nbr[j] = gi;
+                j++;
+            }
+        }
+        if (nbr[0] == 0xFFFFFFu || nbr[1] == 0xFFFFFFu) {
+            if (lane == 0) jw[q] = 1;
+            continue;
+        }
+        const int n0 = (int)nbr[0], n1 = (int)nbr[1];
+        if (n0 > C.N || n1 > C.N) {
+            if (lane == 0) {
+                jw[q] = 1;
+                atomicOr(s_status, S_INDEX);
+            }
+            continue;
+        }
+        // characteristics of n1 in n0's list (find_characteristic, first match)
+        bool c01_ok = !(n1 != 0 && C.state[n1] == G_GONE) && n0 != 0;
+        double c01_mob = 1.0;
+        if (c01_ok) {
+            const Neighbour* nb = C.nb + (int64_t)n0 * C.nbmax;
+            const int n = C.nb_n[n0];
+            int first = -1;
+            for (int e0 = 0; e0 < n && first < 0; e0 += 32) {
+                const int e = e0 + lane;
+                const unsigned hit = __ballot_sync(0xffffffffu, e < n && nb[e].id == n1);
+                if (hit) first = e0 + __ffs(hit) - 1;
+            }
+            if (first >= 0) c01_mob = nb[first].mobility;
+        }
+        double mob = 0, gam = 0;
+        if (lane < 3) {
+            const double* pa = C.quat + 4 * (int64_t)(lane == 1 ? n0 : me);
+            const double* pb = C.quat + 4 * (int64_t)(lane == 0 ? n0 : n1);
+            const double theta = grain_misorientation(pa, pb);
+            gam = read_shockley(theta, C);
+            mob = lane == 1 ? c01_mob : mobility_model(theta, C);
+        }
+        const double m1 = __shfl_sync(0xffffffffu, mob, 1), m2 = __shfl_sync(0xffffffffu, mob, 2);
+        const double g1 = __shfl_sync(0xffffffffu, gam, 1), g2 = __shfl_sync(0xffffffffu, gam, 2);
+        if (lane == 0) {
+            if ((n0 != 0 && C.state[n0] == G_GONE) || (n1 != 0 && C.state[n1] == G_GONE))
+                atomicOr(s_status, S_INDEX);
+            double averageMobility = 0;
+            averageMobility += mob;
+            averageMobility += m1;
+            averageMobility += m2;
+            double sigma = gam - g1 + g2;
+            if (!C.isotropic) {
+                if (C.use_mobility_model > 0 && C.tpd > 0) {
+                    averageMobility /= 3;
+                    const double drag = 1 / ((1 / (C.ds * C.tpd)) + 1 / averageMobility);
+                    sigma *= drag;
+                }
+            }
+            if (sigma < 0.01) sigma = 0.01;
+            jw[q] = sigma;
         }
     }
-    if (nbr[0] == 0xFFFFFFu || nbr[1] == 0xFFFFFFu) return 1;
-    const int n0 = (int)nbr[0], n1 = (int)nbr[1];
-    if (n0 > C.N || n1 > C.N) {
-        *status |= S_INDEX;
-        return 1;
-    }
-    if ((n0 != 0 && C.state[n0] == G_GONE) || (n1 != 0 && C.state[n1] == G_GONE)) *status |= S_INDEX;
-    const double* qm = C.quat + 4 * (int64_t)me;
-    const double* q0 = C.quat + 4 * (int64_t)n0;
-    const double* q1 = C.quat + 4 * (int64_t)n1;
-    double averageMobility = 0;
-    double gamma[3];
-    double theta = grain_misorientation(qm, q0);
-    averageMobility += mobility_model(theta, C);
-    gamma[0] = read_shockley(theta, C);
-    theta = grain_misorientation(q0, q1);
-    const Neighbour* c01 = find_characteristic(C, n0, n1);
-    averageMobility += c01 ? c01->mobility : 1.0;
-    gamma[1] = read_shockley(theta, C);
-    theta = grain_misorientation(qm, q1);
-    averageMobility += mobility_model(theta, C);
-    gamma[2] = read_shockley(theta, C);
-    double sigma = gamma[0] - gamma[1] + gamma[2];
-    if (!C.isotropic) {
-        if (C.use_mobility_model > 0 && C.tpd > 0) {
-            averageMobility /= 3;
-            const double drag = 1 / ((1 / (C.ds * C.tpd)) + 1 / averageMobility);
-            sigma *= drag;
-        }
-    }
-    if (sigma < 0.01) sigma = 0.01;
-    return sigma;
 }
 
 __device__ __forceinline__ double seg_len(const CPoint* P, int a, int b) {
@@ -234,177 +252,211 @@ __device__ void set_points_on_boundary(const CPoint* P, const double* seg, int s
 
 // ExplicitGrainBoundary::buildBoundarySectors (src/grainBoundary.cpp:233-342)
 // plus the per-sector weights of ContourSector::getWeight
-// (src/contourSector.cpp:200-272) that do not depend on the pixel.
-__device__ void build_sectors(const NetConst& C, int g, const CPoint* P, const double* seg, double perimeter, int size,
-                              const Junction* J, int nj, const uint32_t* idl, const Box& ib, SectorSet& S,
-                              const double* jw) {
-    S.nconst = 0;
-    S.ninterp = 0;
-    S.status = 0;
+// (src/contourSector.cpp:200-272) that do not depend on the pixel, run by the
+// 32 lanes of the calling warp.  The contour walks of the reference's
+// sequential build are independent per junction (setPointsOnBoundary) and per
+// pair of neighbouring constant sectors (the interpolating contours), so
+// lanes run them side by side; the order-dependent merge of junction sectors
+// runs on lane 0 over the walked end points.  Every sector, end point and
+// weight is the one the sequential build produces.
+__device__ void build_sectors_warp(const NetConst& C, const NbTable& T, const CPoint* P, const double* seg,
+                                   double perimeter, int size, const Junction* J, int nj, const uint32_t* idl,
+                                   const Box& ib, SectorSet& S, const double* jw, int* jl, int* jr) {
+    const int lane = threadIdx.x & 31;
+    if (lane == 0) {
+        S.nconst = 0;
+        S.ninterp = 0;
+        S.status = 0;
+    }
+    __syncwarp();
     if (nj == 0) return;
     const double h = C.h;
     const int real = size - 1;
-    const long guard = lap_guard(perimeter, size, C.isr > C.csr ? C.isr : C.csr, &S.status);
-    auto push_const = [&](int jidx) -> int {
-        if (S.nconst >= kMaxConstSectors) {
-            S.status |= S_JUNCTION_OVERFLOW;
-            return -1;
-        }
-        ConstSector& c = S.cs[S.nconst];
-        c.nj = 1;
-        c.js[0] = jidx;
-        set_points_on_boundary(P, seg, size, J[jidx], h, C.csr, guard, &c.left, &c.right, &S.status);
-        return S.nconst++;
-    };
-    auto merge = [&](ConstSector& c, int jidx) {
-        if (c.nj < kMaxSectorJunctions)
-            c.js[c.nj++] = jidx;
-        else
-            S.status |= S_JUNCTION_OVERFLOW;
-    };
-    push_const(0);
-    int cb = 0;
-    for (int i = 1; i < nj; i++) {
-        int cl, cr;  // current sector's contour points
-        set_points_on_boundary(P, seg, size, J[i], h, C.csr, guard, &cl, &cr, &S.status);
-        if (within(S.cs[cb].left, S.cs[cb].right, real, cr)) {
-            merge(S.cs[cb], i);
-            S.cs[cb].left = cl;
-            if (i == nj - 1) {
-                if (within(S.cs[0].left, S.cs[0].right, real, S.cs[cb].left)) {
-                    if (cb == 0) {
-                        S.cs[0].left = -1;
-                        S.cs[0].right = -1;
-                    } else {
-                        const int cnt = S.cs[cb].nj;
-                        for (int q = 0; q < cnt; q++) merge(S.cs[0], S.cs[cb].js[q]);
-                        S.cs[0].right = S.cs[cb].right;
+    uint32_t st = 0;
+    const long guard = lap_guard(perimeter, size, C.isr > C.csr ? C.isr : C.csr, &st);
+    // 1. sector end points of every junction (setPointsOnBoundary)
+    for (int q = lane; q < nj; q += 32)
+        set_points_on_boundary(P, seg, size, J[q], h, C.csr, guard, &jl[q], &jr[q], &st);
+    __syncwarp();
+    // 2. merge the junction sectors in junction order
+    if (lane == 0) {
+        auto push_const = [&](int jidx) -> int {
+            if (S.nconst >= kMaxConstSectors) {
+                st |= S_JUNCTION_OVERFLOW;
+                return -1;
+            }
+            ConstSector& c = S.cs[S.nconst];
+            c.nj = 1;
+            c.js[0] = jidx;
+            c.left = jl[jidx];
+            c.right = jr[jidx];
+            return S.nconst++;
+        };
+        auto merge = [&](ConstSector& c, int jidx) {
+            if (c.nj < kMaxSectorJunctions)
+                c.js[c.nj++] = jidx;
+            else
+                st |= S_JUNCTION_OVERFLOW;
+        };
+        push_const(0);
+        int cb = 0;
+        for (int i = 1; i < nj; i++) {
+            const int cl = jl[i], cr = jr[i];
+            if (within(S.cs[cb].left, S.cs[cb].right, real, cr)) {
+                merge(S.cs[cb], i);
+                S.cs[cb].left = cl;
+                if (i == nj - 1) {
+                    if (within(S.cs[0].left, S.cs[0].right, real, S.cs[cb].left)) {
+                        if (cb == 0) {
+                            S.cs[0].left = -1;
+                            S.cs[0].right = -1;
+                        } else {
+                            const int cnt = S.cs[cb].nj;
+                            for (int q = 0; q < cnt; q++) merge(S.cs[0], S.cs[cb].js[q]);
+                            S.cs[0].right = S.cs[cb].right;
+                        }
                     }
                 }
-            }
-        } else {
-            if (i == nj - 1 && within(S.cs[0].left, S.cs[0].right, real, cl)) {
-                S.cs[0].right = cr;
-                merge(S.cs[0], i);
             } else {
-                const int k = push_const(i);
-                if (k >= 0) {
-                    S.cs[k].left = cl;
-                    S.cs[k].right = cr;
-                    cb++;
+                if (i == nj - 1 && within(S.cs[0].left, S.cs[0].right, real, cl)) {
+                    S.cs[0].right = cr;
+                    merge(S.cs[0], i);
+                } else {
+                    if (push_const(i) >= 0) cb++;
                 }
             }
         }
     }
-    // constant-sector weights: mean of junction weights in list order
-    for (int s = 0; s < S.nconst; ++s) {
+    __syncwarp();
+    const int nconst = S.nconst;
+    // 3. constant-sector weights: mean of junction weights in list order
+    for (int s = lane; s < nconst; s += 32) {
         double w = 0;
         for (int q = 0; q < S.cs[s].nj; ++q) w += jw[S.cs[s].js[q] < 64 ? S.cs[s].js[q] : 63];
         S.cs[s].weight = w / (double)S.cs[s].nj;
     }
-    const int sec_len = S.nconst;
-    if (!(S.nconst > 1 || S.cs[0].left != S.cs[0].right)) return;
-    for (int i = 0; i < S.nconst && S.nconst > 1; i++) {
-        const int iR = i, iL = (i + 1 + sec_len) % sec_len;
-        const ConstSector& secR = S.cs[iR];
-        const ConstSector& secL = S.cs[iL];
-        // secR.generateLeftInterpolatingContour (src/contourSector.cpp:103-122)
-        InterpSector nr;
-        {
-            double dist = 0;
-            int j = secR.left;
-            long it = 0;
-            for (; dist <= C.isr; j = wrap_next(j, real)) {
-                dist += seg[j];
-                if (++it > guard) {
-                    S.status |= S_SECTOR_GUARD;
-                    break;
+    __syncwarp();
+    if (nconst > 1 || S.cs[0].left != S.cs[0].right) {
+        // 4. interpolating sectors between constant sector i and i + 1
+        InterpSector out0, out1;
+        int cnt = 0;
+        if (nconst > 1 && lane < nconst) {
+            const int iR = lane, iL = (lane + 1 + nconst) % nconst;
+            const ConstSector& secR = S.cs[iR];
+            const ConstSector& secL = S.cs[iL];
+            // secR.generateLeftInterpolatingContour (src/contourSector.cpp:103-122)
+            InterpSector nr;
+            {
+                double dist = 0;
+                int j = secR.left;
+                long it = 0;
+                for (; dist <= C.isr; j = wrap_next(j, real)) {
+                    dist += seg[j];
+                    if (++it > guard) {
+                        st |= S_SECTOR_GUARD;
+                        break;
+                    }
+                }
+                nr.left = wrap_next(j, real);
+                nr.right = secR.left;
+                nr.lb = -1;
+                nr.rb = iR;
+                nr.length = dist;
+            }
+            // secL.generateRightInterpolatingContour (src/contourSector.cpp:145-168)
+            InterpSector nl;
+            {
+                double dist = 0;
+                int j = secL.right;
+                long it = 0;
+                for (; dist <= C.isr; j = wrap_prev(j, real)) {
+                    dist += seg[wrap_prev(j, real)];
+                    if (++it > guard) {
+                        st |= S_SECTOR_GUARD;
+                        break;
+                    }
+                }
+                nl.left = secL.right;
+                nl.right = wrap_prev(j, real);
+                nl.lb = iL;
+                nl.rb = -1;
+                nl.length = dist;
+            }
+            bool merged = false;
+            {
+                int it = 0;
+                for (int j = nr.right; j != periodic(nr.left + 1, size); j = periodic(j + 1, size)) {
+                    if (j == nl.left || j == nl.right) merged = true;
+                    if (++it > size + 1) {
+                        st |= S_SECTOR_GUARD;
+                        break;
+                    }
                 }
             }
-            nr.left = wrap_next(j, real);
-            nr.right = secR.left;
-            nr.lb = -1;
-            nr.rb = iR;
-            nr.length = dist;
-        }
-        // secL.generateRightInterpolatingContour (src/contourSector.cpp:145-168)
-        InterpSector nl;
-        {
-            double dist = 0;
-            int j = secL.right;
-            long it = 0;
-            for (; dist <= C.isr; j = wrap_prev(j, real)) {
-                dist += seg[wrap_prev(j, real)];
-                if (++it > guard) {
-                    S.status |= S_SECTOR_GUARD;
-                    break;
+            if (merged) {
+                // secL.generateInterpolatingSector(secR) (src/contourSector.cpp:124-143)
+                InterpSector r;
+                r.left = secL.right;
+                r.lb = iL;
+                r.right = secR.left;
+                r.rb = iR;
+                double dist = 0;
+                int it = 0;
+                for (int j = r.right; j != r.left; j = wrap_next(j, real)) {
+                    dist += seg[wrap_prev(j, real)];
+                    if (++it > size + 1) {
+                        st |= S_SECTOR_GUARD;
+                        break;
+                    }
                 }
-            }
-            nl.left = secL.right;
-            nl.right = wrap_prev(j, real);
-            nl.lb = iL;
-            nl.rb = -1;
-            nl.length = dist;
-        }
-        bool merged = false;
-        {
-            int it = 0;
-            for (int j = nr.right; j != periodic(nr.left + 1, size); j = periodic(j + 1, size)) {
-                if (j == nl.left || j == nl.right) merged = true;
-                if (++it > size + 1) {
-                    S.status |= S_SECTOR_GUARD;
-                    break;
-                }
-            }
-        }
-        if (merged) {
-            // secL.generateInterpolatingSector(secR) (src/contourSector.cpp:124-143)
-            InterpSector r;
-            r.left = secL.right;
-            r.lb = iL;
-            r.right = secR.left;
-            r.rb = iR;
-            double dist = 0;
-            int it = 0;
-            for (int j = r.right; j != r.left; j = wrap_next(j, real)) {
-                dist += seg[wrap_prev(j, real)];
-                if (++it > size + 1) {
-                    S.status |= S_SECTOR_GUARD;
-                    break;
-                }
-            }
-            r.length = dist;
-            if (S.ninterp < kMaxInterpSectors) S.is[S.ninterp++] = r; else S.status |= S_JUNCTION_OVERFLOW;
-        } else {
-            if (S.ninterp + 1 < kMaxInterpSectors) {
-                S.is[S.ninterp++] = nr;
-                S.is[S.ninterp++] = nl;
+                r.length = dist;
+                out0 = r;
+                cnt = 1;
             } else {
-                S.status |= S_JUNCTION_OVERFLOW;
+                out0 = nr;
+                out1 = nl;
+                cnt = 2;
+            }
+        }
+        // sectors in pair order (at most 2 x 32 = kMaxInterpSectors)
+        int pos = cnt;
+        for (int d = 1; d < 32; d <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, pos, d);
+            if (lane >= d) pos += v;
+        }
+        const int total = __shfl_sync(0xffffffffu, pos, 31);
+        pos -= cnt;
+        if (cnt >= 1) S.is[pos] = out0;
+        if (cnt == 2) S.is[pos + 1] = out1;
+        if (lane == 0) S.ninterp = total;
+        __syncwarp();
+        // 5. interpolating-sector end weights (pixel independent)
+        for (int s = lane; s < total; s += 32) {
+            InterpSector& q = S.is[s];
+            if (q.lb >= 0) {
+                q.left_w = S.cs[q.lb].weight;
+            } else {
+                const int sx = (int)P[q.left].x, sy = (int)P[q.left].y;
+                q.left_w = table_weight_at(T, idl, ib, sy, sx, &st);
+            }
+            if (q.rb >= 0) {
+                q.right_w = S.cs[q.rb].weight;
+            } else {
+                const int sx = (int)P[q.right].x, sy = (int)P[q.right].y;
+                q.right_w = table_weight_at(T, idl, ib, sy, sx, &st);
+            }
+            q.boundary_w = 0;
+            if (q.lb >= 0 && q.rb >= 0) {
+                const CPoint& smp = P[(q.right + 1) % real];
+                q.boundary_w = table_weight_at(T, idl, ib, (int)smp.y, (int)smp.x, &st);
             }
         }
     }
-    // interpolating-sector end weights (pixel independent)
-    for (int s = 0; s < S.ninterp; ++s) {
-        InterpSector& q = S.is[s];
-        if (q.lb >= 0) {
-            q.left_w = S.cs[q.lb].weight;
-        } else {
-            const int sx = (int)P[q.left].x, sy = (int)P[q.left].y;
-            q.left_w = gb_weight_at(C, g, idl, ib, sy, sx, &S.status);
-        }
-        if (q.rb >= 0) {
-            q.right_w = S.cs[q.rb].weight;
-        } else {
-            const int sx = (int)P[q.right].x, sy = (int)P[q.right].y;
-            q.right_w = gb_weight_at(C, g, idl, ib, sy, sx, &S.status);
-        }
-        q.boundary_w = 0;
-        if (q.lb >= 0 && q.rb >= 0) {
-            const CPoint& smp = P[(q.right + 1) % real];
-            q.boundary_w = gb_weight_at(C, g, idl, ib, (int)smp.y, (int)smp.x, &S.status);
-        }
-    }
+    // status bits of all lanes
+    for (int d = 16; d > 0; d >>= 1) st |= __shfl_xor_sync(0xffffffffu, st, d);
+    __syncwarp();
+    if (lane == 0) S.status |= st;
+    __syncwarp();
 }
 
 __device__ void build_seg_table(const SectorSet& S, const double* seg, int size, SegTable& T) {
@@ -489,10 +541,12 @@ __device__ __forceinline__ double pixel_weight(const NetConst& C, const NbTable&
 }
 
 // Per-grain preparation shared by both correctors: segment lengths (into
-// the seg scratch, one thread per segment), junction weights (one thread per
-// junction), perimeter, then the sequential sector build by thread 0.
+// the seg scratch, one thread per segment) and the neighbour table, junction
+// weights (one warp per junction), perimeter, then the sector build by warp
+// 0 (all its lookups in shared memory).  jl, jr: shared scratch of 64 ints.
 __device__ void prepare_sectors(const NetConst& C, NetState* S, int g, const CPoint* P, int size, double* seg,
-                                SectorSet& sec, double* jw, uint32_t* s_st, double* s_per, NbTable& T) {
+                                SectorSet& sec, double* jw, uint32_t* s_st, double* s_per, NbTable& T, int* jl,
+                                int* jr) {
     const Box ib = S->box_prev[g];
     const uint32_t* idl = S->idPrev + S->off_prev[g];
     const Junction* J = S->jPrev + (int64_t)g * C.jmax;
@@ -502,19 +556,16 @@ __device__ void prepare_sectors(const NetConst& C, NetState* S, int g, const CPo
         const double dx = P[k + 1].x - P[k].x, dy = P[k + 1].y - P[k].y;
         seg[k] = sqrt(dx * dx + dy * dy) * C.h;
     }
-    if ((int)threadIdx.x < nj) {
-        uint32_t st = 0;
-        jw[threadIdx.x] = junction_weight(C, J[threadIdx.x], g, &st);
-        if (st) atomicOr(s_st, st);
-    }
     build_nb_table(C, g, T);
     __syncthreads();
-    if (threadIdx.x == 0) {
+    junction_weights(C, J, nj, g, jw, s_st);
+    __syncthreads();
+    if (threadIdx.x < 32) {
         double per = 0;
         for (int k = 0; k < size - 1; ++k) per += seg[k];
-        *s_per = per;
-        build_sectors(C, g, P, seg, per, size, J, nj, idl, ib, sec, jw);
-        if (sec.status | *s_st) set_status(S, sec.status | *s_st);
+        if (threadIdx.x == 0) *s_per = per;
+        build_sectors_warp(C, T, P, seg, per, size, J, nj, idl, ib, sec, jw, jl, jr);
+        if (threadIdx.x == 0 && (sec.status | *s_st)) set_status(S, sec.status | *s_st);
     }
     __syncthreads();
 }
@@ -530,13 +581,14 @@ __global__ void __launch_bounds__(128) k_corrector(NetConst C, NetState* S) {
     __shared__ NbTable nbt;
     __shared__ double s_seg[kSegShared];
     __shared__ SegTable stab;
+    __shared__ int jl[64], jr[64];
     const CPoint* P = S->contPrev + S->coff_prev[g];
     const int size = S->cn_prev[g];
     if (size < 2) return;
     double* seg = size - 1 <= kSegShared ? s_seg : S->segPrev + S->coff_prev[g];
     const Box ib = S->box_prev[g];
     const uint32_t* idl = S->idPrev + S->off_prev[g];
-    prepare_sectors(C, S, g, P, size, seg, sec, jw, &s_st, &s_per, nbt);
+    prepare_sectors(C, S, g, P, size, seg, sec, jw, &s_st, &s_per, nbt, jl, jr);
     const bool tabled = size - 1 <= kSegTable;
     if (tabled) build_seg_table(sec, seg, size, stab);
     __syncthreads();
