@@ -221,24 +221,64 @@ __global__ void __launch_bounds__(256) k_compare(NetConst C, NetState* S) {
     const uint32_t* idp = S->idPrev + S->off_prev[g];
     uint32_t* idc = S->idCur + S->off_cur[g];
     const R tube = (R)(0.7 * C.delta);
-    const R hh = (R)C.h;
 
     int xmin = bc.x1, xmax = bc.x0, ymin = bc.y1, ymax = bc.y0;
-    for (int64_t p = threadIdx.x; p < area; p += blockDim.x) {
-        const int i = bc.y0 + (int)(p / w);
-        const int j = bc.x0 + (int)(p - (int64_t)(i - bc.y0) * w);
-        uint32_t id = p < keep ? idp[p] : 0u;
+    // one warp per 8 x 4 tile: the warp first picks the list members whose
+    // boxes meet the tile, then every lane takes the maximum over those (in
+    // list order, strict '>') with four members' loads in flight
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int hgt = box_h(bc);
+    const int ntx = (w + 7) >> 3, ntiles = ntx * ((hgt + 3) >> 2);
+    for (int t = warp; t < ntiles; t += nwarps) {
+        const int tx0 = bc.x0 + (t % ntx) * 8, ty0 = bc.y0 + (t / ntx) * 4;
+        const int tx1 = min(tx0 + 8, bc.x1), ty1 = min(ty0 + 4, bc.y1);
+        const int j = tx0 + (lane & 7), i = ty0 + (lane >> 3);
+        const bool inside = j < tx1 && i < ty1;
+        const int64_t p = (int64_t)(i - bc.y0) * w + (j - bc.x0);
+        uint32_t id = inside && p < keep ? idp[p] : 0u;
+        const R in = inside ? self[p] : (R)0;
         R out = (R)-1.0;
-        for (int k = 0; k < nl; ++k) {
-            const Box bk = s_box[k];
-            if (i >= bk.y0 && i < bk.y1 && j >= bk.x0 && j < bk.x1) {
-                const R d = conv[s_off[k] + (int64_t)(i - bk.y0) * (bk.x1 - bk.x0) + (j - bk.x0)];
-                if (d > out) {
-                    out = d;
-                    id = (uint32_t)s_id[k];
+        for (int k0 = 0; k0 < nl; k0 += 32) {
+            bool hit = false;
+            if (k0 + lane < nl) {
+                const Box bk = s_box[k0 + lane];
+                hit = bk.x0 < tx1 && bk.x1 > tx0 && bk.y0 < ty1 && bk.y1 > ty0;
+            }
+            unsigned mask = __ballot_sync(FULL, hit);
+            while (mask) {
+                int ks[4];
+                R ds[4];
+                bool ok[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    ks[u] = -1;
+                    if (mask) {
+                        ks[u] = k0 + __ffs(mask) - 1;
+                        mask &= mask - 1;
+                    }
                 }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    ok[u] = false;
+                    ds[u] = (R)0;
+                    if (ks[u] >= 0 && inside) {
+                        const Box bk = s_box[ks[u]];
+                        if (i >= bk.y0 && i < bk.y1 && j >= bk.x0 && j < bk.x1) {
+                            ok[u] = true;
+                            ds[u] = conv[s_off[ks[u]] + (int64_t)(i - bk.y0) * (bk.x1 - bk.x0) + (j - bk.x0)];
+                        }
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (ok[u] && ds[u] > out) {
+                        out = ds[u];
+                        id = (uint32_t)s_id[ks[u]];
+                    }
             }
         }
+        if (!inside) continue;
         if (bnd) {
             const int dxmin = -(j - b), dymin = -(i - b);
             const int dxmax = (j - (m - b)), dymax = (i - (m - b));
@@ -263,7 +303,6 @@ __global__ void __launch_bounds__(256) k_compare(NetConst C, NetState* S) {
                 id = 0u;
             }
         }
-        const R in = self[p];
         const R v = (fabs((double)in) < (double)tube) ? (R)0.5 * (in - out) : in;
         cmpo[p] = v;
         idc[p] = id;
@@ -273,7 +312,6 @@ __global__ void __launch_bounds__(256) k_compare(NetConst C, NetState* S) {
             ymin = i < ymin ? i : ymin;
             ymax = i > ymax ? i : ymax;
         }
-        (void)hh;
     }
     // CTA reduction of the bounding box
     for (int o = 16; o > 0; o >>= 1) {
@@ -282,7 +320,6 @@ __global__ void __launch_bounds__(256) k_compare(NetConst C, NetState* S) {
         ymin = min(ymin, __shfl_xor_sync(0xffffffffu, ymin, o));
         ymax = max(ymax, __shfl_xor_sync(0xffffffffu, ymax, o));
     }
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (lane == 0) {
         s_red[0][warp] = xmin;
         s_red[1][warp] = xmax;

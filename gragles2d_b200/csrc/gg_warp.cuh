@@ -283,17 +283,36 @@ __device__ int project_xy(const double2* P, int asize, double px, double py, dou
     return minimal_segment;
 }
 
+// ExplicitGrainBoundary::computeVolume / computePerimeter
+// (src/grainBoundary.cpp:201-213, 224-231) by the whole warp: lanes evaluate
+// the per-segment terms side by side, then the terms are added one after the
+// other in contour order (every lane holds the same sum, rounded exactly as
+// the reference's loop).
 __device__ __forceinline__ double volume_xy(const double2* P, int n, double h) {
+    const int lane = threadIdx.x & 31;
     double v = 0;
-    for (int i = 0; i < n - 1; i++) v += (P[i].y + P[i + 1].y) * (P[i].x - P[i + 1].x);
+    for (int i0 = 0; i0 < n - 1; i0 += 32) {
+        const int i = i0 + lane;
+        double t = 0;
+        if (i < n - 1) t = (P[i].y + P[i + 1].y) * (P[i].x - P[i + 1].x);
+        const int m = n - 1 - i0 < 32 ? n - 1 - i0 : 32;
+        for (int q = 0; q < m; ++q) v += __shfl_sync(0xffffffffu, t, q);
+    }
     return fabs(v) * h * h * 0.5;
 }
 
 __device__ __forceinline__ double perimeter_xy(const double2* P, int n, double h) {
+    const int lane = threadIdx.x & 31;
     double p = 0;
-    for (int i = 0; i < n - 1; i++) {
-        const double dx = P[i].x - P[i + 1].x, dy = P[i].y - P[i + 1].y;
-        p += sqrt(dx * dx + dy * dy) * h;
+    for (int i0 = 0; i0 < n - 1; i0 += 32) {
+        const int i = i0 + lane;
+        double t = 0;
+        if (i < n - 1) {
+            const double dx = P[i].x - P[i + 1].x, dy = P[i].y - P[i + 1].y;
+            t = sqrt(dx * dx + dy * dy) * h;
+        }
+        const int m = n - 1 - i0 < 32 ? n - 1 - i0 : 32;
+        for (int q = 0; q < m; ++q) p += __shfl_sync(0xffffffffu, t, q);
     }
     return p;
 }
@@ -402,52 +421,72 @@ __device__ bool extract_warp(const Field<R>& f, const uint32_t* idl, uint32_t ow
     return true;
 }
 
-constexpr int kBitmapRows = 96;  // bitmap walk for boxes up to 96 x 96
-constexpr int kBitmapWords = 4;
-constexpr int kTrace = 640;  // walk steps recorded per warp
+constexpr int kBitmapCap = 400;  // words of the padded bitmap (boxes up to about 94 x 94)
+constexpr int kTrace = 640;      // walk steps recorded per warp
 
 struct WalkShared {
-    uint32_t bm[kBitmapRows * kBitmapWords];
+    uint32_t bm[kBitmapCap];
     uint32_t trace[kTrace];
 };
 
+// Next direction of generateContour's switch for each corner mask
+// (src/marchingSquares.cpp:64-154), two bits per mask; the saddles 6 and 9
+// and the empty / full masks 0 and 15 are decided separately.
+constexpr uint32_t ms_next_bits() {
+    const int dir[16] = {0, MS_UP, MS_RIGHT, MS_RIGHT, MS_LEFT, MS_UP, 0, MS_RIGHT,
+                         MS_DOWN, 0, MS_DOWN, MS_DOWN, MS_LEFT, MS_UP, MS_LEFT, 0};
+    uint32_t t = 0;
+    for (int m = 0; m < 16; ++m) t |= (uint32_t)dir[m] << (2 * m);
+    return t;
+}
+constexpr uint32_t kMsNext = ms_next_bits();
+// masks whose case generates a point (all but 0, 6, 9, 15)
+constexpr uint32_t kMsEmit = 0xFFFFu & ~((1u << 0) | (1u << 6) | (1u << 9) | (1u << 15));
+
 // Marching squares with the inside/outside decisions taken from a bitmap of
-// the box in shared memory (built with one ballot per 32 pixels), the walk
-// recorded as a trace by lane 0, and the points, junctions and duplicate
-// removal evaluated across the lanes in walk order.  Returns 0 if no pixel
-// is inside, 1 on success, -1 if the box or the walk does not fit the
-// shared buffers (the caller then walks in global memory).
+// the box in shared memory (built with one ballot per 32 pixels, with a
+// zero border of one pixel all round so the walk needs no bounds tests), the
+// walk recorded as a trace by lane 0 (one 4-bit corner mask per step from two
+// funnel shifts), and the points, junctions and duplicate removal evaluated
+// across the lanes in walk order.  Returns 0 if no pixel is inside, 1 on
+// success, -1 if the box or the walk does not fit the shared buffers (the
+// caller then walks in global memory).
 template <typename R>
 __device__ int extract_bitmap_warp(const Field<R>& f, const uint32_t* idl, uint32_t own, ContourOut& o, int lane,
                                    double2* xy, WalkShared& ws) {
     const Box b = f.b;
     const int w = box_w(b), hgt = box_h(b);
-    if (w > kBitmapWords * 32 || hgt > kBitmapRows) return -1;
-    const int wpr = (w + 31) >> 5;
-    for (int r = 0; r < hgt; ++r)
+    // padded bitmap: row r + 1, bit c + 1 hold pixel (r, c) of the box
+    const int wpr = (w + 2 + 31) >> 5;
+    if (w + 2 > 1024 || (hgt + 2) * wpr + 1 > kBitmapCap) return -1;
+    for (int r0 = 0; r0 < hgt + 2; r0 += 8)  // eight rows of loads in flight
         for (int q = 0; q < wpr; ++q) {
-            const int c = q * 32 + lane;
-            const bool in = c < w && (double)f.v[r * w + c] >= 0;
-            const uint32_t word = __ballot_sync(0xffffffffu, in);
-            if (lane == 0) ws.bm[r * wpr + q] = word;
+            const int c = q * 32 + lane - 1;
+            bool in[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int r = r0 + u - 1;
+                in[u] = r >= 0 && r < hgt && c >= 0 && c < w && (double)f.v[r * w + c] >= 0;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const uint32_t word = __ballot_sync(0xffffffffu, in[u]);
+                if (lane == 0 && r0 + u < hgt + 2) ws.bm[(r0 + u) * wpr + q] = word;
+            }
         }
+    if (lane == 0) ws.bm[(hgt + 2) * wpr] = 0u;
     __syncwarp();
-    auto inside = [&](int row, int col) -> bool {
-        if (row < b.y0 || row >= b.y1 || col < b.x0 || col >= b.x1) return false;
-        const int rc = col - b.x0;
-        return (ws.bm[(row - b.y0) * wpr + (rc >> 5)] >> (rc & 31)) & 1u;
-    };
     // first inside pixel in row-major order
     int start = -1;
     for (int q0 = 0; q0 < hgt * wpr; q0 += 32) {
         const int q = q0 + lane;
-        const uint32_t word = q < hgt * wpr ? ws.bm[q] : 0u;
+        const uint32_t word = q < hgt * wpr ? ws.bm[wpr + q] : 0u;
         const uint32_t any = __ballot_sync(0xffffffffu, word != 0u);
         if (any) {
             const int src = __ffs(any) - 1;
             const uint32_t wd = __shfl_sync(0xffffffffu, word, src);
             const int qq = q0 + src;
-            start = (qq / wpr) * w + (qq % wpr) * 32 + (__ffs(wd) - 1);
+            start = (qq / wpr) * w + (qq % wpr) * 32 + (__ffs(wd) - 1) - 1;
             break;
         }
     }
@@ -457,55 +496,40 @@ __device__ int extract_bitmap_warp(const Field<R>& f, const uint32_t* idl, uint3
         return 0;
     }
     const int startX = b.x0 + start % w, startY = b.y0 + start / w;
-    // lane 0: the walk of generateContour (src/marchingSquares.cpp:44-187) on the bitmap
+    // lane 0: the walk of generateContour (src/marchingSquares.cpp:44-187) on
+    // the bitmap, in padded coordinates lc = left - x0 + 1, tr = top - y0 + 1
     int nsteps = 0;
     uint32_t st = 0;
     if (lane == 0) {
-        int left = startX - 1, right = startX, top = startY - 1, bottom = startY;
+        const int lc_end = startX - b.x0, tr_end = startY - b.y0;
+        int lc = lc_end, tr = tr_end;
         int next = MS_NONE, prev = MS_NONE;
         const long limit = 4L * (w + 2) * (hgt + 2) + 16;
         long it = 0;
         do {
-            int mask = 0;
-            if (inside(top, left)) mask |= C_TL;
-            if (inside(top, right)) mask |= C_TR;
-            if (inside(bottom, left)) mask |= C_BL;
-            if (inside(bottom, right)) mask |= C_BR;
-            int emit = 1;
-            switch (mask) {
-                case C_TL: next = MS_UP; break;
-                case C_TR: next = MS_RIGHT; break;
-                case C_TL | C_TR: next = MS_RIGHT; break;
-                case C_BL: next = MS_LEFT; break;
-                case C_BL | C_TL: next = MS_UP; break;
-                case C_BL | C_TR:
-                    next = (prev == MS_UP) ? MS_RIGHT : MS_LEFT;
-                    emit = 0;
-                    break;
-                case C_BL | C_TR | C_TL: next = MS_RIGHT; break;
-                case C_BR: next = MS_DOWN; break;
-                case C_BR | C_TL:
-                    next = (prev == MS_RIGHT) ? MS_DOWN : MS_UP;
-                    emit = 0;
-                    break;
-                case C_BR | C_TR: next = MS_DOWN; break;
-                case C_BR | C_TR | C_TL: next = MS_DOWN; break;
-                case C_BR | C_BL: next = MS_LEFT; break;
-                case C_BR | C_BL | C_TL: next = MS_UP; break;
-                case C_BR | C_BL | C_TR: next = MS_LEFT; break;
-                default: emit = 0; break;
-            }
+            const uint32_t* rt = ws.bm + tr * wpr + (lc >> 5);
+            const int sh = lc & 31;
+            const uint32_t top2 = __funnelshift_r(rt[0], rt[1], sh);
+            const uint32_t bot2 = __funnelshift_r(rt[wpr], rt[wpr + 1], sh);
+            const int mask = (int)((top2 & 3u) | ((bot2 & 3u) << 2));
+            if (mask == (C_BL | C_TR))
+                next = (prev == MS_UP) ? MS_RIGHT : MS_LEFT;
+            else if (mask == (C_BR | C_TL))
+                next = (prev == MS_RIGHT) ? MS_DOWN : MS_UP;
+            else if (mask != 0 && mask != 15)
+                next = (int)((kMsNext >> (2 * mask)) & 3u);
+            const uint32_t emit = (kMsEmit >> mask) & 1u;
             if (nsteps >= kTrace) {
                 nsteps = -1;
                 break;
             }
-            ws.trace[nsteps++] = (uint32_t)(left - b.x0 + 1) | ((uint32_t)(top - b.y0 + 1) << 10) |
-                                 ((uint32_t)mask << 20) | ((uint32_t)next << 24) | ((uint32_t)emit << 27);
+            ws.trace[nsteps++] = (uint32_t)lc | ((uint32_t)tr << 10) | ((uint32_t)mask << 20) |
+                                 ((uint32_t)next << 24) | (emit << 27);
             switch (next) {
-                case MS_UP: top--; bottom--; break;
-                case MS_DOWN: top++; bottom++; break;
-                case MS_LEFT: left--; right--; break;
-                case MS_RIGHT: left++; right++; break;
+                case MS_UP: tr--; break;
+                case MS_DOWN: tr++; break;
+                case MS_LEFT: lc--; break;
+                case MS_RIGHT: lc++; break;
                 default: break;
             }
             prev = next;
@@ -513,7 +537,7 @@ __device__ int extract_bitmap_warp(const Field<R>& f, const uint32_t* idl, uint3
                 st |= S_WALK_LIMIT;
                 break;
             }
-        } while (left != startX - 1 || bottom != startY);
+        } while (lc != lc_end || tr != tr_end);
     }
     nsteps = __shfl_sync(0xffffffffu, nsteps, 0);
     if (nsteps < 0) return -1;
@@ -653,8 +677,9 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_levelset_w(NetConst C,
     if (ok) {
         double newVolume = 0;
         bool regular_motion = true;
+        if (shared) newVolume = volume_xy(xy, o.n, C.h);
         if (lane == 0) {
-            newVolume = shared ? volume_xy(xy, o.n, C.h) : contour_volume(o.pts, o.n, C.h);
+            if (!shared) newVolume = contour_volume(o.pts, o.n, C.h);
             regular_motion = motion_regular(old_len, o.n, C.volume[g], newVolume, C.dt, &irregular);
         }
         regular_motion = __shfl_sync(0xffffffffu, regular_motion, 0);
@@ -668,8 +693,9 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_levelset_w(NetConst C,
             __syncwarp();
             ok = extract_warp(f, idl, (uint32_t)g, o, lane, xy, &shared, &s_walk[wid]);
             if (!ok) break;
+            if (shared) newVolume = volume_xy(xy, o.n, C.h);
             if (lane == 0) {
-                newVolume = shared ? volume_xy(xy, o.n, C.h) : contour_volume(o.pts, o.n, C.h);
+                if (!shared) newVolume = contour_volume(o.pts, o.n, C.h);
                 regular_motion = motion_regular(old_len, o.n, C.volume[g], newVolume, C.dt, &irregular);
                 if (++tries > 64) {
                     o.status |= S_RETRY_LIMIT;
@@ -690,7 +716,8 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_levelset_w(NetConst C,
         }
     }
     double perim = 0;
-    if (ok && lane == 0) perim = shared ? perimeter_xy(xy, o.n, C.h) : contour_perimeter(o.pts, o.n, C.h);
+    if (ok && shared) perim = perimeter_xy(xy, o.n, C.h);
+    if (ok && !shared && lane == 0) perim = contour_perimeter(o.pts, o.n, C.h);
     if (lane != 0) return;
     if (o.status) set_status(S, o.status);
     C.regular[g] = 1;
@@ -943,17 +970,23 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_second_order_w(NetCons
 // the input box is read through L1; the result is clamped to +-delta and
 // written back coalesced.
 constexpr int kRedistThreads = 64;
-constexpr int kRedistSmemBytes = 16 * 1024;
+constexpr int kRedistSmemBytes = 24 * 1024;
 
+// The four directional sweeps of LSbox::executeRedistancing
+// (src/box.cpp:1259-1399) over the new box bo.  The input is read through
+// IN(i, j) = in[(i - in_y0) * si + (j - in_x0)] and is only touched inside
+// the intersection of bi and bo; the output through OUT(i, j) =
+// out[(i - bo.y0) * so + (j - bo.x0)].  One thread per column (y sweeps) or
+// row (x sweeps), carrying the running value in a register.
 template <typename R>
-__device__ void redistance_sweeps(const R* __restrict__ in, const Box bi, R* __restrict__ out, const Box bo, R h) {
-    const int wi = box_w(bi), wo = box_w(bo);
+__device__ void redistance_sweeps(const R* __restrict__ in, int in_x0, int in_y0, int si, const Box bi,
+                                  R* __restrict__ out, int so, const Box bo, R h) {
     const int ixmin = (bi.x0 < bo.x0) ? bo.x0 : bi.x0;
     const int iymin = (bi.y0 < bo.y0) ? bo.y0 : bi.y0;
     const int ixmax = (bi.x1 < bo.x1) ? bi.x1 : bo.x1;
     const int iymax = (bi.y1 < bo.y1) ? bi.y1 : bo.y1;
-#define GG_IN(i, j) in[(int64_t)((i) - bi.y0) * wi + ((j) - bi.x0)]
-#define GG_OUT(i, j) out[(int64_t)((i) - bo.y0) * wo + ((j) - bo.x0)]
+#define GG_IN(i, j) in[(int64_t)((i) - in_y0) * si + ((j) - in_x0)]
+#define GG_OUT(i, j) out[(int64_t)((i) - bo.y0) * so + ((j) - bo.x0)]
     for (int j = ixmin + (int)threadIdx.x; j < bo.x1; j += blockDim.x) {
         if (iymin < bo.y1 - 1) {  // y forward
             R cur = GG_OUT(iymin, j);
@@ -1048,6 +1081,12 @@ __device__ void redistance_sweeps(const R* __restrict__ in, const Box bi, R* __r
     __syncthreads();
 }
 
+// LSbox::executeRedistancing, one CTA of 64 threads per grain.  When both
+// fit in kRedistSmemBytes, the input over the intersection of the old and new
+// boxes and the output box are staged in shared memory with odd row strides
+// (so the row-wise sweeps hit distinct banks); a larger box keeps only its
+// output there, and the largest stay in global memory.  clearValues(-1)
+// before, clampValues(-delta, delta) after.
 template <typename R>
 __global__ void __launch_bounds__(kRedistThreads) k_redistance_s(NetConst C, NetState* S) {
     extern __shared__ __align__(16) unsigned char s_raw[];
@@ -1057,19 +1096,67 @@ __global__ void __launch_bounds__(kRedistThreads) k_redistance_s(NetConst C, Net
     R* out_g = phiB_of<R>(S) + S->off_new[g];
     const Box bi = S->box_cur[g], bo = S->box_new[g];
     const R h = (R)C.h, delta = (R)C.delta;
+    const int wi = box_w(bi), wo = box_w(bo), ho = box_h(bo);
     const int64_t ao = box_area(bo);
-    const bool fits = ao * (int64_t)sizeof(R) <= kRedistSmemBytes;
-    R* out = fits ? reinterpret_cast<R*>(s_raw) : out_g;
-    for (int64_t p = threadIdx.x; p < ao; p += blockDim.x) out[p] = (R)-1.0;  // clearValues(-1)
-    __syncthreads();
-    redistance_sweeps<R>(in_g, bi, out, bo, h);
-    for (int64_t p = threadIdx.x; p < ao; p += blockDim.x) {  // clampValues(-delta, delta)
-        R v = out[p];
-        if (v < -delta)
-            v = -delta;
-        else if (v > delta)
-            v = delta;
-        out_g[p] = v;
+    const int ixmin = (bi.x0 < bo.x0) ? bo.x0 : bi.x0;
+    const int iymin = (bi.y0 < bo.y0) ? bo.y0 : bi.y0;
+    const int ixmax = (bi.x1 < bo.x1) ? bi.x1 : bo.x1;
+    const int iymax = (bi.y1 < bo.y1) ? bi.y1 : bo.y1;
+    const int wI = ixmax > ixmin ? ixmax - ixmin : 0, hI = iymax > iymin ? iymax - iymin : 0;
+    const int so = wo | 1, sI = wI | 1;
+    const bool fits = (int64_t)sizeof(R) * ((int64_t)so * ho + (int64_t)sI * hI) <= kRedistSmemBytes;
+    if (fits) {
+        R* out = reinterpret_cast<R*>(s_raw);
+        R* in = out + so * ho;
+        // row by row, eight loads in flight per thread
+        const R* src = in_g + (int64_t)(iymin - bi.y0) * wi + (ixmin - bi.x0);
+        for (int r0 = 0; r0 < hI; r0 += 8)
+            for (int c = threadIdx.x; c < wI; c += blockDim.x) {
+                R v[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) v[u] = r0 + u < hI ? src[(int64_t)(r0 + u) * wi + c] : (R)0;
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (r0 + u < hI) in[(r0 + u) * sI + c] = v[u];
+            }
+        for (int p = threadIdx.x; p < so * ho; p += blockDim.x) out[p] = (R)-1.0;  // clearValues(-1)
+        __syncthreads();
+        redistance_sweeps<R>(in, ixmin, iymin, sI, bi, out, so, bo, h);
+        for (int r = 0; r < ho; ++r)  // clampValues(-delta, delta)
+            for (int c = threadIdx.x; c < wo; c += blockDim.x) {
+                R v = out[r * so + c];
+                if (v < -delta)
+                    v = -delta;
+                else if (v > delta)
+                    v = delta;
+                out_g[(int64_t)r * wo + c] = v;
+            }
+    } else if ((int64_t)sizeof(R) * so * ho <= kRedistSmemBytes) {  // output staged, input read in place
+        R* out = reinterpret_cast<R*>(s_raw);
+        for (int p = threadIdx.x; p < so * ho; p += blockDim.x) out[p] = (R)-1.0;
+        __syncthreads();
+        redistance_sweeps<R>(in_g, bi.x0, bi.y0, wi, bi, out, so, bo, h);
+        for (int r = 0; r < ho; ++r)
+            for (int c = threadIdx.x; c < wo; c += blockDim.x) {
+                R v = out[r * so + c];
+                if (v < -delta)
+                    v = -delta;
+                else if (v > delta)
+                    v = delta;
+                out_g[(int64_t)r * wo + c] = v;
+            }
+    } else {
+        for (int64_t p = threadIdx.x; p < ao; p += blockDim.x) out_g[p] = (R)-1.0;
+        __syncthreads();
+        redistance_sweeps<R>(in_g, bi.x0, bi.y0, wi, bi, out_g, wo, bo, h);
+        for (int64_t p = threadIdx.x; p < ao; p += blockDim.x) {
+            R v = out_g[p];
+            if (v < -delta)
+                v = -delta;
+            else if (v > delta)
+                v = delta;
+            out_g[p] = v;
+        }
     }
 }
 
