@@ -18,57 +18,109 @@ constexpr int kSepStrip = 4;       // outputs per thread along the convolution a
 // The kernel is laid out once as kx[j] = k_n[(j - (n-1)) mod n], j < 2n-1
 // (zero-padded), so output c of a row is sum_c' X[c'] kx[c - c' + n - 1]:
 // each thread accumulates a strip of 4 consecutive outputs while a 4-entry
-// register window slides down kx (one shared-memory load per 4 FMAs).
+// register window slides down kx (one shared-memory load per 4 FMAs).  Taps
+// farther than R (circularly) from the strip are left out: the host sets R
+// so that every dropped k_n entry is below 2^-26 k_n[0].
+
+// The (at most two) index ranges of c' within circular distance R of the
+// strip [c0, c0 + 4), as [s0, e0) and [s1, e1).
+__device__ __forceinline__ void band_ranges(int c0, int n, int R, int* s0, int* e0, int* s1, int* e1) {
+    *s1 = 0;
+    *e1 = 0;
+    if (2 * R + kSepStrip >= n) {
+        *s0 = 0;
+        *e0 = n;
+        return;
+    }
+    const int lo = c0 - R, hi = c0 + kSepStrip + R;
+    if (lo < 0) {
+        *s0 = lo + n;
+        *e0 = n;
+        *e1 = hi;
+    } else if (hi > n) {
+        *s0 = lo;
+        *e0 = n;
+        *e1 = hi - n;
+    } else {
+        *s0 = lo;
+        *e0 = hi;
+    }
+}
+
+// rows: two rows per thread share each kernel window load
 __device__ __forceinline__ void sep_pass_rows(const float* __restrict__ X, float* __restrict__ T,
-                                              const float* __restrict__ kx, int n) {
+                                              const float* __restrict__ kx, int n, int R) {
     const int nb = (n + kSepStrip - 1) / kSepStrip;
-    for (int t = threadIdx.x; t < n * nb; t += blockDim.x) {
-        const int r = t / nb, c0 = (t - r * nb) * kSepStrip;
-        const float* xr = X + r * n;
-        int base = c0 + n - 1;  // kx index of (c0 - c') at c' = 0
-        float w0 = kx[base], w1 = kx[base + 1], w2 = kx[base + 2], w3 = kx[base + 3];
-        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+    const int npair = (n + 1) >> 1;
+    for (int t = threadIdx.x; t < npair * nb; t += blockDim.x) {
+        const int rp = t / nb, c0 = (t - rp * nb) * kSepStrip;
+        const int r = 2 * rp;
+        const bool two = r + 1 < n;
+        const float* xa = X + r * n;
+        const float* xb = two ? xa + n : xa;
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f, b0 = 0.f, b1 = 0.f, b2 = 0.f, b3 = 0.f;
+        int rs[2], re[2];
+        band_ranges(c0, n, R, &rs[0], &re[0], &rs[1], &re[1]);
+        for (int q = 0; q < 2; ++q) {
+            int base = c0 + n - 1 - rs[q];  // kx index of (c0 - c') at c' = rs[q]
+            float w0 = kx[base], w1 = kx[base + 1], w2 = kx[base + 2], w3 = kx[base + 3];
 #pragma unroll 4
-        for (int cp = 0; cp < n; ++cp) {
-            const float x = xr[cp];
-            a0 = fmaf(x, w0, a0);
-            a1 = fmaf(x, w1, a1);
-            a2 = fmaf(x, w2, a2);
-            a3 = fmaf(x, w3, a3);
-            --base;
-            w3 = w2;
-            w2 = w1;
-            w1 = w0;
-            w0 = kx[base];
+            for (int cp = rs[q]; cp < re[q]; ++cp) {
+                const float x = xa[cp], y = xb[cp];
+                a0 = fmaf(x, w0, a0);
+                a1 = fmaf(x, w1, a1);
+                a2 = fmaf(x, w2, a2);
+                a3 = fmaf(x, w3, a3);
+                b0 = fmaf(y, w0, b0);
+                b1 = fmaf(y, w1, b1);
+                b2 = fmaf(y, w2, b2);
+                b3 = fmaf(y, w3, b3);
+                --base;
+                w3 = w2;
+                w2 = w1;
+                w1 = w0;
+                w0 = kx[base];
+            }
         }
-        float* tr = T + r * n + c0;
-        tr[0] = a0;
-        if (c0 + 1 < n) tr[1] = a1;
-        if (c0 + 2 < n) tr[2] = a2;
-        if (c0 + 3 < n) tr[3] = a3;
+        float* ta = T + r * n + c0;
+        ta[0] = a0;
+        if (c0 + 1 < n) ta[1] = a1;
+        if (c0 + 2 < n) ta[2] = a2;
+        if (c0 + 3 < n) ta[3] = a3;
+        if (two) {
+            float* tb = ta + n;
+            tb[0] = b0;
+            if (c0 + 1 < n) tb[1] = b1;
+            if (c0 + 2 < n) tb[2] = b2;
+            if (c0 + 3 < n) tb[3] = b3;
+        }
     }
 }
 
 __device__ __forceinline__ void sep_pass_cols(const float* __restrict__ T, float* __restrict__ out,
-                                              const float* __restrict__ kx, int n) {
+                                              const float* __restrict__ kx, int n, int R) {
     const int nb = (n + kSepStrip - 1) / kSepStrip;
     for (int t = threadIdx.x; t < n * nb; t += blockDim.x) {
         const int rb = t / n, c = t - rb * n, r0 = rb * kSepStrip;
-        int base = r0 + n - 1;
-        float w0 = kx[base], w1 = kx[base + 1], w2 = kx[base + 2], w3 = kx[base + 3];
         float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+        int rs[2], re[2];
+        band_ranges(r0, n, R, &rs[0], &re[0], &rs[1], &re[1]);
+        for (int q = 0; q < 2; ++q) {
+            int base = r0 + n - 1 - rs[q];
+            float w0 = kx[base], w1 = kx[base + 1], w2 = kx[base + 2], w3 = kx[base + 3];
 #pragma unroll 4
-        for (int rp = 0; rp < n; ++rp) {
-            const float x = T[rp * n + c];
-            a0 = fmaf(w0, x, a0);
-            a1 = fmaf(w1, x, a1);
-            a2 = fmaf(w2, x, a2);
-            a3 = fmaf(w3, x, a3);
-            --base;
-            w3 = w2;
-            w2 = w1;
-            w1 = w0;
-            w0 = kx[base];
+            for (int rp = rs[q]; rp < re[q]; ++rp) {
+                const float x = T[rp * n + c];
+                a0 = fmaf(w0, x, a0);
+                a1 = fmaf(w1, x, a1);
+                a2 = fmaf(w2, x, a2);
+                a3 = fmaf(w3, x, a3);
+                --base;
+                w3 = w2;
+                w2 = w1;
+                w1 = w0;
+                w0 = kx[base];
+            }
         }
         out[r0 * n + c] = a0;
         if (r0 + 1 < n) out[(r0 + 1) * n + c] = a1;
@@ -111,9 +163,10 @@ __global__ void __launch_bounds__(128) k_conv_sep(NetConst C, NetState* S) {
     if (fits)
         for (int i = threadIdx.x; i < nn2; i += blockDim.x) X[i] = in[i];
     __syncthreads();
-    sep_pass_rows(fits ? X : in, T, kx, n);
+    const int R = (int)kg[n];  // band radius stored after the n kernel entries
+    sep_pass_rows(fits ? X : in, T, kx, n, R);
     __syncthreads();
-    sep_pass_cols(T, out, kx, n);
+    sep_pass_cols(T, out, kx, n, R);
 }
 
 size_t conv_sep_smem(int tmax) {

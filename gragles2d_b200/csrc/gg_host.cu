@@ -547,7 +547,7 @@ int gg_distance_initialisation(gg_ctx* c) {
         gk_off[n] = gkn;
         gkn += (int64_t)(n / 2 + 1) * (n / 2 + 1);
         ck_off[n] = ckn;
-        ckn += n;
+        ckn += n + 1;  // k_n, then its band radius
     }
     const bool plain = P.precision == GG_PRECISION_PLAIN;
     std::vector<double> tw(plain ? 2 * twn : 2), gk(plain ? gkn : 1);
@@ -577,6 +577,14 @@ int gg_distance_initialisation(gg_ctx* c) {
                 for (int f = 0; f < n; ++f) acc += gf[f] * cos(2.0 * kPiH * (double)((int64_t)f * r % n) / n);
                 ck[ck_off[n] + r] = (float)(acc / n);
             }
+            // band radius: every entry at circular distance > R is below 2^-26 k_n[0]
+            // (under half an FP32 ulp of the centre tap; the dropped tail is the
+            // flat aliasing floor of the truncated Gaussian, ~7e-9 k_n[0])
+            int R = 0;
+            const double tiny = std::ldexp(std::fabs((double)ck[ck_off[n]]), -26);
+            for (int r = 1; r < n; ++r)
+                if (std::fabs((double)ck[ck_off[n] + r]) > tiny) R = std::max(R, std::min(r, n - r));
+            ck[ck_off[n] + n] = (float)R;
         }
     }
     double* d_tw;
