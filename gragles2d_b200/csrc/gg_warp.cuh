@@ -422,12 +422,22 @@ __device__ bool extract_warp(const Field<R>& f, const uint32_t* idl, uint32_t ow
 }
 
 constexpr int kBitmapCap = 400;  // words of the padded bitmap (boxes up to about 94 x 94)
-constexpr int kTrace = 640;      // walk steps recorded per warp
+constexpr int kTrace = 768;      // walk steps recorded per warp
 
 struct WalkShared {
     uint32_t bm[kBitmapCap];
-    uint32_t trace[kTrace];
+    uint16_t trace[kTrace];
 };
+
+// Corner mask of the marching-squares cell whose top-left pixel is at padded
+// row tr, padded column lc (C_TL | C_TR from row tr, C_BL | C_BR from tr + 1).
+__device__ __forceinline__ int cell_mask(const uint32_t* bm, int wpr, int tr, int lc) {
+    const uint32_t* rt = bm + tr * wpr + (lc >> 5);
+    const int sh = lc & 31;
+    const uint32_t top2 = __funnelshift_r(rt[0], rt[1], sh);
+    const uint32_t bot2 = __funnelshift_r(rt[wpr], rt[wpr + 1], sh);
+    return (int)((top2 & 3u) | ((bot2 & 3u) << 2));
+}
 
 // Next direction of generateContour's switch for each corner mask
 // (src/marchingSquares.cpp:64-154), two bits per mask; the saddles 6 and 9
@@ -497,47 +507,38 @@ __device__ int extract_bitmap_warp(const Field<R>& f, const uint32_t* idl, uint3
     }
     const int startX = b.x0 + start % w, startY = b.y0 + start / w;
     // lane 0: the walk of generateContour (src/marchingSquares.cpp:44-187) on
-    // the bitmap, in padded coordinates lc = left - x0 + 1, tr = top - y0 + 1
+    // the bitmap, in padded coordinates lc = left - x0 + 1, tr = top - y0 + 1,
+    // recording the cell index tr * (w + 1) + lc of every step (the step's
+    // direction is recovered later from the next recorded cell).  The switch
+    // of the reference is evaluated as selects, so a step has no branch.
+    const int cw = w + 1;
+    if ((hgt + 1) * cw > 65535) return -1;
     int nsteps = 0;
     uint32_t st = 0;
     if (lane == 0) {
         const int lc_end = startX - b.x0, tr_end = startY - b.y0;
         int lc = lc_end, tr = tr_end;
         int next = MS_NONE, prev = MS_NONE;
-        const long limit = 4L * (w + 2) * (hgt + 2) + 16;
-        long it = 0;
+        const int limit = 4 * (w + 2) * (hgt + 2) + 16;
         do {
-            const uint32_t* rt = ws.bm + tr * wpr + (lc >> 5);
-            const int sh = lc & 31;
-            const uint32_t top2 = __funnelshift_r(rt[0], rt[1], sh);
-            const uint32_t bot2 = __funnelshift_r(rt[wpr], rt[wpr + 1], sh);
-            const int mask = (int)((top2 & 3u) | ((bot2 & 3u) << 2));
-            if (mask == (C_BL | C_TR))
-                next = (prev == MS_UP) ? MS_RIGHT : MS_LEFT;
-            else if (mask == (C_BR | C_TL))
-                next = (prev == MS_RIGHT) ? MS_DOWN : MS_UP;
-            else if (mask != 0 && mask != 15)
-                next = (int)((kMsNext >> (2 * mask)) & 3u);
-            const uint32_t emit = (kMsEmit >> mask) & 1u;
-            if (nsteps >= kTrace) {
-                nsteps = -1;
-                break;
-            }
-            ws.trace[nsteps++] = (uint32_t)lc | ((uint32_t)tr << 10) | ((uint32_t)mask << 20) |
-                                 ((uint32_t)next << 24) | (emit << 27);
-            switch (next) {
-                case MS_UP: tr--; break;
-                case MS_DOWN: tr++; break;
-                case MS_LEFT: lc--; break;
-                case MS_RIGHT: lc++; break;
-                default: break;
-            }
+            const int mask = cell_mask(ws.bm, wpr, tr, lc);
+            const int tab = (int)((kMsNext >> (2 * mask)) & 3u);
+            const int s6 = (prev == MS_UP) ? MS_RIGHT : MS_LEFT;
+            const int s9 = (prev == MS_RIGHT) ? MS_DOWN : MS_UP;
+            next = mask == (C_BL | C_TR) ? s6 : mask == (C_BR | C_TL) ? s9 : (mask == 0 || mask == 15) ? next : tab;
+            ws.trace[nsteps] = (uint16_t)(tr * cw + lc);
+            ++nsteps;
+            lc += (next == MS_RIGHT) - (next == MS_LEFT);
+            tr += (next == MS_DOWN) - (next == MS_UP);
             prev = next;
-            if (++it > limit) {
-                st |= S_WALK_LIMIT;
-                break;
-            }
+            if (nsteps >= kTrace || nsteps > limit) break;
         } while (lc != lc_end || tr != tr_end);
+        if (lc != lc_end || tr != tr_end) {
+            if (nsteps >= kTrace)
+                nsteps = -1;  // longer than the trace buffer: walk again in global memory
+            else
+                st |= S_WALK_LIMIT;
+        }
     }
     nsteps = __shfl_sync(0xffffffffu, nsteps, 0);
     if (nsteps < 0) return -1;
@@ -555,12 +556,15 @@ __device__ int extract_bitmap_warp(const Field<R>& f, const uint32_t* idl, uint3
         uint32_t boxes[4] = {0xFFFFFFu, 0xFFFFFFu, 0xFFFFFFu, 0xFFFFFFu};
         int order = 0, left = 0, top = 0;
         if (t < nsteps) {
-            const uint32_t e = ws.trace[t];
-            left = (int)(e & 1023u) - 1 + b.x0;
-            top = (int)((e >> 10) & 1023u) - 1 + b.y0;
-            const int mask = (int)((e >> 20) & 15u);
-            const int next = (int)((e >> 24) & 7u);
-            emit = (e >> 27) & 1u;
+            // the step's direction is the move to the next recorded cell
+            const int c = ws.trace[t], cn = ws.trace[t + 1 < nsteps ? t + 1 : 0];
+            const int tr = c / cw, lc = c - tr * cw;
+            left = lc - 1 + b.x0;
+            top = tr - 1 + b.y0;
+            const int mask = cell_mask(ws.bm, wpr, tr, lc);
+            const int dcell = cn - c;
+            const int next = dcell == -cw ? MS_UP : dcell == cw ? MS_DOWN : dcell == -1 ? MS_LEFT : MS_RIGHT;
+            emit = (kMsEmit >> mask) & 1u;
             const int right = left + 1, bottom = top + 1;
             if (emit) ms_point(f, next, top, bottom, left, right, &px, &py);
             if (__popc(mask) < 3 && bottom >= b.y0 && bottom < b.y1 && top >= b.y0 && top < b.y1 &&
@@ -763,7 +767,7 @@ template <typename R>
 __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_neighbours_w(NetConst C, NetState* S, PointInfo* scratch) {
     __shared__ int s_cid[kGrainsPerBlock][kNbPts];
     __shared__ double s_len[kGrainsPerBlock][kNbPts];
-    __shared__ double s_term[kGrainsPerBlock][kNbPts];
+    const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;
     const int g = blockIdx.x * kGrainsPerBlock + wid + 1;
@@ -780,17 +784,17 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_neighbours_w(NetConst 
     const bool sh = n - 1 <= kNbPts;
     auto CID = [&](int q) -> int& { return sh ? s_cid[wid][q] : info[q].cid; };
     auto LEN = [&](int q) -> double& { return sh ? s_len[wid][q] : info[q].len; };
-    auto TERM = [&](int q) -> double& { return sh ? s_term[wid][q] : info[q].theta; };
-    // area terms (computeVolume, src/grainBoundary.cpp:201-213)
-    for (int i = lane; i < n - 1; i += 32) TERM(i) = (P[i].y + P[i + 1].y) * (P[i].x - P[i + 1].x);
-    __syncwarp();
-    double newVolume = 0;
-    if (lane == 0) {
-        double v = 0;
-        for (int i = 0; i < n - 1; i++) v += TERM(i);
-        newVolume = fabs(fabs(v) * h * h * 0.5);
+    // area (computeVolume, src/grainBoundary.cpp:201-213): terms side by side,
+    // added in contour order
+    double v = 0;
+    for (int i0 = 0; i0 < n - 1; i0 += 32) {
+        const int i = i0 + lane;
+        double t = 0;
+        if (i < n - 1) t = (P[i].y + P[i + 1].y) * (P[i].x - P[i + 1].x);
+        const int m = n - 1 - i0 < 32 ? n - 1 - i0 : 32;
+        for (int q = 0; q < m; ++q) v += __shfl_sync(FULL, t, q);
     }
-    __syncwarp();
+    const double newVolume = fabs(fabs(v) * h * h * 0.5);
     // probes; the first failing point ends the reference's loop
     int first_bad = 0x7fffffff;
     for (int i = lane; i < n - 1; i += 32) {
@@ -821,56 +825,63 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_neighbours_w(NetConst 
     first_bad = warp_min_i(first_bad);
     const int upto = first_bad < n - 1 ? first_bad : n - 1;
     __syncwarp();
-    // physics of the points before the first failure; energy terms of all points
-    for (int i = lane; i < n - 1; i += 32) {
-        const double dx = P[i].x - P[i + 1].x, dy = P[i].y - P[i + 1].y;
-        const double len = sqrt(dx * dx + dy * dy);
-        double energy = -1.0;  // generatePoint's value, kept where the loop never reached
-        if (i < upto) {
-            const double theta = grain_misorientation(qg, C.quat + 4 * (int64_t)CID(i));
-            P[i].mob = mobility_model(theta, C);
-            energy = read_shockley(theta, C);
-            P[i].energy = energy;
-            LEN(i) = len * h;
+    // physics of the points before the first failure; energy terms of all
+    // points, added in contour order (computeEnergy, src/grainBoundary.cpp:215-222)
+    double energy_sum = 0;
+    for (int i0 = 0; i0 < n - 1; i0 += 32) {
+        const int i = i0 + lane;
+        double term = 0;
+        if (i < n - 1) {
+            const double dx = P[i].x - P[i + 1].x, dy = P[i].y - P[i + 1].y;
+            const double len = sqrt(dx * dx + dy * dy);
+            double energy = -1.0;  // generatePoint's value, kept where the loop never reached
+            if (i < upto) {
+                const double theta = grain_misorientation(qg, C.quat + 4 * (int64_t)CID(i));
+                P[i].mob = mobility_model(theta, C);
+                energy = read_shockley(theta, C);
+                P[i].energy = energy;
+                LEN(i) = len * h;
+            }
+            term = len * energy * h;
         }
-        TERM(i) = len * energy * h;
+        const int m = n - 1 - i0 < 32 ? n - 1 - i0 : 32;
+        for (int q = 0; q < m; ++q) energy_sum += __shfl_sync(FULL, term, q);
     }
     __syncwarp();
-    // the list is built in shared memory (one entry per distinct neighbour)
-    // and written out once, so lane 0 never re-reads its own global stores
+    // neighbour list in first-occurrence order (one entry per distinct
+    // neighbour, at most `cap`; later new neighbours are dropped), then each
+    // entry's length summed over its points in contour order
     __shared__ int s_nid[kGrainsPerBlock][48];
-    __shared__ double s_nlen[kGrainsPerBlock][48];
-    __shared__ int s_first[kGrainsPerBlock][48];
     const int cap = C.nbmax < 48 ? C.nbmax : 48;
     int nn = 0;
     bool overflow = false;
-    if (lane == 0) {
-        for (int i = 0; i < upto; i++) {
-            const int cid = CID(i);
-            int e = 0;
-            for (; e < nn; ++e)
-                if (s_nid[wid][e] == cid) break;
-            if (e == nn) {
-                if (nn >= cap) {
-                    overflow = true;
-                    continue;
-                }
-                s_nid[wid][nn] = cid;
-                s_nlen[wid][nn] = 0;
-                s_first[wid][nn] = i;
-                nn++;
-            }
-            s_nlen[wid][e] += LEN(i);
+    const unsigned lt = (1u << lane) - 1u;
+    for (int i0 = 0; i0 < upto; i0 += 32) {
+        const int i = i0 + lane;
+        const int cid = i < upto ? CID(i) : -2;
+        bool fresh = i < upto;
+        for (int e = 0; e < nn && fresh; ++e)
+            if (s_nid[wid][e] == cid) fresh = false;
+        const unsigned same = __match_any_sync(FULL, cid);
+        fresh = fresh && (__ffs(same) - 1) == lane;
+        const unsigned fb = __ballot_sync(FULL, fresh);
+        if (fresh) {
+            const int pos = nn + __popc(fb & lt);
+            if (pos < cap) s_nid[wid][pos] = cid;
         }
+        if (nn + __popc(fb) > cap) overflow = true;
+        nn = min(nn + __popc(fb), cap);
+        __syncwarp();
     }
-    nn = __shfl_sync(0xffffffffu, nn, 0);
-    __syncwarp();
     Neighbour* nb = C.nb + (int64_t)g * C.nbmax;
     for (int e = lane; e < nn; e += 32) {
         const int cid = s_nid[wid][e];
+        double len = 0;
+        for (int i = 0; i < upto; ++i)
+            if (CID(i) == cid) len += LEN(i);
         const double theta = grain_misorientation(qg, C.quat + 4 * (int64_t)cid);
         nb[e].id = cid;
-        nb[e].length = s_nlen[wid][e];
+        nb[e].length = len;
         nb[e].energy = read_shockley(theta, C);
         nb[e].misori = theta;
         nb[e].mobility = mobility_model(theta, C);
@@ -884,9 +895,7 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_neighbours_w(NetConst 
         P[n - 1].energy = P[0].energy;
         P[n - 1].mob = P[0].mob;
     }
-    double energy = 0;
-    for (int i = 0; i < n - 1; i++) energy += TERM(i);
-    C.energy[g] = energy;
+    C.energy[g] = energy_sum;
     double dA = newVolume - C.volume[g];
     dA = dA / C.dt;
     dA = dA * (3 / kPi);
