@@ -27,6 +27,7 @@ struct ConstSector {
 struct InterpSector {
     int left, right;
     int lb, rb;  // left/right boundary constant sector (-1 if none)
+    int len0, len1;  // segments summed into length: len0 .. len1 forward (len0 = -1: none)
     double length;
     double left_w, right_w, boundary_w;
 };
@@ -348,10 +349,11 @@ __device__ void build_sectors_warp(const NetConst& C, const NbTable& T, const CP
             InterpSector nr;
             {
                 double dist = 0;
-                int j = secR.left;
+                int j = secR.left, last = -1;
                 long it = 0;
                 for (; dist <= C.isr; j = wrap_next(j, real)) {
                     dist += seg[j];
+                    last = j;
                     if (++it > guard) {
                         st |= S_SECTOR_GUARD;
                         break;
@@ -361,16 +363,19 @@ __device__ void build_sectors_warp(const NetConst& C, const NbTable& T, const CP
                 nr.right = secR.left;
                 nr.lb = -1;
                 nr.rb = iR;
+                nr.len0 = last < 0 ? -1 : secR.left;
+                nr.len1 = last;
                 nr.length = dist;
             }
             // secL.generateRightInterpolatingContour (src/contourSector.cpp:145-168)
             InterpSector nl;
             {
                 double dist = 0;
-                int j = secL.right;
+                int j = secL.right, last = -1;
                 long it = 0;
                 for (; dist <= C.isr; j = wrap_prev(j, real)) {
                     dist += seg[wrap_prev(j, real)];
+                    last = wrap_prev(j, real);
                     if (++it > guard) {
                         st |= S_SECTOR_GUARD;
                         break;
@@ -380,6 +385,8 @@ __device__ void build_sectors_warp(const NetConst& C, const NbTable& T, const CP
                 nl.right = wrap_prev(j, real);
                 nl.lb = iL;
                 nl.rb = -1;
+                nl.len0 = last;
+                nl.len1 = last < 0 ? -1 : wrap_prev(secL.right, real);
                 nl.length = dist;
             }
             bool merged = false;
@@ -401,14 +408,17 @@ __device__ void build_sectors_warp(const NetConst& C, const NbTable& T, const CP
                 r.right = secR.left;
                 r.rb = iR;
                 double dist = 0;
-                int it = 0;
+                int it = 0, last = -1;
                 for (int j = r.right; j != r.left; j = wrap_next(j, real)) {
                     dist += seg[wrap_prev(j, real)];
+                    last = wrap_prev(j, real);
                     if (++it > size + 1) {
                         st |= S_SECTOR_GUARD;
                         break;
                     }
                 }
+                r.len0 = last < 0 ? -1 : wrap_prev(r.right, real);
+                r.len1 = last;
                 r.length = dist;
                 out0 = r;
                 cnt = 1;

@@ -135,6 +135,8 @@ struct NetConst {
     const float* ck;         // separable real-space kernel per n at ck_off[n] (batched form)
     const int64_t* ck_off;
     void* ptinfo;            // per-contour-point probe scratch (contCur offsets), 32 bytes each
+    double* dvol;            // tangent mode: d area / d p_k of the last level set, 4 per grain (else null)
+    double* dseg;            // tangent mode: d segment length / d p_k, 4 per previous-contour point (scratch)
 };
 
 // Per-step rotating state, resident in device memory (kernels read it
@@ -184,6 +186,15 @@ struct NetState {
     unsigned long long t_area;    // traffic model scratch (k_traffic)
     unsigned long long t_overlap;
     unsigned long long t_exists;
+    // tangent fields d phi / d p_k of the four calibration parameters (plain
+    // form only; null unless enabled): 4 x phi_cap doubles each, parameter k
+    // at offset k * phi_cap, same per-grain offsets as phiA / phiB
+    void* dphiA;
+    void* dphiB;
+    // tangents of the contour points (8 doubles per point: dx / dp_k, then
+    // dy / dp_k), same offsets and rotation as contPrev / contCur
+    double* dcontPrev;
+    double* dcontCur;
 };
 
 GG_HD void set_status(NetState* S, uint32_t bits) {

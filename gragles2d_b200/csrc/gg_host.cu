@@ -42,6 +42,7 @@ struct gg_ctx {
     int N = 0, nn = 0, m = 0, b = 0, ppg = 0;
     double h = 0, dt = 0, delta = 0, ds = 0;
     bool loaded = false, initialised = false;
+    bool tangents = false;  // carry d phi / d p_k (plain form; set before distance initialisation)
 
     std::vector<int32_t> ids;     // nn*nn
     std::vector<double> euler;    // 3 per grain
@@ -650,6 +651,17 @@ int gg_distance_initialisation(gg_ctx* c) {
         S.phiA = pa;
         S.phiB = pb;
         S.spec = sp_;
+        if (c->tangents) {  // zero tangents: the initial field does not depend on the parameters
+            double *da, *db;
+            ALLOC(da, 4 * (size_t)phi_cap);
+            ALLOC(db, 4 * (size_t)phi_cap);
+            S.dphiA = da;
+            S.dphiB = db;
+            ALLOC(C.dvol, 4 * (size_t)(N + 1));
+            ALLOC(S.dcontPrev, 8 * (size_t)cont_cap);
+            ALLOC(S.dcontCur, 8 * (size_t)cont_cap);
+            ALLOC(C.dseg, 4 * (size_t)cont_cap);
+        }
     } else {
         float *pa, *pb, *sp_;
         ALLOC(pa, phi_cap);
@@ -846,6 +858,7 @@ int gg_grain_updates(gg_ctx* c, int64_t* updates) {
 int gg_profile_steps(gg_ctx* c, int32_t loop, int32_t nsteps, double* stage_ms) {
     if (!c || !stage_ms) return GG_E_INVALID;
     if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
+    if (c->tangents) return fail(c, GG_E_STATE, "stage profiling runs without tangents");
     int rc = set_loop(c, loop);
     if (rc) return rc;
     cudaEvent_t ev[GG_NSTAGES + 1];
@@ -896,6 +909,32 @@ int gg_dims(gg_ctx* c, int32_t* n_grains, int32_t* ngridpoints, double* h, doubl
     if (h) *h = c->h;
     if (delta) *delta = c->delta;
     if (dt) *dt = c->dt;
+    return GG_OK;
+}
+
+int gg_tangent_enable(gg_ctx* c, int32_t enable) {
+    if (!c) return GG_E_INVALID;
+    if (c->initialised) return fail(c, GG_E_STATE, "tangents must be enabled before gg_distance_initialisation");
+    if (enable && c->P.precision != GG_PRECISION_PLAIN)
+        return fail(c, GG_E_INVALID, "tangents need the plain (FP64) form");
+    c->tangents = enable != 0;
+    return GG_OK;
+}
+
+int gg_read_area_tangents(gg_ctx* c, double* out, int32_t capacity) {
+    if (!c || !out) return GG_E_INVALID;
+    if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
+    if (!c->tangents || !c->C.dvol) return fail(c, GG_E_STATE, "tangents not enabled");
+    const int N = c->N;
+    if (capacity < 4 * N) return fail(c, GG_E_INVALID, "capacity smaller than 4 x grain count");
+    std::vector<double> dv(4 * (size_t)(N + 1));
+    GG_CUDA(c, cudaMemcpyAsync(dv.data(), c->C.dvol, sizeof(double) * dv.size(), cudaMemcpyDeviceToHost, c->stream));
+    GG_CUDA(c, cudaStreamSynchronize(c->stream));
+    const double per_degree = kPiH / 180.0;  // the kernels differentiate in radians
+    for (int g = 1; g <= N; ++g) {
+        out[4 * (g - 1) + 0] = dv[4 * (size_t)g + 0] * per_degree;
+        for (int k = 1; k < 4; ++k) out[4 * (g - 1) + k] = dv[4 * (size_t)g + k];
+    }
     return GG_OK;
 }
 

@@ -28,7 +28,7 @@ __device__ __forceinline__ R* phiB_of(NetState* S) {
 // Row r2c, column DFT and Gaussian multiply, inverse column DFT, row c2r.
 // ---------------------------------------------------------------------------
 template <typename R>
-__global__ void __launch_bounds__(256) k_conv_dft(NetConst C, NetState* S) {
+__global__ void __launch_bounds__(256) k_conv_dft(NetConst C, NetState* S, int tk = -1) {
     const int g = blockIdx.x + 1;
     if (g > C.N || C.state[g] != G_EXISTS || halted(S)) return;
     const Box bx = S->box_cur[g];
@@ -39,8 +39,9 @@ __global__ void __launch_bounds__(256) k_conv_dft(NetConst C, NetState* S) {
         return;
     }
     const int half = n / 2 + 1;
-    const R* in = phiA_of<R>(S) + S->off_cur[g];
-    R* out = phiB_of<R>(S) + S->off_cur[g];
+    // tk >= 0: the same (linear) convolution of tangent field tk
+    const R* in = (tk < 0 ? phiA_of<R>(S) : reinterpret_cast<R*>(S->dphiA) + tk * S->phi_cap) + S->off_cur[g];
+    R* out = (tk < 0 ? phiB_of<R>(S) : reinterpret_cast<R*>(S->dphiB) + tk * S->phi_cap) + S->off_cur[g];
     R* s1 = reinterpret_cast<R*>(S->spec) + S->soff_cur[g];  // n x half complex
     R* s2 = s1 + 2 * (int64_t)n * half;                        // n x half complex
     const double* w = C.tw + 2 * C.tw_off[n];
@@ -730,12 +731,18 @@ __global__ void __launch_bounds__(1024) k_finalize(NetConst C, NetState* S, int 
     void* tp = S->phiA;
     S->phiA = S->phiB;
     S->phiB = tp;
+    tp = S->dphiA;
+    S->dphiA = S->dphiB;
+    S->dphiB = tp;
     uint32_t* ti = S->idPrev;
     S->idPrev = S->idCur;
     S->idCur = ti;
     CPoint* tc = S->contPrev;
     S->contPrev = S->contCur;
     S->contCur = tc;
+    double* tdc = S->dcontPrev;
+    S->dcontPrev = S->dcontCur;
+    S->dcontCur = tdc;
     int64_t* tco = S->coff_prev;
     S->coff_prev = S->coff_cur;
     S->coff_cur = S->coff_new;

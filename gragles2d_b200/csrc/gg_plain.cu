@@ -4,6 +4,7 @@
 #include "gg_corrector.cuh"
 #include "gg_kernels.cuh"
 #include "gg_launch.cuh"
+#include "gg_tangent.cuh"
 #include "gg_warp.cuh"
 
 namespace gg {
@@ -12,6 +13,9 @@ __global__ void k_swap_phi(NetState* S) {
     void* t = S->phiA;
     S->phiA = S->phiB;
     S->phiB = t;
+    t = S->dphiA;
+    S->dphiA = S->dphiB;
+    S->dphiB = t;
 }
 
 cudaError_t swap_phi(NetState* dS, cudaStream_t s) {
@@ -76,20 +80,36 @@ cudaError_t plain_stages(const NetConst& C, NetState* dS, int stages, cudaStream
     const int gblocks = (C.N + gt - 1) / gt;
     const int wblocks = (C.N + kGrainsPerBlock - 1) / kGrainsPerBlock;
     (void)gblocks;
+    // tangent mode (C.dvol set): the tangent kernels of gg_tangent.cuh follow
+    // their stages; the corrector's tangent reads the uncorrected convolution,
+    // so it runs first
+    const bool tan = C.dvol != nullptr;
     if (stages & ST_CONV) {
         k_conv_dft<double><<<C.N, cfg.conv_threads, 0, s>>>(C, dS);
+        if (tan)
+            for (int tk = 0; tk < kNP; ++tk) k_conv_dft<double><<<C.N, cfg.conv_threads, 0, s>>>(C, dS, tk);
         if (!C.isotropic) {
+            if (tan) k_corrector_t<<<C.N, 128, 0, s>>>(C, dS);
             cudaError_t e = plain_corrector(C, dS, s);
             if (e != cudaSuccess) return e;
         }
     }
     if (stages & ST_SECOND) k_second_order_w<<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS);
-    if (stages & ST_COMPARE) k_compare<double><<<C.N, cfg.compare_threads, 0, s>>>(C, dS);
-    if (stages & ST_LEVELSET) k_levelset_w<double><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS);
+    if (stages & ST_COMPARE) {
+        k_compare<double><<<C.N, cfg.compare_threads, 0, s>>>(C, dS);
+        if (tan) k_compare_t<<<C.N, 256, 0, s>>>(C, dS);
+    }
+    if (stages & ST_LEVELSET) {
+        k_levelset_w<double><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS);
+        if (tan) k_area_t<<<(C.N + 127) / 128, 128, 0, s>>>(C, dS);
+    }
     if (stages & ST_REDIST) {
         k_alloc<<<1, 1024, 0, s>>>(C, dS, 2);
         k_neighbours_w<double><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS, reinterpret_cast<PointInfo*>(C.ptinfo));
-        k_redistance_s<double><<<C.N, kRedistThreads, kRedistSmemBytes, s>>>(C, dS);
+        if (tan)
+            k_redistance_t<<<C.N, 64, 0, s>>>(C, dS);
+        else
+            k_redistance_s<double><<<C.N, kRedistThreads, kRedistSmemBytes, s>>>(C, dS);
         k_finalize<<<1, 1024, 0, s>>>(C, dS, 1);
     }
     return cudaGetLastError();

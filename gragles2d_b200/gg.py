@@ -27,7 +27,8 @@ EXPORTS = (
     "gg_params_default", "gg_params_from_xml", "gg_create", "gg_destroy", "gg_last_error", "gg_load_voxels",
     "gg_load_voxel_files", "gg_distance_initialisation", "gg_find_neighbors", "gg_set_neighbours",
     "gg_convolution", "gg_update_second_order_neighbors", "gg_comparison", "gg_level_set", "gg_redistancing",
-    "gg_grain_count", "gg_step", "gg_status", "gg_read_grain_stats", "gg_dims", "gg_dump", "gg_last_step_ms",
+    "gg_grain_count", "gg_step", "gg_status", "gg_read_grain_stats", "gg_tangent_enable", "gg_read_area_tangents",
+    "gg_dims", "gg_dump", "gg_last_step_ms",
     "gg_grain_updates", "gg_profile_steps", "gg_traffic", "gg_convolve_box_static",
 )
 STATIC_CONV_MAX_N = 128
@@ -105,6 +106,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "gg_step": (I, [V, I, I]),
         "gg_status": (I, [V, P(ctypes.c_uint32), I]),
         "gg_read_grain_stats": (I, [V, P(GrainStats), I]),
+        "gg_tangent_enable": (I, [V, I]),
+        "gg_read_area_tangents": (I, [V, P(D), I]),
         "gg_dims": (I, [V, P(I), P(I), P(D), P(D), P(D)]),
         "gg_dump": (I, [V, ctypes.c_char_p, I, I]),
         "gg_last_step_ms": (I, [V, P(D)]),
@@ -300,6 +303,19 @@ class GrainHandler:
     def areas(self) -> np.ndarray:
         st = self.grain_stats()
         return np.array([s.area if s.state == 1 else np.nan for s in st])
+
+    def enable_tangents(self, on: bool = True):
+        """Carry d phi / d p for p = (theta_ref [deg], HAGB energy, HAGB
+        mobility, triple-point drag); call before distanceInitialisation."""
+        self._check(self.lib.gg_tangent_enable(self.ctx, int(on)))
+
+    def area_tangents(self) -> np.ndarray:
+        """d area_g / d p of the last level set, shape (N, 4), row g-1 for grain g."""
+        n = self.dims().n_grains
+        out = np.zeros(4 * n, np.float64)
+        self._check(self.lib.gg_read_area_tangents(self.ctx, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                                   out.size))
+        return out.reshape(n, 4)
 
     def grain_updates(self) -> int:
         v = ctypes.c_int64()

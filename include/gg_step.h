@@ -179,6 +179,21 @@ int gg_status(gg_ctx* ctx, uint32_t* status, int32_t clear);
 
 /* Per-grain scalars for grains 1..N (out has room for N entries). */
 int gg_read_grain_stats(gg_ctx* ctx, gg_grain_stats* out, int32_t capacity);
+/*
+ * Parameter derivatives (no counterpart in the reference, which has no
+ * derivative; the calibration interface the drop-in adds).  With tangents
+ * enabled (before gg_distance_initialisation; plain form only), every step
+ * also carries d phi / d p for p = (ThetaRefDegrees, HAGB_RelativeEnergy,
+ * HAGB_RelativeMobility, TriplePointDrag): the tangent-linear step with the
+ * step's discrete decisions fixed (comparison winners, contour edges,
+ * redistancing candidates, corrector sectors).  gg_read_area_tangents
+ * returns d area_g / d p of the contour of the last level set, 4 values per
+ * grain for g = 1..N in that parameter order (theta per degree); capacity
+ * counts doubles.  A loss gradient is sum_g dL/darea_g * out[4 (g-1) + k].
+ */
+int gg_tangent_enable(gg_ctx* ctx, int32_t enable);
+int gg_read_area_tangents(gg_ctx* ctx, double* out, int32_t capacity);
+
 /* Number of grain slots N and the grid size (ngridpoints). */
 int gg_dims(gg_ctx* ctx, int32_t* n_grains, int32_t* ngridpoints, double* h, double* delta, double* dt);
 

@@ -1,0 +1,133 @@
+"""Parameter derivatives of the plain FP64 step (gg_tangent_enable /
+gg_read_area_tangents) against central finite differences of the same
+forward run, per grain and through a calibration loss wrapped in a
+torch.autograd.Function (test harness only).
+
+Case: mob_v30 (30 grains on 120^2, Read-Shockley energy, mobility model,
+triple-junction drag 5), 8 steps.  Parameters: ThetaRefDegrees,
+HAGB_RelativeEnergy, HAGB_RelativeMobility, TriplePointDrag.
+"""
+import os
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from gragles2d_b200 import gg
+
+pytestmark = pytest.mark.gpu
+
+CASE = "mob_v30"
+STEPS = 8
+NAMES = ("theta_ref_deg", "gamma_hagb", "m_hagb", "triple_point_drag")
+
+
+def _xml(golden_dir):
+    return os.path.join(golden_dir, CASE, CASE + ".xml")
+
+
+def _run(xml, params, tangents=False):
+    h = gg.GrainHandler(gg.Settings(xml, precision=gg.PRECISION_PLAIN, **params), device=0)
+    try:
+        h.load_voxel_files()
+        if tangents:
+            h.enable_tangents()
+        h.distanceInitialisation()
+        h.find_neighbors()
+        h.step(STEPS)
+        areas = np.array([s.area if s.state == 1 else np.nan for s in h.grain_stats()])
+        tang = h.area_tangents() if tangents else None
+    finally:
+        h.close()
+    return areas, tang
+
+
+@pytest.fixture(scope="module")
+def base(golden_dir):
+    xml = _xml(golden_dir)
+    s = gg.Settings(xml)
+    p0 = {k: float(getattr(s.p, k)) for k in NAMES}
+    areas, tang = _run(xml, p0, tangents=True)
+    return xml, p0, areas, tang
+
+
+def _central(xml, p0, name, rel):
+    hk = p0[name] * rel
+    ap, _ = _run(xml, {**p0, name: p0[name] + hk})
+    am, _ = _run(xml, {**p0, name: p0[name] - hk})
+    return (ap - am) / (2 * hk)
+
+
+def test_tangent_run_keeps_the_forward_values(base, golden_dir):
+    """Carrying tangents changes nothing in the forward result."""
+    xml, p0, areas, _ = base
+    plain, _ = _run(xml, p0)
+    np.testing.assert_array_equal(areas, plain)
+
+
+@pytest.mark.parametrize("k", range(4))
+def test_area_tangents_match_central_differences(base, k):
+    """Per grain, d area / d p against central differences with h = 1e-5
+    relative (the discrete decisions, held fixed by the tangents, stay put
+    at that step): median relative error <= 1e-5, every grain <= 1e-3."""
+    xml, p0, areas, tang = base
+    fd = _central(xml, p0, NAMES[k], 1e-5)
+    m = np.isfinite(fd) & np.isfinite(tang[:, k])
+    assert m.sum() >= 25
+    scale = np.abs(fd[m]).max()
+    rel = np.abs(tang[m, k] - fd[m]) / np.maximum(np.abs(fd[m]), 1e-3 * scale)
+    assert np.median(rel) <= 1e-5, (NAMES[k], np.median(rel))
+    assert rel.max() <= 1e-3, (NAMES[k], rel.max())
+
+
+class FinalAreas(torch.autograd.Function):
+    """Final grain areas of a STEPS-step plain run as a function of the four
+    parameters; backward is J^T g with J = d area / d p from the tangents."""
+
+    @staticmethod
+    def forward(ctx, params, xml):
+        p = {n: float(v) for n, v in zip(NAMES, params.tolist())}
+        areas, tang = _run(xml, p, tangents=True)
+        ctx.save_for_backward(torch.from_numpy(np.nan_to_num(tang)))
+        return torch.from_numpy(areas)
+
+    @staticmethod
+    def backward(ctx, grad_areas):
+        (jac,) = ctx.saved_tensors
+        return torch.nan_to_num(grad_areas) @ jac, None
+
+
+def test_calibration_loss_gradient(base, golden_dir):
+    """Loss sum_g (A_g - A*_g)^2 with the targets A* from a run at
+    (12 deg, 1, 0.8, 0.3); the autograd gradient through the tangents
+    agrees with central differences of the loss (h = 1e-6 relative) to 1e-4."""
+    xml, p0, _, _ = base
+    target_params = {**p0, "theta_ref_deg": 12.0, "m_hagb": 0.8, "triple_point_drag": 0.3}
+    target, _ = _run(xml, target_params)
+    tgt = torch.from_numpy(target)
+    params = torch.tensor([p0[n] for n in NAMES], dtype=torch.float64, requires_grad=True)
+    areas = FinalAreas.apply(params, xml)
+    alive = torch.isfinite(areas) & torch.isfinite(tgt)
+    loss = ((areas - tgt)[alive] ** 2).sum()
+    loss.backward()
+    grad = params.grad.numpy()
+
+    def loss_at(p):
+        a, _ = _run(xml, p)
+        m = np.isfinite(a) & np.isfinite(target)
+        return float(((a - target)[m] ** 2).sum())
+
+    for k, name in enumerate(NAMES):
+        hk = p0[name] * 1e-6
+        fd = (loss_at({**p0, name: p0[name] + hk}) - loss_at({**p0, name: p0[name] - hk})) / (2 * hk)
+        assert abs(grad[k] - fd) <= 1e-4 * abs(fd) + 1e-14, (name, grad[k], fd)
+
+
+def test_tangents_need_the_plain_form(golden_dir):
+    h = gg.GrainHandler(gg.Settings(_xml(golden_dir), precision=gg.PRECISION_BATCHED), device=0)
+    try:
+        with pytest.raises(gg.GGError):
+            h.enable_tangents()
+    finally:
+        h.close()
