@@ -250,6 +250,10 @@ def run_ours(args, rank, world, local_rank):
     both = np.isfinite(areas_b) & np.isfinite(areas_p) & (areas_p > 0)
     rel = np.abs(areas_b - areas_p) / np.where(areas_p > 0, areas_p, 1.0)
     area_err = float(np.max(rel[both])) if both.any() else None
+    # relative error is only meaningful while a grain has some cells left:
+    # also report it over grains of at least 25 cells in both forms
+    big = both & (areas_p >= 25.0 / (w["grid"] ** 2)) & (areas_b >= 25.0 / (w["grid"] ** 2))
+    area_err_big = float(np.max(rel[big])) if big.any() else None
     px = 1.0 / (w["grid"] ** 2)  # area of one grid cell in domain units
     worst = [int(i) for i in np.argsort(np.where(both, rel, -1))[::-1][:5]]
     area_diag = {"grains_compared": int(both.sum()),
@@ -257,6 +261,7 @@ def run_ours(args, rank, world, local_rank):
                  "alive_only_batched": int((np.isfinite(areas_b) & ~np.isfinite(areas_p)).sum()),
                  "p50": float(np.median(rel[both])), "p99": float(np.quantile(rel[both], 0.99)),
                  "over_1e-3": int((rel[both] > 1e-3).sum()),
+                 "max_abs_px": float(np.max(np.abs(areas_b - areas_p)[both]) / px) if both.any() else None,
                  "worst": [{"id": i + 1, "area_px_plain": float(areas_p[i] / px),
                             "area_px_batched": float(areas_b[i] / px), "rel": float(rel[i]),
                             "regular_plain": int(reg_p[i]), "regular_batched": int(reg_b[i])} for i in worst]}
@@ -308,11 +313,14 @@ def run_ours(args, rank, world, local_rank):
         "plain_fp64": {"value": upd_p / (ms_p / 1e3), "ms_per_step": ms_p / kp, "steps": kp},
         "batched_vs_plain": (upd_b / (t_ms / 1e3)) / (upd_p / (ms_p / 1e3)),
         "area_rel_err_max": area_err,
+        "area_rel_err_max_ge_25px": area_err_big,
         "area_err_detail": area_diag,
         "clocks": clk.summary(),
         "gpu_launches": (9 if aniso else 8) * K,
         "status": status_b,
     }
+    if not args.no_gradient:
+        out["gradient"] = gradient_check(device)
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(xml, args.cpu_steps)
     return out
@@ -370,6 +378,70 @@ def run_reference(args, rank, world):
 
 PROFILE_CASE = dict(name="voronoi_5000g_1800_rs15", grains=5000, grid=1800, seed=4, iso=0, mobility=0, tpd=0.0)
 
+GRAD_PARAMS = ("theta_ref_deg", "gamma_hagb", "m_hagb", "triple_point_drag")
+
+
+def gradient_check(device: int) -> dict:
+    """Parameter derivatives of the plain FP64 step (tangent mode) against
+    central differences (h = 1e-5 relative) on the committed 30-grain
+    mobility-model case, 8 steps; and the cost of carrying the four tangents
+    on the 5,000-grain Voronoi case (20 steps) next to the plain step."""
+    from gragles2d_b200 import gg
+
+    xml = os.path.join(ROOT, "tests", "golden", "mob_v30", "mob_v30.xml")
+    steps = 8
+
+    def run(params, tangents=False):
+        h = gg.GrainHandler(gg.Settings(xml, precision=gg.PRECISION_PLAIN, **params), device=device)
+        h.load_voxel_files()
+        if tangents:
+            h.enable_tangents()
+        h.distanceInitialisation()
+        h.find_neighbors()
+        h.step(steps)
+        a = np.array([x.area if x.state == 1 else np.nan for x in h.grain_stats()])
+        t = h.area_tangents() if tangents else None
+        h.close()
+        return a, t
+
+    s = gg.Settings(xml)
+    p0 = {k: float(getattr(s.p, k)) for k in GRAD_PARAMS}
+    areas, tang = run(p0, True)
+    target, _ = run({**p0, "theta_ref_deg": 12.0, "m_hagb": 0.8, "triple_point_drag": 0.3})
+    alive = np.isfinite(areas) & np.isfinite(target)
+    per_param = {}
+    for k, name in enumerate(GRAD_PARAMS):
+        hk = p0[name] * 1e-5
+        ap, _ = run({**p0, name: p0[name] + hk})
+        am, _ = run({**p0, name: p0[name] - hk})
+        fd = (ap - am) / (2 * hk)
+        m = np.isfinite(fd) & np.isfinite(tang[:, k])
+        rel = np.abs(tang[m, k] - fd[m]) / np.maximum(np.abs(fd[m]), 1e-3 * np.abs(fd[m]).max())
+        g_t = float(np.sum(2 * (areas - target)[alive] * tang[alive, k]))
+        lp = float(np.nansum(((ap - target)[alive]) ** 2))
+        lm = float(np.nansum(((am - target)[alive]) ** 2))
+        g_fd = (lp - lm) / (2 * hk)
+        per_param[name] = {"area_rel_err_median": float(np.median(rel)), "area_rel_err_max": float(rel.max()),
+                           "loss_grad": g_t, "loss_grad_fd": g_fd,
+                           "loss_grad_rel_err": abs(g_t - g_fd) / max(abs(g_fd), 1e-300)}
+    # cost of the tangents at scale
+    pxml, _ = workload_case(PROFILE_CASE)
+    cost = {}
+    for tangents in (False, True):
+        h = gg.GrainHandler(gg.Settings(pxml, precision=gg.PRECISION_PLAIN), device=device)
+        h.load_voxel_files()
+        if tangents:
+            h.enable_tangents()
+        h.distanceInitialisation()
+        h.find_neighbors()
+        h.step(3)
+        cost["tangent" if tangents else "plain"] = h.step(20) / 20
+        h.close()
+    return {"form": "tangent-linear (forward mode), plain FP64", "case": "mob_v30: 30 grains, 120^2, "
+            "Read-Shockley + mobility model + drag 5, 8 steps; loss sum (A - A*)^2, A* at (12 deg, 1, 0.8, 0.3)",
+            "fd": "central, h = 1e-5 relative", "params": per_param,
+            "ms_per_step_5000g": cost}
+
 
 def run_profile_case(args, local_rank):
     """Small case for ncu captures: 5,000 grains on 1800^2 (Read-Shockley),
@@ -397,6 +469,7 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=20)
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-gradient", action="store_true", help="skip the parameter-derivative check")
     ap.add_argument("--ref-max-steps", type=int, default=6)
     ap.add_argument("--profile-case", action="store_true", help="small stage-by-stage run for ncu captures")
     ap.add_argument("--profile-plain", action="store_true")
