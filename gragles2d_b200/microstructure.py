@@ -86,7 +86,7 @@ def _label_nearest(seeds: np.ndarray, nn: int, chunk_rows: int = 256) -> np.ndar
         y1 = min(nn, y0 + chunk_rows)
         ys = (np.arange(y0, y1, dtype=np.float64) + 0.5) / nn
         pts = np.stack(np.meshgrid(xs, ys), axis=-1).reshape(-1, 2)
-        _, idx = tree.query(pts, k=1)
+        _, idx = tree.query(pts, k=1, workers=-1)
         labels[y0:y1] = (idx.astype(np.int32) + 1).reshape(y1 - y0, nn)
     return labels
 

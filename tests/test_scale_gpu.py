@@ -1,0 +1,81 @@
+"""The larger configurations at full size, through size-independent checks.
+
+- 50,000 grains on 5600^2 (Voronoi, seed 3), Read-Shockley energy with the
+  mobility model and triple-junction drag Lambda = 0.1 (TriplePointDrag =
+  Lambda / a, a = 0.69 / sqrt(N) the mean edge length of a Poisson-Voronoi
+  tessellation of the unit square): batched FP32 and plain FP64 side by side.
+- 100,000 grains on 8192^2 from a Matern cluster process (radius 0.01, 100
+  daughters per cluster on average, 95% of the seeds) mixed with uniform
+  seeds: equivalent diameters lognormal-like with sigma ~0.6 and boxes from
+  about 16 to 250 cells; batched FP32.
+
+Checks: no device status bit, the grains still tile the domain (sum of areas
+within 2e-3 of the unit square and drifting by less than 1e-3), and for the
+first configuration the per-grain area agreement of the two forms.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from gragles2d_b200 import gg
+from gragles2d_b200 import microstructure as ms
+
+pytestmark = pytest.mark.gpu
+
+
+def _case(root, name, micro, **params):
+    d = os.path.join(root, name)
+    return ms.make_case(d, name, micro, NumberOfTimesteps=10, **params)
+
+
+@pytest.fixture(scope="module")
+def cases(tmp_path_factory):
+    root = str(tmp_path_factory.mktemp("scale"))
+    n4 = 50000
+    c4 = _case(root, "voronoi_50000g_5600", ms.voronoi(n4, 5600, 3), IsIsotropicNetwork=0, UseMobilityModel=1,
+               TriplePointDrag=round(0.1 / (0.69 / np.sqrt(n4)), 3))
+    m3 = ms.clustered(100000, 8192, 5, cluster_fraction=0.95, cluster_radius=0.01, mean_daughters=100.0)
+    dia = ms.equivalent_diameters(m3)
+    c3 = _case(root, "clustered_100000g_8192", m3, IsIsotropicNetwork=0)
+    return {"c4": c4, "c3": c3, "c3_dia": dia}
+
+
+def _run(xml, precision, steps):
+    h = gg.GrainHandler(gg.Settings(xml, precision=precision), device=0)
+    try:
+        h.load_voxel_files()
+        h.distanceInitialisation()
+        h.find_neighbors()
+        a0 = np.nansum([s.area for s in h.grain_stats() if s.state == 1])
+        h.step(steps)
+        st = h.grain_stats()
+        areas = np.array([s.area if s.state == 1 else np.nan for s in st])
+        edges = np.array([s.box[1] - s.box[0] for s in st if s.state == 1])
+        return {"status": h.status(), "a0": a0, "areas": areas, "edges": edges}
+    finally:
+        h.close()
+
+
+def test_50000_grains_batched_and_plain(cases):
+    b = _run(cases["c4"], gg.PRECISION_BATCHED, 5)
+    p = _run(cases["c4"], gg.PRECISION_PLAIN, 5)
+    for r in (b, p):
+        assert r["status"] == 0
+        assert abs(r["a0"] - 1.0) < 2e-3
+        assert abs(np.nansum(r["areas"]) - r["a0"]) < 1e-3
+    assert np.array_equal(np.isfinite(b["areas"]), np.isfinite(p["areas"]))
+    m = np.isfinite(b["areas"]) & (p["areas"] > 25.0 / 5600**2)
+    rel = np.abs(b["areas"][m] - p["areas"][m]) / p["areas"][m]
+    assert np.median(rel) < 1e-5
+    assert np.quantile(rel, 0.99) < 1e-3
+
+
+def test_100000_clustered_grains_batched(cases):
+    dia = cases["c3_dia"]
+    assert 0.5 < np.std(np.log(dia[dia > 0])) < 0.7
+    r = _run(cases["c3"], gg.PRECISION_BATCHED, 3)
+    assert r["status"] == 0
+    assert r["edges"].min() <= 24 and r["edges"].max() >= 200
+    assert abs(r["a0"] - 1.0) < 2e-3
+    assert abs(np.nansum(r["areas"]) - r["a0"]) < 1e-3
