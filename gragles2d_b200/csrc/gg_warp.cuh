@@ -996,14 +996,24 @@ __device__ void redistance_sweeps(const R* __restrict__ in, int in_x0, int in_y0
     const int iymax = (bi.y1 < bo.y1) ? bi.y1 : bo.y1;
 #define GG_IN(i, j) in[(int64_t)((i) - in_y0) * si + ((j) - in_x0)]
 #define GG_OUT(i, j) out[(int64_t)((i) - bo.y0) * so + ((j) - bo.x0)]
+    // Each recurrence carries its running value in a register; the loads of
+    // the next step (which no store of the current step touches) are issued
+    // one step ahead so their latency overlaps the current step.
     for (int j = ixmin + (int)threadIdx.x; j < bo.x1; j += blockDim.x) {
+        const bool col_in = j < ixmax;
         if (iymin < bo.y1 - 1) {  // y forward
             R cur = GG_OUT(iymin, j);
+            R nxt = GG_OUT(iymin + 1, j);
+            R a = (R)0, c = (R)0;
+            if (col_in && iymin < iymax - 1) {
+                a = GG_IN(iymin, j);
+                c = GG_IN(iymin + 1, j);
+            }
             for (int i = iymin; i < bo.y1 - 1; i++) {
-                R nxt = GG_OUT(i + 1, j);
+                const R nxt_n = i + 2 < bo.y1 ? GG_OUT(i + 2, j) : (R)0;
+                const R c_n = (col_in && i + 1 < iymax - 1) ? GG_IN(i + 2, j) : (R)0;
                 R cand;
-                if (j < ixmax && i < iymax - 1) {
-                    const R a = GG_IN(i, j), c = GG_IN(i + 1, j);
+                if (col_in && i < iymax - 1) {
                     if (a * c <= (R)0.0) {
                         const R slope = (c - a) / h;
                         const R dz = -a / slope;
@@ -1021,15 +1031,21 @@ __device__ void redistance_sweeps(const R* __restrict__ in, int in_x0, int in_y0
                     GG_OUT(i + 1, j) = nxt;
                 }
                 cur = nxt;
+                nxt = nxt_n;
+                a = c;
+                c = c_n;
             }
         }
         if (iymax - 1 > bo.y0) {  // y backward
             R cur = GG_OUT(iymax - 1, j);
+            R prv = GG_OUT(iymax - 2, j);
+            R ip = (col_in && iymax - 1 > iymin) ? GG_IN(iymax - 2, j) : (R)0;
             for (int i = iymax - 1; i > bo.y0; i--) {
-                R prv = GG_OUT(i - 1, j);
+                const R prv_n = i - 2 >= bo.y0 ? GG_OUT(i - 2, j) : (R)0;
+                const R ip_n = (col_in && i - 1 > iymin) ? GG_IN(i - 2, j) : (R)0;
                 R cand;
-                if (j < ixmax && i > iymin)
-                    cand = cur + ((R)sgn(GG_IN(i - 1, j)) * h);
+                if (col_in && i > iymin)
+                    cand = cur + ((R)sgn(ip) * h);
                 else
                     cand = cur + ((R)sgn(prv) * h);
                 if (fabs(cand) < fabs(prv)) {
@@ -1037,18 +1053,27 @@ __device__ void redistance_sweeps(const R* __restrict__ in, int in_x0, int in_y0
                     GG_OUT(i - 1, j) = prv;
                 }
                 cur = prv;
+                prv = prv_n;
+                ip = ip_n;
             }
         }
     }
     __syncthreads();
     for (int i = iymin + (int)threadIdx.x; i < bo.y1; i += blockDim.x) {
+        const bool row_in = i < iymax;
         if (ixmin < bo.x1 - 1) {  // x forward
             R cur = GG_OUT(i, ixmin);
+            R nxt = GG_OUT(i, ixmin + 1);
+            R a = (R)0, c = (R)0;
+            if (row_in && ixmin < ixmax - 1) {
+                a = GG_IN(i, ixmin);
+                c = GG_IN(i, ixmin + 1);
+            }
             for (int j = ixmin; j < bo.x1 - 1; j++) {
-                R nxt = GG_OUT(i, j + 1);
+                const R nxt_n = j + 2 < bo.x1 ? GG_OUT(i, j + 2) : (R)0;
+                const R c_n = (row_in && j + 1 < ixmax - 1) ? GG_IN(i, j + 2) : (R)0;
                 R cand;
-                if (j < ixmax - 1 && i < iymax) {
-                    const R a = GG_IN(i, j), c = GG_IN(i, j + 1);
+                if (j < ixmax - 1 && row_in) {
                     if (a * c <= (R)0.0) {
                         const R slope = (c - a) / h;
                         const R dz = -a / slope;
@@ -1066,15 +1091,21 @@ __device__ void redistance_sweeps(const R* __restrict__ in, int in_x0, int in_y0
                     GG_OUT(i, j + 1) = nxt;
                 }
                 cur = nxt;
+                nxt = nxt_n;
+                a = c;
+                c = c_n;
             }
         }
         if (ixmax - 1 > bo.x0) {  // x backward
             R cur = GG_OUT(i, ixmax - 1);
+            R prv = GG_OUT(i, ixmax - 2);
+            R ip = (ixmax - 1 > ixmin && row_in) ? GG_IN(i, ixmax - 2) : (R)0;
             for (int j = ixmax - 1; j > bo.x0; j--) {
-                R prv = GG_OUT(i, j - 1);
+                const R prv_n = j - 2 >= bo.x0 ? GG_OUT(i, j - 2) : (R)0;
+                const R ip_n = (j - 1 > ixmin && row_in) ? GG_IN(i, j - 2) : (R)0;
                 R cand;
-                if (j > ixmin && i < iymax)
-                    cand = cur + ((R)sgn(GG_IN(i, j - 1)) * h);
+                if (j > ixmin && row_in)
+                    cand = cur + ((R)sgn(ip) * h);
                 else
                     cand = cur + (R)sgn(prv) * h;
                 if (fabs(cand) < fabs(prv)) {
@@ -1082,6 +1113,8 @@ __device__ void redistance_sweeps(const R* __restrict__ in, int in_x0, int in_y0
                     GG_OUT(i, j - 1) = prv;
                 }
                 cur = prv;
+                prv = prv_n;
+                ip = ip_n;
             }
         }
     }
