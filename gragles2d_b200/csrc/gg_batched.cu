@@ -530,4 +530,31 @@ cudaError_t batched_stages(const NetConst& C, NetState* dS, int stages, cudaStre
     return cudaGetLastError();
 }
 
+cudaError_t batched_step_graph(const NetConst& C, NetState* dS, cudaStream_t s, cudaStream_t s2, cudaEvent_t* ev,
+                               const LaunchCfg& cfg) {
+    if (C.N <= 0) return cudaSuccess;
+    const int wblocks = (C.N + kGrainsPerBlock - 1) / kGrainsPerBlock;
+    cudaError_t e;
+    // second-order lists (lists and boxes only) beside convolution + corrector (fields)
+    if ((e = cudaEventRecord(ev[0], s)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(s2, ev[0], 0)) != cudaSuccess) return e;
+    k_second_order_w<<<wblocks, 32 * kGrainsPerBlock, 0, s2>>>(C, dS);
+    if ((e = cudaEventRecord(ev[1], s2)) != cudaSuccess) return e;
+    k_conv_sep<<<C.N, 128, conv_sep_smem(C.tmax), s>>>(C, dS);
+    if (!C.isotropic) k_corrector_f<<<C.N, 128, 0, s>>>(C, dS);
+    if ((e = cudaStreamWaitEvent(s, ev[1], 0)) != cudaSuccess) return e;
+    k_compare<float><<<C.N, cfg.compare_threads, 0, s>>>(C, dS);
+    k_levelset_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS);
+    k_alloc<<<1, 1024, 0, s>>>(C, dS, 1);
+    // volume / energy / neighbours (contours, lists) beside redistancing (fields)
+    if ((e = cudaEventRecord(ev[2], s)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(s2, ev[2], 0)) != cudaSuccess) return e;
+    k_neighbours_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s2>>>(C, dS, reinterpret_cast<PointInfo*>(C.ptinfo));
+    if ((e = cudaEventRecord(ev[3], s2)) != cudaSuccess) return e;
+    k_redistance_s<float><<<C.N, kRedistThreads, kRedistSmemBytes, s>>>(C, dS);
+    if ((e = cudaStreamWaitEvent(s, ev[3], 0)) != cudaSuccess) return e;
+    k_finalize<<<1, 1024, 0, s>>>(C, dS, 1);
+    return cudaGetLastError();
+}
+
 }  // namespace gg

@@ -57,6 +57,8 @@ struct gg_ctx {
 
     cudaGraphExec_t graph = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaStream_t stream2 = nullptr;  // second branch of the captured batched step
+    cudaEvent_t fork[4] = {nullptr, nullptr, nullptr, nullptr};
     double last_ms = 0;
 
     ~gg_ctx() {
@@ -64,6 +66,9 @@ struct gg_ctx {
         for (void* p : allocs) cudaFree(p);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        for (cudaEvent_t e : fork)
+            if (e) cudaEventDestroy(e);
+        if (stream2) cudaStreamDestroy(stream2);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -328,6 +333,8 @@ int gg_create(const gg_params* p, int device, gg_ctx** out) {
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking);
+    for (int k = 0; k < 4 && e == cudaSuccess; ++k) e = cudaEventCreateWithFlags(&c->fork[k], cudaEventDisableTiming);
     if (e != cudaSuccess) {
         c->err = std::string("stream/event: ") + cudaGetErrorString(e);
         *out = c;
@@ -811,7 +818,7 @@ int gg_step(gg_ctx* c, int32_t loop, int32_t nsteps) {
         if (!c->graph) {
             cudaGraph_t gr;
             GG_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-            cudaError_t e = batched_stages(c->C, c->dS, ST_ALL, c->stream, c->cfg);
+            cudaError_t e = batched_step_graph(c->C, c->dS, c->stream, c->stream2, c->fork, c->cfg);
             cudaError_t e2 = cudaStreamEndCapture(c->stream, &gr);
             if (e != cudaSuccess) return cuda_fail(c, e, "capture");
             if (e2 != cudaSuccess) return cuda_fail(c, e2, "end capture");

@@ -31,6 +31,11 @@ cudaError_t plain_stages(const NetConst& C, NetState* dS, int stages, cudaStream
 cudaError_t plain_init(const NetConst& C, NetState* dS, const int32_t* d_ids, cudaStream_t s);
 cudaError_t plain_corrector(const NetConst& C, NetState* dS, cudaStream_t s);
 cudaError_t batched_stages(const NetConst& C, NetState* dS, int stages, cudaStream_t s, const LaunchCfg& cfg);
+// The whole batched step for graph capture on s, with the independent stages
+// (second-order lists beside convolution + corrector, volume / energy /
+// neighbours beside redistancing) forked onto s2 through the events ev[0..3].
+cudaError_t batched_step_graph(const NetConst& C, NetState* dS, cudaStream_t s, cudaStream_t s2, cudaEvent_t* ev,
+                               const LaunchCfg& cfg);
 size_t conv_sep_smem(int tmax);
 cudaError_t batched_prepare(int tmax);
 cudaError_t batched_init(const NetConst& C, NetState* dS, const int32_t* d_ids, cudaStream_t s);
