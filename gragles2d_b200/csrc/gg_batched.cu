@@ -181,7 +181,7 @@ size_t conv_sep_smem(int tmax) {
 // nearest-vertex search as one: chunks of 8 contour points whose bounding box
 // is farther from the tile than every lane's best point so far are skipped
 // by all lanes together.
-constexpr int kCorrMaxPts = 1024;
+constexpr int kCorrMaxPts = 512;
 
 constexpr int kChunk = 8;  // contour points per bounding box of the nearest-vertex search
 
@@ -331,7 +331,7 @@ __device__ __forceinline__ int project_warp(const float2* P, const float4* cbb, 
     return seg;
 }
 
-__global__ void __launch_bounds__(128, 6) k_corrector_f(NetConst C, NetState* S) {
+__global__ void __launch_bounds__(128, 8) k_corrector_f(NetConst C, NetState* S) {
     const int g = blockIdx.x + 1;
     if (g > C.N || C.state[g] != G_EXISTS || C.regular[g] == 0 || S->loop == 0 || halted(S)) return;
     __shared__ SectorSet sec;

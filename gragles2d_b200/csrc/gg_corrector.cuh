@@ -15,7 +15,7 @@ namespace {  // internal linkage: each form's translation unit has its own copy
 constexpr int kMaxConstSectors = 32;
 constexpr int kMaxSectorJunctions = 24;
 constexpr int kMaxInterpSectors = 2 * kMaxConstSectors;
-constexpr int kSegShared = 1024;  // contours up to this length keep their segment lengths in shared memory
+constexpr int kSegShared = 512;  // contours up to this length keep their segment lengths in shared memory
 
 struct ConstSector {
     int left, right;  // contour point IDs (-1, -1: whole contour)
@@ -44,7 +44,7 @@ struct SectorSet {
 // an interpolating sector, the partial sum of segment lengths from the
 // sector's right point up to the segment, accumulated in the same order as
 // ContourSector::getWeight (src/contourSector.cpp:242-246).
-constexpr int kSegTable = 1024;
+constexpr int kSegTable = 512;
 struct SegTable {
     short sector[kSegTable];  // >= 0 constant, <= -2 interpolating (-2 - q), -1 none
     double acc[kSegTable];
