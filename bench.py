@@ -65,6 +65,13 @@ def workload_case(w: dict) -> tuple[str, dict]:
     return xml, w
 
 
+def workload_config(w: dict, world: int) -> dict:
+    """The `config` of both arms' JSON lines (the same workload)."""
+    return {"workload": "20000-grain Voronoi (seed 1) on 3600x3600, Read-Shockley 15 deg, "
+                        "batched FP32 graph-captured step", "grains": w["grains"], "grid": w["grid"],
+            "l2": "working set larger than L2 (no flush)", "parallelism": f"replicas{world}"}
+
+
 def load_inputs(xml: str):
     """Host buffers of the voxelized input (ids, euler, bbox)."""
     from gragles2d_b200 import microstructure as ms
@@ -298,9 +305,7 @@ def run_ours(args, rank, world, local_rank):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": "20000-grain Voronoi (seed 1) on 3600x3600, Read-Shockley 15 deg, "
-                               "batched FP32 graph-captured step", "grains": w["grains"], "grid": w["grid"],
-                   "l2": "working set larger than L2 (no flush)", "parallelism": f"replicas{world}"},
+        "config": workload_config(w, world),
         "e2e": {"value": aggregate_throughput(world, upd_e2e, t_e2e * 1e3), "unit": METRIC, "h2d_bytes_per_step": h2d / (W + K),
                 "d2h_bytes_per_step": stats_bytes / (W + K),
                 "includes": "load from host buffers + distance init + neighbour search + W+K steps with "
@@ -370,8 +375,7 @@ def run_reference(args, rank, world):
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "20000-grain Voronoi (seed 1) on 3600x3600, Read-Shockley 15 deg",
-                       "grains": w["grains"], "grid": w["grid"]},
+            "config": workload_config(w, world),
             "cpu_baseline": cb,
             "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
