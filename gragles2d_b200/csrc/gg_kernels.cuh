@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(256) k_compare(NetConst C, NetState* S) {
     const int g = blockIdx.x + 1;
     if (g > C.N || C.state[g] != G_EXISTS || halted(S)) return;
     __shared__ Box s_box[kListMaxSmem];
-    __shared__ int64_t s_off[kListMaxSmem];
+    __shared__ int64_t s_org[kListMaxSmem];  // arena index of the member's pixel (0, 0)
     __shared__ int s_id[kListMaxSmem];
     __shared__ int s_red[4][8];
     const int K = C.kmax;
@@ -197,9 +197,10 @@ __global__ void __launch_bounds__(256) k_compare(NetConst C, NetState* S) {
         const int id = C.cmp_ids[(int64_t)g * K + k];
         C.sec_ids[(int64_t)g * K + k] = id;  // m_secondOrderNeighbours = m_comparisonList
         if (k < kListMaxSmem) {
+            const Box bk = S->box_cur[id];
             s_id[k] = id;
-            s_box[k] = S->box_cur[id];
-            s_off[k] = S->off_cur[id];
+            s_box[k] = bk;
+            s_org[k] = S->off_cur[id] - ((int64_t)bk.y0 * (bk.x1 - bk.x0) + bk.x0);
         }
     }
     if (threadIdx.x == 0) C.sec_n[g] = C.cmp_n[g];
@@ -231,8 +232,16 @@ __global__ void __launch_bounds__(256) k_compare(NetConst C, NetState* S) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const int hgt = box_h(bc);
     const int ntx = (w + 7) >> 3, ntiles = ntx * ((hgt + 3) >> 2);
+    int tcol = warp % ntx, trow = warp / ntx;  // tile t = trow * ntx + tcol, advanced without division
+    const int dcol = nwarps % ntx, drow = nwarps / ntx;
     for (int t = warp; t < ntiles; t += nwarps) {
-        const int tx0 = bc.x0 + (t % ntx) * 8, ty0 = bc.y0 + (t / ntx) * 4;
+        const int tx0 = bc.x0 + tcol * 8, ty0 = bc.y0 + trow * 4;
+        tcol += dcol;
+        trow += drow;
+        if (tcol >= ntx) {
+            tcol -= ntx;
+            ++trow;
+        }
         const int tx1 = min(tx0 + 8, bc.x1), ty1 = min(ty0 + 4, bc.y1);
         const int j = tx0 + (lane & 7), i = ty0 + (lane >> 3);
         const bool inside = j < tx1 && i < ty1;
@@ -267,7 +276,7 @@ __global__ void __launch_bounds__(256) k_compare(NetConst C, NetState* S) {
                         const Box bk = s_box[ks[u]];
                         if (i >= bk.y0 && i < bk.y1 && j >= bk.x0 && j < bk.x1) {
                             ok[u] = true;
-                            ds[u] = conv[s_off[ks[u]] + (int64_t)(i - bk.y0) * (bk.x1 - bk.x0) + (j - bk.x0)];
+                            ds[u] = conv[s_org[ks[u]] + (int64_t)i * (bk.x1 - bk.x0) + j];
                         }
                     }
                 }
@@ -304,7 +313,7 @@ __global__ void __launch_bounds__(256) k_compare(NetConst C, NetState* S) {
                 id = 0u;
             }
         }
-        const R v = (fabs((double)in) < (double)tube) ? (R)0.5 * (in - out) : in;
+        const R v = (fabs(in) < tube) ? (R)0.5 * (in - out) : in;  // tube = (R)(0.7 delta): same test as in double
         cmpo[p] = v;
         idc[p] = id;
         if (v >= 0) {
