@@ -36,7 +36,7 @@ constexpr size_t kScratchDoubles = kSpecDoubles + kTwDoubles + kGDoubles;
 // The fixed device scratch.  In host code this name is only a host-side
 // stand-in for the symbol, not a device address: the address used by kernels
 // comes from cudaGetSymbolAddress on each device (see scratch_on_device).
-__device__ __align__(256) double g_conv_scratch[kScratchDoubles];
+static __device__ __align__(256) double g_conv_scratch[kScratchDoubles];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
