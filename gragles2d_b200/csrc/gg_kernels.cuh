@@ -462,66 +462,101 @@ __global__ void k_levelset(NetConst C, NetState* S) {
 // (distance fields), spectral scratch and contour capacities; one CTA.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(1024) k_alloc(NetConst C, NetState* S, int spec_per_complex) {
-    __shared__ int64_t s_a[1024], s_s[1024], s_c[1024];
+    // Exclusive prefix sums over slots 0..N of the new box areas, spectral
+    // scratch sizes and contour capacities of existing grains.  Each warp owns
+    // a contiguous run of slots and reads it 32 consecutive slots at a time
+    // (coalesced); pass 1 totals each run, warp 0 scans the 32 totals, pass 2
+    // scans every 32-slot piece with shuffles and writes the offsets.
+    __shared__ int64_t s_tot[32][3];
+    __shared__ int64_t s_base[32][3];
     const int N = C.N;
-    const int T = blockDim.x;
-    const int per = (N + T) / T;  // slots 0..N
-    const int g0 = threadIdx.x * per;
-    const int g1 = min(N + 1, g0 + per);
-    int64_t a = 0, sp = 0, c = 0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int slots = N + 1;
+    const int run = ((slots + nw - 1) / nw + 31) & ~31;
+    const int r0 = warp * run, r1 = min(slots, r0 + run);
+    auto sizes = [&](int g, int64_t* a, int64_t* sp, int64_t* c, int* cc, bool* range) {
+        *a = 0;
+        *sp = 0;
+        *c = 0;
+        *cc = 0;
+        if (g >= 1 && g <= N && C.state[g] == G_EXISTS) {
+            const Box bx = S->box_new[g];
+            const int n = box_w(bx);
+            *a = box_area(bx);
+            *sp = (int64_t)spec_per_complex * 2 * (int64_t)n * (n / 2 + 1);
+            *cc = contour_capacity(n);
+            *c = *cc;
+            if (n > C.tmax) *range = true;
+        }
+    };
     bool range = false;
-    for (int g = g0; g < g1; ++g) {
-        if (g >= 1 && C.state[g] == G_EXISTS) {
-            const Box bx = S->box_new[g];
-            const int n = box_w(bx);
-            a += box_area(bx);
-            sp += (int64_t)spec_per_complex * 2 * (int64_t)n * (n / 2 + 1);
-            c += contour_capacity(n);
-            if (n > C.tmax) range = true;
-        }
+    int64_t ta = 0, ts = 0, tc = 0;
+    for (int g0 = r0; g0 < r1; g0 += 32) {
+        int64_t a, sp, c;
+        int cc;
+        sizes(g0 + lane < r1 ? g0 + lane : -1, &a, &sp, &c, &cc, &range);
+        ta += a;
+        ts += sp;
+        tc += c;
     }
-    s_a[threadIdx.x] = a;
-    s_s[threadIdx.x] = sp;
-    s_c[threadIdx.x] = c;
+    for (int o = 16; o > 0; o >>= 1) {
+        ta += __shfl_xor_sync(0xffffffffu, ta, o);
+        ts += __shfl_xor_sync(0xffffffffu, ts, o);
+        tc += __shfl_xor_sync(0xffffffffu, tc, o);
+    }
+    if (lane == 0) {
+        s_tot[warp][0] = ta;
+        s_tot[warp][1] = ts;
+        s_tot[warp][2] = tc;
+    }
     __syncthreads();
-    for (int o = 1; o < T; o <<= 1) {
-        int64_t va = 0, vs = 0, vc = 0;
-        if ((int)threadIdx.x >= o) {
-            va = s_a[threadIdx.x - o];
-            vs = s_s[threadIdx.x - o];
-            vc = s_c[threadIdx.x - o];
+    if (warp == 0) {
+        int64_t v[3] = {0, 0, 0};
+        if (lane < nw)
+            for (int q = 0; q < 3; ++q) v[q] = s_tot[lane][q];
+        int64_t inc[3] = {v[0], v[1], v[2]};
+        for (int o = 1; o < 32; o <<= 1)
+            for (int q = 0; q < 3; ++q) {
+                const int64_t u = __shfl_up_sync(0xffffffffu, inc[q], o);
+                if (lane >= o) inc[q] += u;
+            }
+        if (lane < nw)
+            for (int q = 0; q < 3; ++q) s_base[lane][q] = inc[q] - v[q];
+        if (lane == 31) {
+            if (inc[0] > S->phi_cap || inc[1] > S->spec_cap || inc[2] > S->cont_cap) set_status(S, S_ARENA_FULL);
+            S->phi_used = inc[0];
+            S->spec_used = inc[1];
+            S->cont_used = inc[2];
         }
-        __syncthreads();
-        s_a[threadIdx.x] += va;
-        s_s[threadIdx.x] += vs;
-        s_c[threadIdx.x] += vc;
-        __syncthreads();
     }
-    int64_t ra = s_a[threadIdx.x] - a, rs = s_s[threadIdx.x] - sp, rc = s_c[threadIdx.x] - c;
-    for (int g = g0; g < g1; ++g) {
-        S->off_new[g] = ra;
-        S->soff_new[g] = rs;
-        S->coff_new[g] = rc;
-        if (g >= 1 && C.state[g] == G_EXISTS) {
-            const Box bx = S->box_new[g];
-            const int n = box_w(bx);
-            ra += box_area(bx);
-            rs += (int64_t)spec_per_complex * 2 * (int64_t)n * (n / 2 + 1);
-            const int cc = contour_capacity(n);
-            S->ccap_new[g] = cc;
-            rc += cc;
-        } else {
-            S->ccap_new[g] = 0;
+    __syncthreads();
+    int64_t ba = s_base[warp][0], bs = s_base[warp][1], bc = s_base[warp][2];
+    for (int g0 = r0; g0 < r1; g0 += 32) {
+        const int g = g0 + lane;
+        int64_t a, sp, c;
+        int cc;
+        sizes(g < r1 ? g : -1, &a, &sp, &c, &cc, &range);
+        int64_t ia = a, is = sp, ic = c;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t ua = __shfl_up_sync(0xffffffffu, ia, o), us = __shfl_up_sync(0xffffffffu, is, o),
+                          uc = __shfl_up_sync(0xffffffffu, ic, o);
+            if (lane >= o) {
+                ia += ua;
+                is += us;
+                ic += uc;
+            }
         }
+        if (g < r1) {
+            S->off_new[g] = ba + ia - a;
+            S->soff_new[g] = bs + is - sp;
+            S->coff_new[g] = bc + ic - c;
+            S->ccap_new[g] = cc;
+        }
+        ba += __shfl_sync(0xffffffffu, ia, 31);
+        bs += __shfl_sync(0xffffffffu, is, 31);
+        bc += __shfl_sync(0xffffffffu, ic, 31);
     }
     if (range) set_status(S, S_TABLE_RANGE);
-    if (threadIdx.x == T - 1) {
-        if (s_a[T - 1] > S->phi_cap || s_s[T - 1] > S->spec_cap || s_c[T - 1] > S->cont_cap)
-            set_status(S, S_ARENA_FULL);
-        S->phi_used = s_a[T - 1];
-        S->spec_used = s_s[T - 1];
-        S->cont_used = s_c[T - 1];
-    }
 }
 
 // ---------------------------------------------------------------------------
