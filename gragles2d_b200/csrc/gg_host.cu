@@ -133,6 +133,36 @@ void euler2quaternion(const double* e, double* q) {
     q[3] = co1 * sin((p1 + p2) / 2);
 }
 
+// Quaternion to Euler (Bunge ZXZ, Diebel's (3,1,3) case), with the branch for
+// sin(PHI) = 0 where phi1 + phi2 alone is defined and phi2 is set to 0:
+// Quaternion::quaternion2EulerConst (src/Quaternion.cpp:242-289).  Angles in
+// [0, 2 pi).
+void quaternion2euler(const double* q, double* e) {
+    const double q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3];
+    double cosPHI = q3 * q3 - q2 * q2 - q1 * q1 + q0 * q0;
+    const double y0 = 2 * q1 * q3 - 2 * q0 * q2;
+    const double x0 = 2 * q2 * q3 + 2 * q0 * q1;
+    const double y1 = 2 * q1 * q3 + 2 * q0 * q2;
+    const double x1 = -2 * q2 * q3 + 2 * q0 * q1;
+    if (cosPHI > 1.) cosPHI = 1.;
+    const double one_minus = 1. - cosPHI;
+    const double PHI = one_minus * one_minus <= 1e-20 ? 0. : acos(cosPHI);  // QUAT2EUL_ETA, src/mymath.h:31
+    const double sP = sin(PHI);
+    double phi1, phi2;
+    if (sP != 0) {
+        phi2 = atan2(y0 / sP, x0 / sP);
+        phi1 = atan2(y1 / sP, x1 / sP);
+    } else {
+        phi1 = atan2((2 * q1 * q2 + 2 * q0 * q3), q0 * q0 + q1 * q1 - q2 * q2 - q3 * q3);
+        phi2 = 0.;
+    }
+    if (phi1 < 0.0) phi1 += 2 * kPiH;
+    if (phi2 < 0.0) phi2 += 2 * kPiH;
+    e[0] = phi1;
+    e[1] = PHI;
+    e[2] = phi2;
+}
+
 // DimensionalBuffer::resizeToSquare (src/dimensionalBuffer.h:123-160)
 Box host_resize_to_square(Box r, int maximumLength) {
     int grid_size = maximumLength - 1;
@@ -267,6 +297,7 @@ int gg_params_from_xml(const char* path, gg_params* p) {
         geti("NumberOfParticles", &p->number_of_particles);
         geti("NumberOfPointsPerGrain", &p->number_of_points_per_grain);
         geti("AnalysisTimestep", &p->analysis_timestep);
+        geti("DiscreteSamplingRate", &p->discrete_sampling_rate);
         geti("NumberOfTimesteps", &p->number_of_timesteps);
         geti("BreakupNumber", &p->breakup_number);
         geti("DomainBorderSize", &p->domain_border_size);
@@ -324,6 +355,7 @@ int gg_create(const gg_params* p, int device, gg_ctx** out) {
     if (p->precision != GG_PRECISION_PLAIN && p->precision != GG_PRECISION_BATCHED) return bad("bad precision");
     if (p->domain_border_size < 1) return bad("DomainBorderSize must be >= 1");
     if (p->analysis_timestep <= 0) return bad("AnalysisTimestep must be > 0");
+    if (p->discrete_sampling_rate < 0) return bad("DiscreteSamplingRate must be >= 0");
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) {
         c->err = std::string("cudaSetDevice: ") + cudaGetErrorString(e);
@@ -545,6 +577,8 @@ int gg_distance_initialisation(gg_ctx* c) {
     ALLOC(C.sec_ids, (size_t)C.kmax * (N + 1));
     ALLOC(C.nb_n, N + 1);
     ALLOC(C.nb, (size_t)C.nbmax * (N + 1));
+    ALLOC(C.gone_loop, N + 1);
+    GG_CUDA(c, cudaMemsetAsync(C.gone_loop, 0xff, sizeof(int32_t) * (N + 1), c->stream));
 
     // tables: twiddles and Gaussian multipliers (plain), separable kernels (batched)
     std::vector<int64_t> tw_off(tmax + 1, 0), gk_off(tmax + 1, 0), ck_off(tmax + 1, 0);
@@ -942,6 +976,105 @@ int gg_read_area_tangents(gg_ctx* c, double* out, int32_t capacity) {
         out[4 * (g - 1) + 0] = dv[4 * (size_t)g + 0] * per_degree;
         for (int k = 1; k < 4; ++k) out[4 * (g - 1) + k] = dv[4 * (size_t)g + k];
     }
+    return GG_OK;
+}
+
+int gg_write_analysis(gg_ctx* c, const char* directory, int32_t loop) {
+    if (!c || !directory) return GG_E_INVALID;
+    if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
+    int rc = refresh_state(c);
+    if (rc) return rc;
+    if (loop < c->P.start_time || c->hS.loop != loop + 1)
+        return fail(c, GG_E_STATE, "loop is not the last completed step");
+    const int N = c->N;
+    const bool aniso = c->P.is_isotropic_network == 0;
+    const NetConst& C = c->C;
+    std::vector<int32_t> state(N + 1), reg(N + 1), bnd(N + 1), nbn(N + 1), gone(N + 1);
+    std::vector<double> vol(N + 1), en(N + 1), per(N + 1), mda(N + 1);
+    std::vector<Neighbour> nb;
+    auto d2h = [&](void* dst, const void* src, size_t bytes) {
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream);
+    };
+    GG_CUDA(c, d2h(state.data(), C.state, 4 * (N + 1)));
+    GG_CUDA(c, d2h(reg.data(), C.regular, 4 * (N + 1)));
+    GG_CUDA(c, d2h(bnd.data(), C.inter_bnd, 4 * (N + 1)));
+    GG_CUDA(c, d2h(nbn.data(), C.nb_n, 4 * (N + 1)));
+    GG_CUDA(c, d2h(gone.data(), C.gone_loop, 4 * (N + 1)));
+    GG_CUDA(c, d2h(vol.data(), C.volume, 8 * (N + 1)));
+    GG_CUDA(c, d2h(en.data(), C.energy, 8 * (N + 1)));
+    GG_CUDA(c, d2h(per.data(), C.perimeter, 8 * (N + 1)));
+    GG_CUDA(c, d2h(mda.data(), C.meanda, 8 * (N + 1)));
+    if (c->P.discrete_sampling_rate > 0) {
+        nb.resize((size_t)C.nbmax * (N + 1));
+        GG_CUDA(c, d2h(nb.data(), C.nb, sizeof(Neighbour) * nb.size()));
+    }
+    GG_CUDA(c, cudaStreamSynchronize(c->stream));
+
+    const std::string dir(directory);
+    const std::string tex_path = dir + "/Texture_" + std::to_string(loop) + ".ori";
+    const std::string modf_path = dir + "/MODF_" + std::to_string(loop) + ".txt";
+    const std::string stats_path = dir + "/NrGrains&EnergyStatistics.txt";
+    std::ofstream tex(tex_path);
+    if (!tex) return fail(c, GG_E_IO, "cannot write " + tex_path);
+    // save_Texture (src/grainhdl.cpp:871-1023): one line per existing grain
+    // with regular motion; the MODF takes half of each boundary length in the
+    // bin of its misorientation and is renormalised to unit sum after every
+    // grain.
+    const int nbins = c->P.discrete_sampling_rate;
+    const double dh = 62.8 / (double)nbins;  // LatticeType 0
+    std::vector<double> modf(nbins, 0.0);
+    double total_energy = 0.0;
+    for (int g = 1; g <= N; ++g) {
+        if (state[g] != G_EXISTS || reg[g] == 0) continue;
+        total_energy += en[g];
+        double eul[3], q[4];
+        euler2quaternion(&c->euler[3 * (size_t)(g - 1)], q);
+        quaternion2euler(q, eul);
+        if (nbins > 0) {
+            // ExplicitGrainBoundary::calculateDiscreteEnergyDistribution
+            // (src/grainBoundary.cpp:578-598): lengths summed per bin in
+            // neighbour order, bins visited in ascending order
+            std::vector<std::pair<int, double>> local;
+            const Neighbour* L = nb.data() + (size_t)g * C.nbmax;
+            for (int e = 0; e < nbn[g]; ++e) {
+                const int key = (int)((L[e].misori * 180 / kPiH) / dh - 0.5);
+                auto it = std::find_if(local.begin(), local.end(), [&](const auto& kv) { return kv.first == key; });
+                if (it == local.end()) local.emplace_back(key, L[e].length);
+                else it->second += L[e].length;
+            }
+            std::sort(local.begin(), local.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+            for (const auto& kv : local)
+                if (kv.first >= 0 && kv.first < nbins) modf[kv.first] += kv.second / 2;
+        }
+        tex << g << '\t' << nbn[g] << '\t' << (bnd[g] != 0) << '\t' << vol[g] << '\t'
+            << mda[g] / (double)c->P.analysis_timestep << '\t' << per[g] << '\t' << en[g] << '\t' << 0.0
+            << '\t' << eul[0] << '\t' << eul[1] << '\t' << eul[2] << std::endl;
+        double sum = 0.0;
+        for (int i = 0; i < nbins; ++i) sum += modf[i];
+        for (int i = 0; i < nbins; ++i)
+            if (modf[i] > 0) modf[i] = modf[i] / sum;
+    }
+    tex.close();
+    FILE* mf = std::fopen(modf_path.c_str(), "w");
+    if (!mf) return fail(c, GG_E_IO, "cannot write " + modf_path);
+    if (aniso)
+        for (int i = 0; i < nbins; ++i) std::fprintf(mf, "%lf\t%lf\n", (float)(dh * (i + 1)), (float)modf[i]);
+    std::fclose(mf);
+
+    // save_NrGrainsStats (src/grainhdl.cpp:1225-1241): simulated time before
+    // this step's increment (src/grainhdl.cpp:1115-1117), grains present when
+    // the step began (get_biggestGrainVol of the previous step,
+    // src/grainhdl.cpp:1744-1754: vanished grains count until the next level
+    // set deletes them), total energy, grid size
+    int nr = 0;
+    for (int g = 1; g <= N; ++g) nr += (state[g] != G_GONE || gone[g] == loop) ? 1 : 0;
+    const double inc = (c->dt * (c->P.physical_domain_size * c->P.physical_domain_size) /
+                        (c->P.time_slope * c->P.hagb_energy * c->P.hagb_mobility));
+    double realtime = 0.0;
+    for (int l = c->P.start_time; l < loop; ++l) realtime += inc;
+    std::ofstream st(stats_path, loop == 0 ? std::ios::out : std::ios::app);
+    if (!st) return fail(c, GG_E_IO, "cannot write " + stats_path);
+    st << realtime << "\t" << nr << "\t" << 0.5 * total_energy << "\t" << c->nn << std::endl;
     return GG_OK;
 }
 

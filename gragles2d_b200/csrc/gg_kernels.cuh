@@ -401,7 +401,10 @@ __global__ void k_levelset(NetConst C, NetState* S) {
     const int st = C.state[g];
     const Box bc = S->box_cur[g];
     if (st != G_EXISTS) {
-        if (st == G_VANISHED) C.state[g] = G_GONE;  // delete grains[id] (src/grainhdl.cpp:840-842)
+        if (st == G_VANISHED) {  // delete grains[id] (src/grainhdl.cpp:840-842)
+            C.state[g] = G_GONE;
+            C.gone_loop[g] = S->loop;
+        }
         S->box_new[g] = bc;
         S->cn_cur[g] = 0;
         S->jn_cur[g] = 0;

@@ -662,7 +662,10 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_levelset_w(NetConst C,
     const Box bc = S->box_cur[g];
     if (st != G_EXISTS) {
         if (lane == 0) {
-            if (st == G_VANISHED) C.state[g] = G_GONE;
+            if (st == G_VANISHED) {
+                C.state[g] = G_GONE;
+                C.gone_loop[g] = S->loop;
+            }
             S->box_new[g] = bc;
             S->cn_cur[g] = 0;
             S->jn_cur[g] = 0;

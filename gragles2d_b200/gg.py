@@ -28,7 +28,7 @@ EXPORTS = (
     "gg_load_voxel_files", "gg_distance_initialisation", "gg_find_neighbors", "gg_set_neighbours",
     "gg_convolution", "gg_update_second_order_neighbors", "gg_comparison", "gg_level_set", "gg_redistancing",
     "gg_grain_count", "gg_step", "gg_status", "gg_read_grain_stats", "gg_tangent_enable", "gg_read_area_tangents",
-    "gg_dims", "gg_dump", "gg_last_step_ms",
+    "gg_write_analysis", "gg_dims", "gg_dump", "gg_last_step_ms",
     "gg_grain_updates", "gg_profile_steps", "gg_traffic", "gg_convolve_box_static",
 )
 STATIC_CONV_MAX_N = 128
@@ -55,7 +55,7 @@ class Params(ctypes.Structure):
         ("research_mode", ctypes.c_int32), ("research_project", ctypes.c_int32),
         ("decouple_grains", ctypes.c_int32), ("grid_coarsement", ctypes.c_int32),
         ("use_stored_elastic_energy", ctypes.c_int32), ("use_magnetic_field", ctypes.c_int32),
-        ("reserved_i", ctypes.c_int32 * 5),
+        ("discrete_sampling_rate", ctypes.c_int32), ("reserved_i", ctypes.c_int32 * 4),
         ("triple_point_drag", ctypes.c_double), ("constant_sector_radius", ctypes.c_double),
         ("interpolating_sector_radius", ctypes.c_double), ("hagb_energy", ctypes.c_double),
         ("hagb_mobility", ctypes.c_double), ("physical_domain_size", ctypes.c_double),
@@ -108,6 +108,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "gg_read_grain_stats": (I, [V, P(GrainStats), I]),
         "gg_tangent_enable": (I, [V, I]),
         "gg_read_area_tangents": (I, [V, P(D), I]),
+        "gg_write_analysis": (I, [V, ctypes.c_char_p, I]),
         "gg_dims": (I, [V, P(I), P(I), P(D), P(D), P(D)]),
         "gg_dump": (I, [V, ctypes.c_char_p, I, I]),
         "gg_last_step_ms": (I, [V, P(D)]),
@@ -262,13 +263,18 @@ class GrainHandler:
         self.lib.gg_last_step_ms(self.ctx, ctypes.byref(ms))
         return ms.value
 
-    def run_sim(self, steps: int | None = None, stage_calls: bool = False):
+    def run_sim(self, steps: int | None = None, stage_calls: bool = False, analysis_dir: str | None = None):
         """distanceInitialisation, find_neighbors, then the time loop
-        (src/grainhdl.cpp:1035-1142); stops early below BreakupNumber."""
+        (src/grainhdl.cpp:1035-1142); stops early below BreakupNumber.  With
+        `analysis_dir`, writes the texture / MODF / statistics files into it
+        every AnalysisTimestep steps and after step NumberOfTimesteps
+        (src/grainhdl.cpp:1098-1105)."""
         self.distanceInitialisation()
         self.find_neighbors()
-        total = (self.settings.p.number_of_timesteps + 1) if steps is None else steps
+        p = self.settings.p
+        total = (p.number_of_timesteps + 1) if steps is None else steps
         for _ in range(total):
+            loop = self.loop
             if stage_calls:
                 self.convolution()
                 self.updateSecondOrderNeighbors()
@@ -277,6 +283,9 @@ class GrainHandler:
                 self.redistancing()
             else:
                 self.step(1)
+            if analysis_dir is not None and ((loop - p.start_time) % p.analysis_timestep == 0
+                                             or loop == p.number_of_timesteps):
+                self.write_analysis(analysis_dir, loop)
             live, _ = self.get_biggestGrainVol()
             if live < self.settings.p.breakup_number:
                 break
@@ -316,6 +325,11 @@ class GrainHandler:
         self._check(self.lib.gg_read_area_tangents(self.ctx, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                                    out.size))
         return out.reshape(n, 4)
+
+    def write_analysis(self, directory: str, loop: int | None = None):
+        """save_Texture + save_NrGrainsStats of the completed step `loop`
+        (default: the last one) into `directory`."""
+        self._check(self.lib.gg_write_analysis(self.ctx, directory.encode(), self.loop - 1 if loop is None else loop))
 
     def grain_updates(self) -> int:
         v = ctypes.c_int64()

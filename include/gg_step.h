@@ -89,7 +89,8 @@ typedef struct gg_params {
     int32_t grid_coarsement;          /* GridCoarsement (0 supported) */
     int32_t use_stored_elastic_energy;/* UseStoredElasticEnergy (0 supported) */
     int32_t use_magnetic_field;       /* UseMagneticField (0 supported) */
-    int32_t reserved_i[5];
+    int32_t discrete_sampling_rate;   /* DiscreteSamplingRate (bins of the MODF output) */
+    int32_t reserved_i[4];
     double triple_point_drag;         /* TriplePointDrag */
     double constant_sector_radius;    /* ConstantSectorRadius (grid points) */
     double interpolating_sector_radius; /* InterpolatingSectorRadius (grid points) */
@@ -193,6 +194,26 @@ int gg_read_grain_stats(gg_ctx* ctx, gg_grain_stats* out, int32_t capacity);
  */
 int gg_tangent_enable(gg_ctx* ctx, int32_t enable);
 int gg_read_area_tangents(gg_ctx* ctx, double* out, int32_t capacity);
+
+/*
+ * Analysis output of one timestep, the files grainhdl::save_Texture and
+ * grainhdl::save_NrGrainsStats write (src/grainhdl.cpp:871-1023, 1225-1241),
+ * in their formats, into `directory`:
+ *  - Texture_<loop>.ori: per existing grain with regular motion, in ID order:
+ *    ID, direct-neighbour count, boundary flag, area, mean dA / AnalysisTimestep,
+ *    perimeter, energy, stored elastic energy (0), Bunge Euler angles;
+ *  - MODF_<loop>.txt (anisotropic networks): the boundary-length-weighted
+ *    misorientation distribution over DiscreteSamplingRate bins;
+ *  - NrGrains&EnergyStatistics.txt: one line appended (the file is started
+ *    afresh at loop 0): simulated time, grain count at the step's start,
+ *    total boundary energy, grid size.
+ * Call it after the step `loop` has completed (gg_step or gg_redistancing);
+ * the reference calls it when (loop - StartTime) % AnalysisTimestep == 0 and
+ * after the last step.  The simulated time is the sum of the reference's
+ * per-step increments dt PhysicalDomainSize^2 / (TimeSlope HAGB_Energy
+ * HAGB_Mobility) over the steps before `loop`.
+ */
+int gg_write_analysis(gg_ctx* ctx, const char* directory, int32_t loop);
 
 /* Number of grain slots N and the grid size (ngridpoints). */
 int gg_dims(gg_ctx* ctx, int32_t* n_grains, int32_t* ngridpoints, double* h, double* delta, double* dt);

@@ -14,13 +14,16 @@
  *     src/grainhdl.h:53, used by src/grainhdl.cpp:250-274) reads 0 and dt
  *     keeps its documented value;
  *   - runs run_sim's prologue and loop body (src/grainhdl.cpp:1035-1142)
- *     stage by stage, skipping only the analysis file writers
- *     (save_Texture / save_NetworkPlot / save_NrGrainsStats / restart
- *     files), which change no grain state;
+ *     stage by stage, skipping the analysis file writers (save_Texture /
+ *     save_NetworkPlot / save_NrGrainsStats / restart files), which change
+ *     no grain state, unless an analysis directory is given: then
+ *     save_Texture and save_NrGrainsStats run on the reference's schedule
+ *     (src/grainhdl.cpp:1098-1105) with that directory as the working
+ *     directory;
  *   - writes a binary dump of every LSbox after initialisation and after
  *     chosen steps (format below), and the loop's wall time.
  *
- * Usage: gg_ref <parameters.xml> <dump.bin|-> [dump_every] [quiet]
+ * Usage: gg_ref <parameters.xml> <dump.bin|-> [dump_every] [quiet] [analysis_dir]
  *   dump_every = k > 0 dumps after every k-th step (and after init);
  *   0 dumps only the initial and final states.
  *
@@ -178,6 +181,7 @@ int main(int argc, char** argv) {
     const std::string dump_path = argv[2];
     const int dump_every = argc > 3 ? std::atoi(argv[3]) : 0;
     const bool quiet = argc > 4 && std::atoi(argv[4]) != 0;
+    const char* analysis_dir = argc > 5 ? argv[5] : nullptr;
 
     std::streambuf* saved = nullptr;
     std::ofstream devnull;
@@ -209,6 +213,11 @@ int main(int argc, char** argv) {
         w.f64(sim->get_dt());
     }
 
+    if (analysis_dir && chdir(analysis_dir) != 0) {
+        std::fprintf(stderr, "cannot enter %s\n", analysis_dir);
+        return 2;
+    }
+
     // run_sim prologue (src/grainhdl.cpp:1041-1048)
     const double t_init0 = now_s();
     sim->distanceInitialisation();
@@ -218,7 +227,7 @@ int main(int argc, char** argv) {
     const double t_init = now_s() - t_init0;
     if (w.f) dump_state(w, sim, 0);
 
-    // run_sim loop body (src/grainhdl.cpp:1049-1142), analysis output omitted
+    // run_sim loop body (src/grainhdl.cpp:1049-1142)
     double t_loop = 0.0;
     unsigned long grain_updates = 0;
     int steps = 0;
@@ -242,6 +251,11 @@ int main(int argc, char** argv) {
         }
         sim->level_set();
         sim->redistancing();
+        if (analysis_dir && (((sim->loop - Settings::StartTime) % int(Settings::AnalysisTimestep)) == 0 ||
+                             sim->loop == Settings::NumberOfTimesteps)) {
+            sim->save_Texture();
+            sim->save_NrGrainsStats();
+        }
         sim->Realtime += (sim->get_dt() * (Settings::Physical_Domain_Size * Settings::Physical_Domain_Size) /
                           (sim->TimeSlope * Settings::HAGB_Energy * Settings::HAGB_Mobility));
         sim->get_biggestGrainVol();

@@ -35,6 +35,13 @@ CASES = {
     # every step dumped: the per-routine restatement in oracle/gg_oracle.c is
     # checked on each consecutive pair of records
     "seq_v24": ("voronoi", 24, 100, 5, 6, 1, {"IsIsotropicNetwork": 1}),
+    # analysis output (Texture_<loop>.ori, MODF_<loop>.txt,
+    # NrGrains&EnergyStatistics.txt) every 5 steps, written by the reference
+    # into <case>/analysis
+    "ana_iso_v80": ("voronoi", 80, 100, 11, 40, 0, {"IsIsotropicNetwork": 1, "AnalysisTimestep": 5}),
+    "ana_mob_v80": ("voronoi", 80, 100, 12, 40, 0,
+                    {"IsIsotropicNetwork": 0, "UseMobilityModel": 1, "TriplePointDrag": 2.0,
+                     "AnalysisTimestep": 5}),
 }
 
 
@@ -46,8 +53,11 @@ def make_case(name: str, spec) -> dict:
     micro = ms.voronoi(n, nn, seed) if gen == "voronoi" else ms.clustered(n, nn, seed)
     xml = ms.make_case(d, name, micro, NumberOfTimesteps=steps, **over)
     dump = os.path.join(d, "reference.dump")
-    out = subprocess.run([GG_REF, os.path.basename(xml), "reference.dump", str(every), "1"], cwd=d,
-                         check=True, capture_output=True, text=True)
+    cmd = [GG_REF, os.path.basename(xml), "reference.dump", str(every), "1"]
+    if name.startswith("ana_"):
+        os.makedirs(os.path.join(d, "analysis"))
+        cmd.append("analysis")
+    out = subprocess.run(cmd, cwd=d, check=True, capture_output=True, text=True)
     info = json.loads(out.stdout.strip().splitlines()[-1])
     with open(dump, "rb") as f, gzip.open(dump + ".gz", "wb", compresslevel=9) as g:
         shutil.copyfileobj(f, g)

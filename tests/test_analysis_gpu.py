@@ -1,0 +1,116 @@
+"""The analysis writer (gg_write_analysis) against the files GraGLeS2D itself
+wrote in the same run (ana_* fixtures): Texture_<loop>.ori, MODF_<loop>.txt
+and NrGrains&EnergyStatistics.txt on the reference's schedule (every
+AnalysisTimestep steps and after the last).  The plain FP64 form must write
+the same bytes; the batched FP32 form the same grains and counts with areas,
+energies and MODF values within FP32 tolerances.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from gragles2d_b200 import gg
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["ana_iso_v80", "ana_mob_v80"]
+
+
+def _run(golden_dir, name, precision, out, run_sim=False):
+    """Steps the case and writes the analysis files on the reference's
+    schedule, either call by call or through GrainHandler.run_sim."""
+    d = os.path.join(golden_dir, name)
+    with open(os.path.join(d, "case.json")) as f:
+        info = json.load(f)
+    at = info["overrides"]["AnalysisTimestep"]
+    written = [lp for lp in range(info["steps"] + 1) if lp % at == 0 or lp == info["steps"]]
+    h = gg.GrainHandler(gg.Settings(os.path.join(d, name + ".xml"), precision=precision), device=0)
+    try:
+        h.load_voxel_files()
+        if run_sim:
+            h.run_sim(analysis_dir=str(out))
+        else:
+            h.distanceInitialisation()
+            h.find_neighbors()
+            for loop in range(info["steps"] + 1):
+                h.step(1)
+                if loop in written:
+                    h.write_analysis(str(out), loop)
+        assert h.loop == info["steps"] + 1
+        assert h.status() == 0
+    finally:
+        h.close()
+    return d, info, written
+
+
+def _files(loops):
+    names = ["NrGrains&EnergyStatistics.txt"]
+    for lp in loops:
+        names += [f"Texture_{lp}.ori", f"MODF_{lp}.txt"]
+    return names
+
+
+def _text(path):
+    with open(path) as f:
+        return f.read()
+
+
+@pytest.mark.parametrize("name,run_sim", [(CASES[0], False), (CASES[1], False), (CASES[0], True)])
+def test_plain_form_writes_the_reference_files(golden_dir, name, run_sim, tmp_path):
+    d, info, loops = _run(golden_dir, name, gg.PRECISION_PLAIN, tmp_path, run_sim)
+    ref_dir = os.path.join(d, "analysis")
+    assert sorted(os.listdir(ref_dir)) == sorted(_files(loops))
+    for fn in _files(loops):
+        assert _text(tmp_path / fn) == _text(os.path.join(ref_dir, fn)), fn
+
+
+def _table(path):
+    rows = [l.split("\t") for l in _text(path).splitlines()]
+    return np.array([[float(x) for x in r] for r in rows]) if rows else np.zeros((0, 2))
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_batched_form_within_fp32_tolerance(golden_dir, name, tmp_path):
+    d, info, loops = _run(golden_dir, name, gg.PRECISION_BATCHED, tmp_path)
+    ref_dir = os.path.join(d, "analysis")
+    st, rs = _table(tmp_path / "NrGrains&EnergyStatistics.txt"), _table(os.path.join(ref_dir, "NrGrains&EnergyStatistics.txt"))
+    np.testing.assert_array_equal(st[:, [0, 3]], rs[:, [0, 3]])
+    assert np.abs(st[:, 1] - rs[:, 1]).max() <= 1  # a vanishing grain may go one step apart
+    np.testing.assert_allclose(st[:, 2], rs[:, 2], rtol=1e-4)
+    for lp in loops:
+        t, r = _table(tmp_path / f"Texture_{lp}.ori"), _table(os.path.join(ref_dir, f"Texture_{lp}.ori"))
+        common = np.intersect1d(t[:, 0], r[:, 0])
+        assert len(common) >= len(r) - 1
+        t = t[np.isin(t[:, 0], common)]
+        r = r[np.isin(r[:, 0], common)]
+        np.testing.assert_array_equal(t[:, [0, 2, 8, 9, 10]], r[:, [0, 2, 8, 9, 10]])
+        big = r[:, 3] > 25.0 / info["grid"] ** 2
+        np.testing.assert_allclose(t[big, 3], r[big, 3], rtol=1e-3)   # area
+        # perimeter and energy: within a tenth of a grid spacing (a contour
+        # point beside a saddle may take the other edge in FP32)
+        np.testing.assert_allclose(t[big, 5], r[big, 5], rtol=0, atol=0.1 / info["grid"])
+        np.testing.assert_allclose(t[big, 6], r[big, 6], rtol=0, atol=0.1 / info["grid"])
+        m, mr = _table(tmp_path / f"MODF_{lp}.txt"), _table(os.path.join(ref_dir, f"MODF_{lp}.txt"))
+        assert m.shape == mr.shape
+        if m.size:
+            np.testing.assert_array_equal(m[:, 0], mr[:, 0])
+            np.testing.assert_allclose(m[:, 1], mr[:, 1], atol=2e-3)
+
+
+def test_rejects_a_loop_that_is_not_the_last_step(golden_dir, tmp_path):
+    d = os.path.join(golden_dir, "ana_iso_v80")
+    h = gg.GrainHandler(gg.Settings(os.path.join(d, "ana_iso_v80.xml")), device=0)
+    try:
+        h.load_voxel_files()
+        h.distanceInitialisation()
+        h.find_neighbors()
+        h.step(3)
+        with pytest.raises(gg.GGError) as e:
+            h.write_analysis(str(tmp_path), 0)
+        assert e.value.code == 4
+        h.write_analysis(str(tmp_path), 2)
+        assert (tmp_path / "Texture_2.ori").exists()
+    finally:
+        h.close()
