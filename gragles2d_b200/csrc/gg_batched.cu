@@ -219,11 +219,19 @@ __device__ __forceinline__ unsigned long long f2_fma(unsigned long long a, unsig
 // projectToGrainBondary (src/grainBoundary.cpp:365-447) in FP32 for the
 // pixels (px, py) of the 32 lanes of a warp (all lanes call it; `valid` lanes
 // are the warp's real pixels, the others only follow along).  The nearest
-// vertex of each lane is the first one at the smallest distance: chunks are
-// visited out of index order (first the chunk `*wseed` that held the nearest
-// vertex of the warp's previous tile, then the others that the bound does
-// not rule out), comparing (distance, index) pairs.  P holds the contour with
-// a 16-byte aligned start, two points per float4.
+// vertex of each lane is the first one at the smallest distance, with
+// distances compared to 14 mantissa bits: each candidate is one 32-bit key,
+// the squared distance's bits with the low 9 replaced by the vertex index
+// (contours of up to 512 points), so one unsigned minimum keeps the smallest
+// distance and, among equal keys, the lowest index.  Chunks are visited out
+// of index order (first the chunk `*wseed` that held the nearest vertex of
+// the warp's previous tile, then the others that the bound does not rule
+// out).  P holds the contour with a 16-byte aligned start, two points per
+// float4.
+constexpr unsigned kKeyIndexBits = 9;
+constexpr unsigned kKeyIndexMask = (1u << kKeyIndexBits) - 1u;
+static_assert(kCorrMaxPts <= (1 << kKeyIndexBits), "vertex index must fit the key");
+
 __device__ __forceinline__ int project_warp(const float2* P, const float4* cbb, int asize, int px, int py,
                                             bool valid, float* out_lambda, int* wseed) {
     const unsigned FULL = 0xffffffffu;
@@ -233,14 +241,7 @@ __device__ __forceinline__ int project_warp(const float2* P, const float4* cbb, 
     const int npts = asize - 1;
     const int nch = (npts + kChunk - 1) / kChunk;
     const float4* P2 = reinterpret_cast<const float4*>(P);
-    float best = 3.0e38f;
-    int nearest = -1;
-    auto take = [&](float d, int k) {
-        if (d < best || (d == best && k < nearest)) {
-            nearest = k;
-            best = d;
-        }
-    };
+    unsigned key = 0xffffffffu;
     auto scan = [&](int ch) {
         const int k0 = ch * kChunk, k1 = min(k0 + kChunk, npts);
         for (int k = k0; k < k1; k += 2) {
@@ -248,15 +249,20 @@ __device__ __forceinline__ int project_warp(const float2* P, const float4* cbb, 
             const unsigned long long DX = f2_sub(FX, f2_pack(v.x, v.z)), DY = f2_sub(FY, f2_pack(v.y, v.w));
             float d0, d1;
             f2_unpack(f2_fma(DY, DY, f2_mul(DX, DX)), d0, d1);
-            take(d0, k);
-            if (k + 1 < k1) take(d1, k + 1);
+            key = min(key, (__float_as_uint(d0) & ~kKeyIndexMask) | (unsigned)k);
+            if (k + 1 < k1) key = min(key, (__float_as_uint(d1) & ~kKeyIndexMask) | (unsigned)(k + 1));
         }
+    };
+    // an upper bound of the lanes' best squared distances (keys rounded up)
+    auto bound = [&]() {
+        const unsigned up = min(key | kKeyIndexMask, 0x7f7fffffu);
+        return __uint_as_float(__reduce_max_sync(FULL, valid ? up : 0u));
     };
     const int sc = *wseed < nch ? *wseed : 0;
     scan(sc);
     const int bx0 = __reduce_min_sync(FULL, valid ? px : INT_MAX), bx1 = __reduce_max_sync(FULL, valid ? px : INT_MIN);
     const int by0 = __reduce_min_sync(FULL, valid ? py : INT_MAX), by1 = __reduce_max_sync(FULL, valid ? py : INT_MIN);
-    float U = __uint_as_float(__reduce_max_sync(FULL, valid ? __float_as_uint(best) : 0u));
+    float U = bound();
     for (int c0 = 0; c0 < nch; c0 += 32) {
         const int ch = c0 + lane;
         float lb = 3.0e38f;
@@ -273,9 +279,10 @@ __device__ __forceinline__ int project_warp(const float2* P, const float4* cbb, 
             const float lbc = __shfl_sync(FULL, lb, bit);
             if (lbc > U * kBoundSlack) continue;
             scan(c0 + bit);
-            U = __uint_as_float(__reduce_max_sync(FULL, valid ? __float_as_uint(best) : 0u));
+            U = bound();
         }
     }
+    const int nearest = key == 0xffffffffu ? -1 : (int)(key & kKeyIndexMask);
     {
         const int src = __ffs(__ballot_sync(FULL, valid)) - 1;
         const int sn = __shfl_sync(FULL, nearest, src < 0 ? 0 : src);

@@ -5,6 +5,7 @@
 // blends its convolved value with the sector / junction / boundary weight.
 #pragma once
 
+#include <cfloat>
 #include "gg_grain.cuh"
 #include "gg_kernels.cuh"
 
@@ -208,6 +209,45 @@ __device__ __forceinline__ long lap_guard(double perimeter, int size, double rad
     return (long)(laps * (size + 1)) + 8;
 }
 
+// Whole laps of a contour walk at once, with the step-by-step result.  A walk
+// adds seg[p], seg[p + dir], ... (indices mod n) to dist while dist stays
+// below a limit; on a nearly vanished grain (perimeter far below the sector
+// radius) that takes millions of steps.  Inside one binade [2^(e-1), 2^e)
+// every double is a multiple of u = 2^(e-53), so each rounded addition
+// dist + s adds exactly u * rint(s / u), unless s / u ends in exactly one
+// half (the rounding would then depend on dist's last bit): a lap adds the
+// exact quantum Q, and m laps that stay below the binade's top and the limit
+// add m Q with no rounding at all.  Returns the laps taken (0 when the skip
+// does not apply); it leaves at least two laps before the limit, so the
+// caller's next step still runs, and takes at most `max_laps`.
+constexpr long kSkipAfter = 64;  // steps before a walk tries to skip laps
+
+__device__ long skip_laps(double* dist, double limit, const double* seg, int p, int dir, int n, long max_laps) {
+    const double d = *dist;
+    if (!(d >= DBL_MIN) || !(d < limit) || n <= 0 || max_laps < 1) return 0;
+    int e;
+    frexp(d, &e);
+    const double u = ldexp(1.0, e - 53);
+    const double top = ldexp(1.0, e);
+    double Q = 0;
+    int k = p;
+    for (int i = 0; i < n; ++i) {
+        const double r = seg[k] / u;  // exact: u is a power of two
+        if (r - floor(r) == 0.5) return 0;
+        Q += rint(r) * u;
+        k += dir;
+        if (k >= n) k -= n;
+        if (k < 0) k += n;
+    }
+    if (!(Q > 0)) return 0;
+    double mm = floor((fmin(limit, top) - d) / Q) - 2;
+    if (mm > (double)max_laps) mm = (double)max_laps;
+    if (!(mm >= 1)) return 0;
+    const long m = (long)mm;
+    *dist = d + (double)m * Q;  // m Q < top - d: a multiple of u, exact
+    return m;
+}
+
 // ExplicitGrainBoundary::setPointsOnBoundary (src/grainBoundary.cpp:524-559).
 // seg[k] = |P[k+1] - P[k]| h, the term the reference recomputes at every step
 // of its walks (same expression, so the sums are bit-identical).
@@ -222,7 +262,10 @@ __device__ void set_points_on_boundary(const CPoint* P, const double* seg, int s
     }
     l = periodic(l + 1, size);
     long it = 0;
+    const int n = size - 1;
     while (dist < csr) {
+        if (it >= kSkipAfter && (it & (kSkipAfter - 1)) == 0)
+            it += n * skip_laps(&dist, csr, seg, l, 1, n, (guard - it) / n - 2);
         dist += seg[l];
         l = periodic(l + 1, size);
         if (++it > guard) {
@@ -240,6 +283,8 @@ __device__ void set_points_on_boundary(const CPoint* P, const double* seg, int s
     r = periodic(r, size);
     it = 0;
     while (dist < csr) {
+        if (it >= kSkipAfter && (it & (kSkipAfter - 1)) == 0)
+            it += n * skip_laps(&dist, csr, seg, periodic(r - 1, size), -1, n, (guard - it) / n - 2);
         dist += seg[periodic(r - 1, size)];
         r = periodic(r - 1, size);
         if (++it > guard) {
@@ -352,6 +397,8 @@ __device__ void build_sectors_warp(const NetConst& C, const NbTable& T, const CP
                 int j = secR.left, last = -1;
                 long it = 0;
                 for (; dist <= C.isr; j = wrap_next(j, real)) {
+                    if (it >= kSkipAfter && (it & (kSkipAfter - 1)) == 0)
+                        it += real * skip_laps(&dist, C.isr, seg, j, 1, real, (guard - it) / real - 2);
                     dist += seg[j];
                     last = j;
                     if (++it > guard) {
@@ -374,6 +421,8 @@ __device__ void build_sectors_warp(const NetConst& C, const NbTable& T, const CP
                 int j = secL.right, last = -1;
                 long it = 0;
                 for (; dist <= C.isr; j = wrap_prev(j, real)) {
+                    if (it >= kSkipAfter && (it & (kSkipAfter - 1)) == 0)
+                        it += real * skip_laps(&dist, C.isr, seg, wrap_prev(j, real), -1, real, (guard - it) / real - 2);
                     dist += seg[wrap_prev(j, real)];
                     last = wrap_prev(j, real);
                     if (++it > guard) {
