@@ -8,7 +8,7 @@
 
 namespace gg {
 
-constexpr int kSepSmemMaxN = 64;  // box + intermediate in shared memory up to this edge
+constexpr int kSepSmemMaxN = 64;  // intermediate in shared memory up to this edge
 constexpr int kSepStrip = 4;       // outputs per thread along the convolution axis
 
 // Gaussian convolution as a separable circular convolution in real space:
@@ -147,12 +147,10 @@ __global__ void __launch_bounds__(128) k_conv_sep(NetConst C, NetState* S) {
     const float* in = reinterpret_cast<const float*>(S->phiA) + S->off_cur[g];
     float* out = reinterpret_cast<float*>(S->phiB) + S->off_cur[g];
     const float* kg = C.ck + C.ck_off[n];
-    const int nn2 = n * n;
     const bool fits = n <= kSepSmemMaxN;
     float* kx = sm + 1;  // sm[0] is the guard entry kx[-1]
     const int kl = kx_len(n);
-    float* X = sm + 1 + kl;
-    float* T = fits ? X + nn2 : reinterpret_cast<float*>(S->spec) + S->soff_cur[g];
+    float* T = fits ? sm + 1 + kl : reinterpret_cast<float*>(S->spec) + S->soff_cur[g];
     for (int j = threadIdx.x; j < kl; j += blockDim.x) {
         int m = j - (n - 1);
         m %= n;
@@ -160,18 +158,21 @@ __global__ void __launch_bounds__(128) k_conv_sep(NetConst C, NetState* S) {
         kx[j] = j < 2 * n - 1 ? kg[m] : 0.f;
     }
     if (threadIdx.x == 0) sm[0] = 0.f;
-    if (fits)
-        for (int i = threadIdx.x; i < nn2; i += blockDim.x) X[i] = in[i];
     __syncthreads();
     const int R = (int)kg[n];  // band radius stored after the n kernel entries
-    sep_pass_rows(fits ? X : in, T, kx, n, R);
+    sep_pass_rows(in, T, kx, n, R);
     __syncthreads();
     sep_pass_cols(T, out, kx, n, R);
 }
 
 size_t conv_sep_smem(int tmax) {
+    // the row-pass intermediate of a box (edge up to kSepSmemMaxN) with its
+    // extended kernel, or the extended kernel alone of the largest box (whose
+    // intermediate goes to the grain's scratch in device memory)
     const int n = tmax < kSepSmemMaxN ? tmax : kSepSmemMaxN;
-    return sizeof(float) * (size_t)(2 * n * n + 2 * kSepSmemMaxN + kSepStrip + 2);
+    const size_t staged = (size_t)n * n + 2 * (size_t)n + kSepStrip + 2;
+    const size_t kernel_only = 2 * (size_t)tmax + kSepStrip + 2;
+    return sizeof(float) * (staged > kernel_only ? staged : kernel_only);
 }
 
 // Batched-form corrector: same sectors as k_corrector (built by one warp),
