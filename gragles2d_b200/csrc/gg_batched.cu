@@ -339,6 +339,8 @@ __device__ __forceinline__ int project_warp(const float2* P, const float4* cbb, 
     return seg;
 }
 
+// kStored: with the stored-energy term (UseStoredElasticEnergy).
+template <bool kStored>
 __global__ void __launch_bounds__(128, 8) k_corrector_f(NetConst C, NetState* S) {
     const int g = blockIdx.x + 1;
     if (g > C.N || C.state[g] != G_EXISTS || C.regular[g] == 0 || S->loop == 0 || halted(S)) return;
@@ -409,7 +411,9 @@ __global__ void __launch_bounds__(128, 8) k_corrector_f(NetConst C, NetState* S)
             id = idl[(i - ib.y0) * wi + (j - ib.x0)];
         }
         const bool valid = inside && val > -delta;
-        if (inside && !valid) out[k] = -delta;
+        // stored-energy term (src/box.cpp:511-517) of inside pixels
+        const float se = (kStored && inside) ? (float)(nb_stored_force(nbt, (int)id) * C.dt / C.time_slope) : 0.f;
+        if (inside && !valid) out[k] = -delta - se;
         if (__ballot_sync(0xffffffffu, valid) == 0u) continue;
         float lambda = 0.f;
         int segment;
@@ -476,11 +480,18 @@ __global__ void __launch_bounds__(128, 8) k_corrector_f(NetConst C, NetState* S)
                 weight = interpolator * lw + (1 - interpolator) * rw;
             }
         }
-        out[k] = val + (conv - val) * weight;
+        out[k] = val + (conv - val) * weight - se;
     }
     if (st) set_status(S, st);
 }
 
+
+void launch_corrector_f(const NetConst& C, NetState* dS, cudaStream_t s) {
+    if (C.stored)
+        k_corrector_f<true><<<C.N, 128, 0, s>>>(C, dS);
+    else
+        k_corrector_f<false><<<C.N, 128, 0, s>>>(C, dS);
+}
 
 cudaError_t batched_prepare(int tmax) {
     return cudaFuncSetAttribute(k_conv_sep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conv_sep_smem(tmax));
@@ -504,7 +515,7 @@ cudaError_t batched_stage_kernel(const NetConst& C, NetState* dS, int which, cud
     (void)gblocks;
     switch (which) {
         case 0: k_conv_sep<<<C.N, 128, conv_sep_smem(C.tmax), s>>>(C, dS); break;
-        case 1: if (!C.isotropic) k_corrector_f<<<C.N, 128, 0, s>>>(C, dS); break;
+        case 1: if (!C.isotropic) launch_corrector_f(C, dS, s); break;
         case 2: k_second_order_w<<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS); break;
         case 3: k_compare<float><<<C.N, cfg.compare_threads, 0, s>>>(C, dS); break;
         case 4: k_levelset_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS); break;
@@ -524,7 +535,7 @@ cudaError_t batched_stages(const NetConst& C, NetState* dS, int stages, cudaStre
     (void)gblocks;
     if (stages & ST_CONV) {
         k_conv_sep<<<C.N, 128, conv_sep_smem(C.tmax), s>>>(C, dS);
-        if (!C.isotropic) k_corrector_f<<<C.N, 128, 0, s>>>(C, dS);
+        if (!C.isotropic) launch_corrector_f(C, dS, s);
     }
     if (stages & ST_SECOND) k_second_order_w<<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS);
     if (stages & ST_COMPARE) k_compare<float><<<C.N, cfg.compare_threads, 0, s>>>(C, dS);
@@ -549,7 +560,7 @@ cudaError_t batched_step_graph(const NetConst& C, NetState* dS, cudaStream_t s, 
     k_second_order_w<<<wblocks, 32 * kGrainsPerBlock, 0, s2>>>(C, dS);
     if ((e = cudaEventRecord(ev[1], s2)) != cudaSuccess) return e;
     k_conv_sep<<<C.N, 128, conv_sep_smem(C.tmax), s>>>(C, dS);
-    if (!C.isotropic) k_corrector_f<<<C.N, 128, 0, s>>>(C, dS);
+    if (!C.isotropic) launch_corrector_f(C, dS, s);
     if ((e = cudaStreamWaitEvent(s, ev[1], 0)) != cudaSuccess) return e;
     k_compare<float><<<C.N, cfg.compare_threads, 0, s>>>(C, dS);
     k_levelset_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS);

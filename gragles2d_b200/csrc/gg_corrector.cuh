@@ -79,6 +79,7 @@ struct NbTable {
     int n;
     int id[48];
     double w[48];
+    double f[48];  // stored-energy driving force (own - neighbour energy) x mobility, when stored energies are on
 };
 
 __device__ void build_nb_table(const NetConst& C, int owner, NbTable& T) {
@@ -91,7 +92,28 @@ __device__ void build_nb_table(const NetConst& C, int owner, NbTable& T) {
         T.id[e] = gone ? -2 : id;
         const double v = nb[e].energy * nb[e].mobility;
         T.w[e] = v > 0.01 ? v : 0.01;
+        T.f[e] = (C.stored && !gone) ? (C.stored[owner] - C.stored[id]) * nb[e].mobility : 0.0;
     }
+}
+
+// ExplicitGrainBoundary::get_f_StoredElasticEnergy (src/grainBoundary.cpp:
+// 607-615) for the grain `id`: the first characteristic with that ID, else -1.
+__device__ __forceinline__ double nb_stored_force(const NbTable& T, int id) {
+    for (int e = 0; e < T.n; ++e)
+        if (T.id[e] == id) return T.f[e];
+    return -1.0;
+}
+
+// The stored-energy term the corrector subtracts at (row, col)
+// (src/box.cpp:511-517): f(IDLocal) dt / TimeSlope.
+__device__ __forceinline__ double stored_energy_term(const NetConst& C, const NbTable& T, const uint32_t* idl,
+                                                     const Box& ib, int row, int col, uint32_t* status) {
+    uint32_t k;
+    if (!buf_index(ib, row, col, &k)) {
+        *status |= S_INDEX;
+        return 0.0;
+    }
+    return nb_stored_force(T, (int)idl[k]) * C.dt / C.time_slope;
 }
 
 // getGBEnergyTimesGBMobility(i, j) through the table (first match, as the
@@ -674,6 +696,7 @@ __global__ void __launch_bounds__(128) k_corrector(NetConst C, NetState* S) {
         } else {
             out[k] = -delta;
         }
+        if (C.stored) out[k] = (R)((double)out[k] - stored_energy_term(C, nbt, idl, ib, i, j, &st));
     }
     if (st) set_status(S, st);
 }

@@ -127,6 +127,8 @@ struct NetConst {
     int32_t* nb_n;
     Neighbour* nb;     // nbmax per grain
     int32_t* gone_loop;  // loop of the step whose level set deleted the grain, else -1
+    double* stored;      // UseStoredElasticEnergy: scaled stored energy per grain, slot 0 = boundary (else null)
+    double time_slope;   // GaussianKernelUserDefTimeSlope
 
     // tables (host-computed, libm on the host)
     const double* tw;        // twiddles exp(-2 pi i k / n), interleaved, at tw_off[n]

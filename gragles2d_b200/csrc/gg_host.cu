@@ -47,6 +47,8 @@ struct gg_ctx {
     std::vector<int32_t> ids;     // nn*nn
     std::vector<double> euler;    // 3 per grain
     std::vector<int32_t> bbox;    // 5 per grain
+    std::vector<double> stored;   // .uds stored energy per grain (empty: none given)
+    std::vector<double> stored_scaled;  // UseStoredElasticEnergy: scaled values, slot 0 = boundary
 
     NetConst C{};
     NetState hS{};               // host copy of the device NetState (pointers)
@@ -325,6 +327,8 @@ int gg_params_from_xml(const char* path, gg_params* p) {
         getd("ThetaRefDegrees", &p->theta_ref_deg);
         getd("HAGB_RelativeEnergy", &p->gamma_hagb);
         getd("HAGB_RelativeMobility", &p->m_hagb);
+        getd("DislocEnPerM", &p->dislocation_energy_per_m);
+        getd("BoxDefaultStoredElasticEnergy", &p->box_default_stored_elastic_energy);
         geti("Precision", &p->precision);
     } catch (...) {
         return GG_E_IO;
@@ -348,8 +352,9 @@ int gg_create(const gg_params* p, int device, gg_ctx** out) {
     if (p->lattice_type != 0) return bad("only LatticeType 0 (cubic) is supported");
     if (p->research_mode != 0) return bad("only ResearchMode 0 is supported");
     if (p->grid_coarsement != 0) return bad("GridCoarsement must be 0");
-    if (p->use_stored_elastic_energy != 0 || p->use_magnetic_field != 0)
-        return bad("stored-energy and magnetic driving forces are not supported");
+    if (p->use_magnetic_field != 0) return bad("the magnetic driving force is not supported");
+    if (p->use_stored_elastic_energy < 0 || p->use_stored_elastic_energy > 1)
+        return bad("UseStoredElasticEnergy must be 0 or 1");
     if (p->identify_twins != 0) return bad("IdentifyTwins is not supported");
     if (p->use_mobility_model < 0 || p->use_mobility_model > 1) return bad("UseMobilityModel must be 0 or 1");
     if (p->precision != GG_PRECISION_PLAIN && p->precision != GG_PRECISION_BATCHED) return bad("bad precision");
@@ -394,7 +399,17 @@ int gg_load_voxels(gg_ctx* c, int32_t nn, const int32_t* ids, int32_t n_grains, 
     c->ids.assign(ids, ids + (size_t)nn * nn);
     c->euler.assign(euler, euler + 3 * (size_t)n_grains);
     c->bbox.assign(bbox, bbox + 5 * (size_t)n_grains);
+    c->stored.clear();
     c->loaded = true;
+    return GG_OK;
+}
+
+int gg_load_stored_energy(gg_ctx* c, const double* stored, int32_t n_grains) {
+    if (!c || !stored) return GG_E_INVALID;
+    if (!c->loaded) return fail(c, GG_E_STATE, "no microstructure loaded");
+    if (c->initialised) return fail(c, GG_E_STATE, "network already initialised");
+    if (n_grains != c->N) return fail(c, GG_E_INVALID, "one stored energy per grain");
+    c->stored.assign(stored, stored + n_grains);
     return GG_OK;
 }
 
@@ -428,7 +443,7 @@ int gg_load_voxel_files(gg_ctx* c, const char* base_dir) {
         std::fclose(f);
         return fail(c, GG_E_IO, "bad .uds header (need NX == NY > 0 and a grain count)");
     }
-    std::vector<double> eul(3 * (size_t)grains);
+    std::vector<double> eul(3 * (size_t)grains), stored(grains);
     std::vector<int32_t> bb(5 * (size_t)grains);
     for (int k = 0; k < grains; ++k) {
         int id, xmin, xmax, ymin, ymax, cnt;
@@ -450,6 +465,7 @@ int gg_load_voxel_files(gg_ctx* c, const char* base_dir) {
         bb[5 * k + 2] = ymin;
         bb[5 * k + 3] = ymax;
         bb[5 * k + 4] = cnt;
+        stored[k] = se;
     }
     std::fclose(f);
     FILE* fb = std::fopen(join(c->P.read_from_filename).c_str(), "rb");
@@ -462,7 +478,9 @@ int gg_load_voxel_files(gg_ctx* c, const char* base_dir) {
         v = v - (id_offset - 1);
         if (v < 0) v = 0;
     }
-    return gg_load_voxels(c, NX, ids.data(), grains, eul.data(), bb.data());
+    int rc = gg_load_voxels(c, NX, ids.data(), grains, eul.data(), bb.data());
+    if (rc == GG_OK && c->P.use_stored_elastic_energy) rc = gg_load_stored_energy(c, stored.data(), grains);
+    return rc;
 }
 
 int gg_distance_initialisation(gg_ctx* c) {
@@ -480,6 +498,37 @@ int gg_distance_initialisation(gg_ctx* c) {
         P.decouple_grains == 1 ? (unsigned long)P.number_of_points_per_grain : (unsigned long)c->ppg;
     c->dt = 0.8 / double(realDomainSize * realDomainSize) * ppg_used / 2 / 5.0;
     c->h = 1.0 / double(realDomainSize);
+    // Stored elastic energies: each grain's value scaled as LSbox's voxel
+    // constructor scales it (src/box.cpp:163-175), the domain boundary's
+    // default value (src/box.cpp:35-43), and the time step shortened so that
+    // the largest stored-energy difference moves a boundary by at most half a
+    // grid spacing per step (grainhdl::read_HeaderCPG, src/grainhdl.cpp:404-460;
+    // grainhdl::find_correctTimestepSize, 250-274).  Slot 0 is the boundary.
+    std::vector<double>& stored_scaled = c->stored_scaled;
+    stored_scaled.clear();
+    if (P.use_stored_elastic_energy) {
+        if (c->stored.size() != (size_t)c->N) return fail(c, GG_E_STATE, "no stored energies loaded");
+        const double D = P.dislocation_energy_per_m, H = P.hagb_energy, L = P.physical_domain_size;
+        stored_scaled.assign((size_t)c->N + 1, 0.0);
+        stored_scaled[0] = P.box_default_stored_elastic_energy;
+        stored_scaled[0] *= D / H * L;
+        double lo = 1e20, hi = 0;
+        for (int g = 1; g <= c->N; ++g) {
+            const double v = c->stored[g - 1];
+            if (std::fabs(v) < lo) lo = std::fabs(v);
+            if (std::fabs(v) > hi) hi = std::fabs(v);
+            stored_scaled[g] = v;
+            stored_scaled[g] *= D / H * L;
+        }
+        if (std::fabs(stored_scaled[0]) / D * H / L < lo) lo = std::fabs(stored_scaled[0]) / D * H / L;
+        if (std::fabs(stored_scaled[0]) / D * H / L > hi) hi = std::fabs(stored_scaled[0]) / D * H / L;
+        if (c->N == 1) lo = 0.0;
+        const double energy_delta_max = D * (hi - lo) / H * L;
+        const double vmax = energy_delta_max * c->dt;
+        double correction = 0.5 / (vmax / c->h);
+        if (correction > 1.0) correction = 1.0;
+        c->dt *= correction;
+    }
     c->delta = (unsigned long)P.domain_border_size * 1 / double(realDomainSize);
     c->b = P.domain_border_size;
     c->m = realDomainSize + 2 * c->b;
@@ -578,6 +627,8 @@ int gg_distance_initialisation(gg_ctx* c) {
     ALLOC(C.nb_n, N + 1);
     ALLOC(C.nb, (size_t)C.nbmax * (N + 1));
     ALLOC(C.gone_loop, N + 1);
+    C.time_slope = P.time_slope;
+    if (P.use_stored_elastic_energy) ALLOC(C.stored, N + 1);
     GG_CUDA(c, cudaMemsetAsync(C.gone_loop, 0xff, sizeof(int32_t) * (N + 1), c->stream));
 
     // tables: twiddles and Gaussian multipliers (plain), separable kernels (batched)
@@ -755,6 +806,7 @@ int gg_distance_initialisation(gg_ctx* c) {
     GG_CUDA(c, h2d(C.state, state.data(), sizeof(int32_t) * (N + 1)));
     GG_CUDA(c, h2d(C.regular, ones.data(), sizeof(int32_t) * (N + 1)));
     GG_CUDA(c, h2d(C.quat, quat.data(), sizeof(double) * quat.size()));
+    if (C.stored) GG_CUDA(c, h2d(C.stored, stored_scaled.data(), sizeof(double) * stored_scaled.size()));
     GG_CUDA(c, h2d(c->d_ids, c->ids.data(), sizeof(int32_t) * c->ids.size()));
     S.phi_used = a;
     S.spec_used = sp;
@@ -958,6 +1010,8 @@ int gg_tangent_enable(gg_ctx* c, int32_t enable) {
     if (c->initialised) return fail(c, GG_E_STATE, "tangents must be enabled before gg_distance_initialisation");
     if (enable && c->P.precision != GG_PRECISION_PLAIN)
         return fail(c, GG_E_INVALID, "tangents need the plain (FP64) form");
+    if (enable && c->P.use_stored_elastic_energy)
+        return fail(c, GG_E_INVALID, "tangents do not cover the stored-energy driving force");
     c->tangents = enable != 0;
     return GG_OK;
 }
@@ -1047,8 +1101,8 @@ int gg_write_analysis(gg_ctx* c, const char* directory, int32_t loop) {
                 if (kv.first >= 0 && kv.first < nbins) modf[kv.first] += kv.second / 2;
         }
         tex << g << '\t' << nbn[g] << '\t' << (bnd[g] != 0) << '\t' << vol[g] << '\t'
-            << mda[g] / (double)c->P.analysis_timestep << '\t' << per[g] << '\t' << en[g] << '\t' << 0.0
-            << '\t' << eul[0] << '\t' << eul[1] << '\t' << eul[2] << std::endl;
+            << mda[g] / (double)c->P.analysis_timestep << '\t' << per[g] << '\t' << en[g] << '\t'
+            << (c->stored_scaled.empty() ? 0.0 : c->stored_scaled[g]) << '\t' << eul[0] << '\t' << eul[1] << '\t' << eul[2] << std::endl;
         double sum = 0.0;
         for (int i = 0; i < nbins; ++i) sum += modf[i];
         for (int i = 0; i < nbins; ++i)

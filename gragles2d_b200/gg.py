@@ -25,7 +25,7 @@ ERRORS = {1: "invalid", 2: "cuda", 3: "io", 4: "state", 5: "capacity", 6: "numer
 # Entry points declared in include/gg_step.h, in declaration order.
 EXPORTS = (
     "gg_params_default", "gg_params_from_xml", "gg_create", "gg_destroy", "gg_last_error", "gg_load_voxels",
-    "gg_load_voxel_files", "gg_distance_initialisation", "gg_find_neighbors", "gg_set_neighbours",
+    "gg_load_voxel_files", "gg_load_stored_energy", "gg_distance_initialisation", "gg_find_neighbors", "gg_set_neighbours",
     "gg_convolution", "gg_update_second_order_neighbors", "gg_comparison", "gg_level_set", "gg_redistancing",
     "gg_grain_count", "gg_step", "gg_status", "gg_read_grain_stats", "gg_tangent_enable", "gg_read_area_tangents",
     "gg_write_analysis", "gg_dims", "gg_dump", "gg_last_step_ms",
@@ -60,7 +60,8 @@ class Params(ctypes.Structure):
         ("interpolating_sector_radius", ctypes.c_double), ("hagb_energy", ctypes.c_double),
         ("hagb_mobility", ctypes.c_double), ("physical_domain_size", ctypes.c_double),
         ("time_slope", ctypes.c_double), ("theta_ref_deg", ctypes.c_double), ("gamma_hagb", ctypes.c_double),
-        ("m_hagb", ctypes.c_double), ("reserved_d", ctypes.c_double * 6),
+        ("m_hagb", ctypes.c_double), ("dislocation_energy_per_m", ctypes.c_double),
+        ("box_default_stored_elastic_energy", ctypes.c_double), ("reserved_d", ctypes.c_double * 4),
         ("read_from_filename", ctypes.c_char * 512), ("additional_filename", ctypes.c_char * 512),
     ]
 
@@ -94,6 +95,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "gg_last_error": (ctypes.c_char_p, [V]),
         "gg_load_voxels": (I, [V, I, P(I), I, P(D), P(I)]),
         "gg_load_voxel_files": (I, [V, ctypes.c_char_p]),
+        "gg_load_stored_energy": (I, [V, P(D), I]),
         "gg_distance_initialisation": (I, [V]),
         "gg_find_neighbors": (I, [V]),
         "gg_set_neighbours": (I, [V, P(I), P(I)]),
@@ -200,7 +202,9 @@ class GrainHandler:
     def load_voxel_files(self):
         self._check(self.lib.gg_load_voxel_files(self.ctx, self.settings.base_dir.encode()))
 
-    def load_voxels(self, ids: np.ndarray, euler: np.ndarray, bbox: np.ndarray):
+    def load_voxels(self, ids: np.ndarray, euler: np.ndarray, bbox: np.ndarray, stored: np.ndarray | None = None):
+        """Voxelized input from host arrays; `stored` holds the .uds stored
+        energies (one per grain), used when UseStoredElasticEnergy is set."""
         ids = np.ascontiguousarray(ids, dtype=np.int32)
         euler = np.ascontiguousarray(euler, dtype=np.float64)
         bbox = np.ascontiguousarray(bbox, dtype=np.int32)
@@ -208,6 +212,10 @@ class GrainHandler:
         self._check(self.lib.gg_load_voxels(
             self.ctx, ids.shape[0], ids.ctypes.data_as(P(ctypes.c_int32)), euler.shape[0],
             euler.ctypes.data_as(P(ctypes.c_double)), bbox.ctypes.data_as(P(ctypes.c_int32))))
+        if stored is not None:
+            stored = np.ascontiguousarray(stored, dtype=np.float64)
+            self._check(self.lib.gg_load_stored_energy(self.ctx, stored.ctypes.data_as(P(ctypes.c_double)),
+                                                       stored.shape[0]))
 
     def setSimulationParameter(self):
         self.load_voxel_files()

@@ -36,6 +36,7 @@ class Microstructure:
     labels: np.ndarray  # (nn, nn) int32, 1-based grain IDs
     seeds: np.ndarray  # (n_grains, 2) float64 in [0,1)^2 (x, y)
     euler: np.ndarray  # (n_grains, 3) float64 Bunge phi1, PHI, phi2
+    stored: np.ndarray | None = None  # (n_grains,) float64 stored elastic energies (.uds column 12), else 0
 
     @property
     def nn(self) -> int:
@@ -161,9 +162,10 @@ def write_mode4(prefix: str, ms: Microstructure) -> tuple[str, str]:
         for g in range(ms.n_grains):
             xmin, xmax, ymin, ymax, cnt = (int(v) for v in tab[g])
             e = ms.euler[g]
+            se = f"{ms.stored[g]:.17g}" if ms.stored is not None else "0.0"
             f.write(
                 f"{g + 1}\t {ms.seeds[g, 0]:.10f}\t {ms.seeds[g, 1]:.10f}\t {e[0]:.17g}\t {e[1]:.17g}\t {e[2]:.17g}\t "
-                f"{xmin}\t {xmax}\t {ymin}\t {ymax}\t {cnt}\t 0.0 \n"
+                f"{xmin}\t {xmax}\t {ymin}\t {ymax}\t {cnt}\t {se} \n"
             )
     ms.labels.astype("<i4").tofile(binp)
     return uds, binp

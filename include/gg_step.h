@@ -87,7 +87,7 @@ typedef struct gg_params {
     int32_t research_project;         /* ResearchProject */
     int32_t decouple_grains;          /* DecoupleGrains */
     int32_t grid_coarsement;          /* GridCoarsement (0 supported) */
-    int32_t use_stored_elastic_energy;/* UseStoredElasticEnergy (0 supported) */
+    int32_t use_stored_elastic_energy;/* UseStoredElasticEnergy (0, 1) */
     int32_t use_magnetic_field;       /* UseMagneticField (0 supported) */
     int32_t discrete_sampling_rate;   /* DiscreteSamplingRate (bins of the MODF output) */
     int32_t reserved_i[4];
@@ -101,7 +101,9 @@ typedef struct gg_params {
     double theta_ref_deg;             /* Read-Shockley cut-off angle */
     double gamma_hagb;                /* relative high-angle boundary energy */
     double m_hagb;                    /* relative high-angle boundary mobility */
-    double reserved_d[6];
+    double dislocation_energy_per_m;  /* DislocEnPerM (scales the stored energies) */
+    double box_default_stored_elastic_energy; /* BoxDefaultStoredElasticEnergy (domain boundary) */
+    double reserved_d[4];
     char read_from_filename[512];     /* ReadFromFilename (.bin ID field) */
     char additional_filename[512];    /* AdditionalFilename (.uds header) */
 } gg_params;
@@ -148,6 +150,11 @@ int gg_load_voxels(gg_ctx* ctx, int32_t nn, const int32_t* ids, int32_t n_grains
 /* Same, reading the .uds/.bin pair named by the parameters (paths relative to
  * base_dir when not absolute). */
 int gg_load_voxel_files(gg_ctx* ctx, const char* base_dir);
+/* Stored elastic energies, one per grain (index id-1), the .uds storedEnergy
+ * column that grainhdl::read_HeaderCPG reads when UseStoredElasticEnergy is
+ * set (src/grainhdl.cpp:404-425); gg_load_voxel_files reads them from the
+ * file.  Call after gg_load_voxels, before gg_distance_initialisation. */
+int gg_load_stored_energy(gg_ctx* ctx, const double* stored, int32_t n_grains);
 
 /* grainhdl::distanceInitialisation for mode-4 input (src/grainhdl.cpp:728-753,
  * src/box.cpp:322-341): +-h field, redistancing, contour. */
@@ -201,7 +208,7 @@ int gg_read_area_tangents(gg_ctx* ctx, double* out, int32_t capacity);
  * in their formats, into `directory`:
  *  - Texture_<loop>.ori: per existing grain with regular motion, in ID order:
  *    ID, direct-neighbour count, boundary flag, area, mean dA / AnalysisTimestep,
- *    perimeter, energy, stored elastic energy (0), Bunge Euler angles;
+ *    perimeter, energy, stored elastic energy, Bunge Euler angles;
  *  - MODF_<loop>.txt (anisotropic networks): the boundary-length-weighted
  *    misorientation distribution over DiscreteSamplingRate bins;
  *  - NrGrains&EnergyStatistics.txt: one line appended (the file is started

@@ -60,6 +60,19 @@ def g6(x) -> str:
     return "%.6g" % x
 
 
+def read_uds_stored(path: str) -> dict:
+    """Grain ID -> stored energy (column 12) from a mode-4 .uds header."""
+    out = {}
+    with open(path) as f:
+        lines = f.read().splitlines()
+    start = next(i for i, l in enumerate(lines) if l.split()[:2] == ["ID", "x"]) + 1
+    for line in lines[start:]:
+        parts = line.split()
+        if len(parts) >= 12:
+            out[int(parts[0])] = float(parts[11])
+    return out
+
+
 def read_uds_euler(path: str) -> dict:
     """Grain ID -> Bunge angles from a mode-4 .uds header."""
     out = {}
@@ -73,9 +86,10 @@ def read_uds_euler(path: str) -> dict:
     return out
 
 
-def texture(record, euler: dict, analysis_timestep: int, nbins: int):
+def texture(record, euler: dict, analysis_timestep: int, nbins: int, stored: dict | None = None):
     """(Texture_<loop>.ori text, MODF values, total energy) of a record taken
-    right after the analysed step."""
+    right after the analysed step; `stored` maps grain IDs to their scaled
+    stored energies (LSbox's m_StoredElasticEnergy), else 0 is written."""
     lines = []
     modf = [0.0] * nbins
     dh = 62.8 / nbins if nbins else math.inf
@@ -94,7 +108,8 @@ def texture(record, euler: dict, analysis_timestep: int, nbins: int):
             if 0 <= key < nbins:
                 modf[key] += local[key] / 2
         fields = [str(gid), str(len(g.neighbours)), str(int(bool(g.boundary))), g6(g.volume),
-                  g6(g.mean_da / float(analysis_timestep)), g6(g.perimeter), g6(g.energy), "0",
+                  g6(g.mean_da / float(analysis_timestep)), g6(g.perimeter), g6(g.energy),
+                  g6(stored[gid]) if stored else "0",
                   g6(e[0]), g6(e[1]), g6(e[2])]
         lines.append("\t".join(fields) + "\n")
         s = 0.0

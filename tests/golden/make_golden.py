@@ -17,6 +17,8 @@ import shutil
 import subprocess
 import sys
 
+import numpy as np
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.abspath(os.path.join(HERE, "..", ".."))
 sys.path.insert(0, ROOT)
@@ -39,6 +41,12 @@ CASES = {
     # NrGrains&EnergyStatistics.txt) every 5 steps, written by the reference
     # into <case>/analysis
     "ana_iso_v80": ("voronoi", 80, 100, 11, 40, 0, {"IsIsotropicNetwork": 1, "AnalysisTimestep": 5}),
+    # stored elastic energies uniform in [0, 3000) (seeded separately), a
+    # boundary default of 500: the stored-energy term of the corrector and the
+    # time-step correction it implies; analysis files every 5 steps
+    "se_v30": ("voronoi", 30, 120, 6, 20, 5,
+               {"IsIsotropicNetwork": 0, "UseStoredElasticEnergy": 1, "DislocEnPerM": 1.0,
+                "BoxDefaultStoredElasticEnergy": 500.0, "AnalysisTimestep": 5}),
     "ana_mob_v80": ("voronoi", 80, 100, 12, 40, 0,
                     {"IsIsotropicNetwork": 0, "UseMobilityModel": 1, "TriplePointDrag": 2.0,
                      "AnalysisTimestep": 5}),
@@ -51,10 +59,12 @@ def make_case(name: str, spec) -> dict:
     if os.path.isdir(d):
         shutil.rmtree(d)
     micro = ms.voronoi(n, nn, seed) if gen == "voronoi" else ms.clustered(n, nn, seed)
+    if over.get("UseStoredElasticEnergy"):
+        micro.stored = np.random.default_rng(1000 + seed).uniform(0.0, 3000.0, n)
     xml = ms.make_case(d, name, micro, NumberOfTimesteps=steps, **over)
     dump = os.path.join(d, "reference.dump")
     cmd = [GG_REF, os.path.basename(xml), "reference.dump", str(every), "1"]
-    if name.startswith("ana_"):
+    if name.startswith("ana_") or "AnalysisTimestep" in over:
         os.makedirs(os.path.join(d, "analysis"))
         cmd.append("analysis")
     out = subprocess.run(cmd, cwd=d, check=True, capture_output=True, text=True)

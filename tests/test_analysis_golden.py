@@ -16,7 +16,7 @@ sys.path.insert(0, ROOT)
 from oracle import analysis  # noqa: E402
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-CASES = ["ana_iso_v80", "ana_mob_v80"]
+CASES = ["ana_iso_v80", "ana_mob_v80", "se_v30"]
 
 
 def _case(name):
@@ -40,7 +40,12 @@ def test_last_texture_and_modf_restated_from_the_final_state(name):
     final = dump.records[-1]
     assert final.steps == steps + 1
     iso = info["overrides"]["IsIsotropicNetwork"] == 1
-    text, modf, _ = analysis.texture(final, euler, info["overrides"]["AnalysisTimestep"], 31)
+    stored = None
+    if info["overrides"].get("UseStoredElasticEnergy"):
+        # m_StoredElasticEnergy = value * DislocEnPerM / HAGB_Energy * Physical_Domain_Size (all 1 here)
+        stored = {g: v * (info["overrides"]["DislocEnPerM"] / 1.0 * 1.0)
+                  for g, v in analysis.read_uds_stored(os.path.join(d, name + ".uds")).items()}
+    text, modf, _ = analysis.texture(final, euler, info["overrides"]["AnalysisTimestep"], 31, stored)
     assert text == _read(os.path.join(d, "analysis", f"Texture_{steps}.ori"))
     assert analysis.modf_text(modf, iso) == _read(os.path.join(d, "analysis", f"MODF_{steps}.txt"))
     if not iso:

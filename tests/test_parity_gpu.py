@@ -20,7 +20,7 @@ from tests.parity import compare_records, ownership_mismatch
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 ISO = ["iso_v20", "iso_v60"]
-ANISO = ["rs_v30", "mob_v30"]
+ANISO = ["rs_v30", "mob_v30", "se_v30"]
 
 
 def _run_against_reference(case, tmp_path, *, exact, inject=True, precision=0):
@@ -89,7 +89,7 @@ def _areas(h):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["iso_v60", "rs_v30", "mob_v30"])
+@pytest.mark.parametrize("case", ["iso_v60", "rs_v30", "mob_v30", "se_v30"])
 def test_batched_fp32_area_error_vs_plain(case):
     """The batched FP32 form (graph-captured steps) against the plain FP64
     form from the same initial state: per-grain relative area error <= 1e-3
@@ -119,3 +119,25 @@ def test_batched_fp32_area_error_vs_plain(case):
         assert h.status() == 0
         h.close()
     assert worst <= 1e-3, worst
+
+
+@pytest.mark.gpu
+def test_stored_energy_time_step_and_tangent_guard():
+    """UseStoredElasticEnergy: the time step is the reference's, shortened by
+    the largest stored-energy difference (find_correctTimestepSize), and the
+    parameter derivatives, which do not cover the stored-energy term, are
+    refused."""
+    from gragles2d_b200 import gg
+
+    d = os.path.join(GOLDEN, "se_v30")
+    ref = dumpfile.read(os.path.join(d, "reference.dump.gz"))
+    h = gg.GrainHandler(gg.Settings(os.path.join(d, "se_v30.xml")))
+    try:
+        h.load_voxel_files()
+        with pytest.raises(gg.GGError):
+            h.enable_tangents()
+        h.distanceInitialisation()
+        assert h.dims().dt == ref.dt
+        assert ref.dt < 0.8 / 120**2 * 21 / 2 / 5.0 / 10  # shortened well below the uncorrected step
+    finally:
+        h.close()
