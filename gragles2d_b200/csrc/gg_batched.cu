@@ -339,8 +339,8 @@ __device__ __forceinline__ int project_warp(const float2* P, const float4* cbb, 
     return seg;
 }
 
-// kStored: with the stored-energy term (UseStoredElasticEnergy).
-template <bool kStored>
+// kForces: with the stored-energy and / or magnetic driving-force terms.
+template <bool kForces>
 __global__ void __launch_bounds__(128, 8) k_corrector_f(NetConst C, NetState* S) {
     const int g = blockIdx.x + 1;
     if (g > C.N || C.state[g] != G_EXISTS || C.regular[g] == 0 || S->loop == 0 || halted(S)) return;
@@ -411,8 +411,14 @@ __global__ void __launch_bounds__(128, 8) k_corrector_f(NetConst C, NetState* S)
             id = idl[(i - ib.y0) * wi + (j - ib.x0)];
         }
         const bool valid = inside && val > -delta;
-        // stored-energy term (src/box.cpp:511-517) of inside pixels
-        const float se = (kStored && inside) ? (float)(nb_stored_force(nbt, (int)id) * C.dt / C.time_slope) : 0.f;
+        // driving-force terms (src/box.cpp:511-527) of inside pixels
+        float se = 0.f;
+        if (kForces && inside) {
+            double f = 0;
+            if (C.stored) f += nb_stored_force(nbt, (int)id) * C.dt / C.time_slope;
+            if (C.magnetic) f += nb_magnetic_force(nbt, (int)id) * C.dt / C.time_slope;
+            se = (float)f;
+        }
         if (inside && !valid) out[k] = -delta - se;
         if (__ballot_sync(0xffffffffu, valid) == 0u) continue;
         float lambda = 0.f;
@@ -487,7 +493,7 @@ __global__ void __launch_bounds__(128, 8) k_corrector_f(NetConst C, NetState* S)
 
 
 void launch_corrector_f(const NetConst& C, NetState* dS, cudaStream_t s) {
-    if (C.stored)
+    if (C.stored || C.magnetic)
         k_corrector_f<true><<<C.N, 128, 0, s>>>(C, dS);
     else
         k_corrector_f<false><<<C.N, 128, 0, s>>>(C, dS);

@@ -79,7 +79,8 @@ struct NbTable {
     int n;
     int id[48];
     double w[48];
-    double f[48];  // stored-energy driving force (own - neighbour energy) x mobility, when stored energies are on
+    double f[48];   // stored-energy driving force (own - neighbour energy) x mobility, when stored energies are on
+    double fm[48];  // magnetic driving force, the same with the magnetic energies, when the field is on
 };
 
 __device__ void build_nb_table(const NetConst& C, int owner, NbTable& T) {
@@ -93,6 +94,7 @@ __device__ void build_nb_table(const NetConst& C, int owner, NbTable& T) {
         const double v = nb[e].energy * nb[e].mobility;
         T.w[e] = v > 0.01 ? v : 0.01;
         T.f[e] = (C.stored && !gone) ? (C.stored[owner] - C.stored[id]) * nb[e].mobility : 0.0;
+        T.fm[e] = (C.magnetic && !gone) ? (C.magnetic[owner] - C.magnetic[id]) * nb[e].mobility : 0.0;
     }
 }
 
@@ -104,16 +106,27 @@ __device__ __forceinline__ double nb_stored_force(const NbTable& T, int id) {
     return -1.0;
 }
 
-// The stored-energy term the corrector subtracts at (row, col)
-// (src/box.cpp:511-517): f(IDLocal) dt / TimeSlope.
-__device__ __forceinline__ double stored_energy_term(const NetConst& C, const NbTable& T, const uint32_t* idl,
-                                                     const Box& ib, int row, int col, uint32_t* status) {
+// ExplicitGrainBoundary::get_f_magneticEnergy (src/grainBoundary.cpp:623-631).
+__device__ __forceinline__ double nb_magnetic_force(const NbTable& T, int id) {
+    for (int e = 0; e < T.n; ++e)
+        if (T.id[e] == id) return T.fm[e];
+    return -1.0;
+}
+
+// The driving-force terms the corrector subtracts at (row, col), stored
+// energy first, then magnetic (src/box.cpp:511-527): f(IDLocal) dt / TimeSlope.
+template <typename R>
+__device__ __forceinline__ R subtract_driving_forces(const NetConst& C, const NbTable& T, const uint32_t* idl,
+                                                     const Box& ib, int row, int col, R value, uint32_t* status) {
     uint32_t k;
     if (!buf_index(ib, row, col, &k)) {
         *status |= S_INDEX;
-        return 0.0;
+        return value;
     }
-    return nb_stored_force(T, (int)idl[k]) * C.dt / C.time_slope;
+    const int id = (int)idl[k];
+    if (C.stored) value = (R)((double)value - nb_stored_force(T, id) * C.dt / C.time_slope);
+    if (C.magnetic) value = (R)((double)value - nb_magnetic_force(T, id) * C.dt / C.time_slope);
+    return value;
 }
 
 // getGBEnergyTimesGBMobility(i, j) through the table (first match, as the
@@ -696,7 +709,7 @@ __global__ void __launch_bounds__(128) k_corrector(NetConst C, NetState* S) {
         } else {
             out[k] = -delta;
         }
-        if (C.stored) out[k] = (R)((double)out[k] - stored_energy_term(C, nbt, idl, ib, i, j, &st));
+        if (C.stored || C.magnetic) out[k] = subtract_driving_forces<R>(C, nbt, idl, ib, i, j, out[k], &st);
     }
     if (st) set_status(S, st);
 }

@@ -128,6 +128,7 @@ struct NetConst {
     Neighbour* nb;     // nbmax per grain
     int32_t* gone_loop;  // loop of the step whose level set deleted the grain, else -1
     double* stored;      // UseStoredElasticEnergy: scaled stored energy per grain, slot 0 = boundary (else null)
+    double* magnetic;    // UseMagneticField: magnetic energy per grain, slot 0 = boundary (else null)
     double time_slope;   // GaussianKernelUserDefTimeSlope
 
     // tables (host-computed, libm on the host)

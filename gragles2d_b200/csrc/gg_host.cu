@@ -49,6 +49,7 @@ struct gg_ctx {
     std::vector<int32_t> bbox;    // 5 per grain
     std::vector<double> stored;   // .uds stored energy per grain (empty: none given)
     std::vector<double> stored_scaled;  // UseStoredElasticEnergy: scaled values, slot 0 = boundary
+    std::vector<double> magnetic;       // UseMagneticField: magnetic energies, slot 0 = boundary
 
     NetConst C{};
     NetState hS{};               // host copy of the device NetState (pointers)
@@ -163,6 +164,25 @@ void quaternion2euler(const double* q, double* e) {
     e[0] = phi1;
     e[1] = PHI;
     e[2] = phi2;
+}
+
+// LSbox::calculateMagneticEnergy (src/box.cpp:2238-2292): the grain's c axis
+// (the sample normal rotated by its Bunge angles) against the field direction,
+// 1/2 mu0 dchi B^2 cos^2, normalised by HAGB_Energy and the domain size.
+double magnetic_energy(const double* q, const gg_params& P) {
+    double e[3];
+    quaternion2euler(q, e);
+    const double p1 = e[0], t = e[1];
+    // row 3 of the rotation matrix (the rotated normal), each entry summed
+    // onto zero as the reference's matrix-vector loop does
+    const double axis[3] = {0.0 + sin(p1) * sin(t), 0.0 + -cos(p1) * sin(t), 0.0 + cos(t)};
+    double cosine = (P.magnetic_vector[0] * axis[0]) + (P.magnetic_vector[1] * axis[1]) +
+                    (P.magnetic_vector[2] * axis[2]);
+    if (cosine > 1) cosine = 1.0;
+    double energy = 0.5 * P.vacuum_permeability * P.delta_mag_sys * P.magnetic_force_field * P.magnetic_force_field *
+                    cosine * cosine;
+    energy = energy / P.hagb_energy * P.physical_domain_size;
+    return energy;
 }
 
 // DimensionalBuffer::resizeToSquare (src/dimensionalBuffer.h:123-160)
@@ -330,6 +350,36 @@ int gg_params_from_xml(const char* path, gg_params* p) {
         getd("DislocEnPerM", &p->dislocation_energy_per_m);
         getd("BoxDefaultStoredElasticEnergy", &p->box_default_stored_elastic_energy);
         geti("Precision", &p->precision);
+        // magnetic field parameters from the file MagneticParams names
+        // (Settings::readMagneticFieldParams, src/Settings.cpp:291-347); a
+        // relative name is looked up beside the parameters file first
+        if (p->use_magnetic_field == 1) {
+            std::string name;
+            if (!xml_tag(doc, "MagneticParams", &name)) return GG_E_IO;
+            name = trim(name);
+            std::ifstream mf;
+            if (!name.empty() && name[0] != '/') {
+                std::string dir(path);
+                const size_t slash = dir.rfind('/');
+                dir = slash == std::string::npos ? std::string() : dir.substr(0, slash + 1);
+                mf.open(dir + name);
+            }
+            if (!mf) mf.open(name);
+            if (!mf) return GG_E_IO;
+            std::stringstream ms;
+            ms << mf.rdbuf();
+            const std::string mdoc = ms.str();
+            if (mdoc.find("<Parameters>") == std::string::npos) return GG_E_IO;
+            auto getm = [&](const char* tag, double* dst) {
+                if (xml_tag(mdoc, tag, &v)) *dst = std::stod(trim(v));
+            };
+            getm("VacuumPermeability", &p->vacuum_permeability);
+            getm("MagneticVector_x", &p->magnetic_vector[0]);
+            getm("MagneticVector_y", &p->magnetic_vector[1]);
+            getm("MagneticVector_z", &p->magnetic_vector[2]);
+            getm("deltaMagSys", &p->delta_mag_sys);
+            getm("MagneticForceField", &p->magnetic_force_field);
+        }
     } catch (...) {
         return GG_E_IO;
     }
@@ -352,7 +402,7 @@ int gg_create(const gg_params* p, int device, gg_ctx** out) {
     if (p->lattice_type != 0) return bad("only LatticeType 0 (cubic) is supported");
     if (p->research_mode != 0) return bad("only ResearchMode 0 is supported");
     if (p->grid_coarsement != 0) return bad("GridCoarsement must be 0");
-    if (p->use_magnetic_field != 0) return bad("the magnetic driving force is not supported");
+    if (p->use_magnetic_field < 0 || p->use_magnetic_field > 1) return bad("UseMagneticField must be 0 or 1");
     if (p->use_stored_elastic_energy < 0 || p->use_stored_elastic_energy > 1)
         return bad("UseStoredElasticEnergy must be 0 or 1");
     if (p->identify_twins != 0) return bad("IdentifyTwins is not supported");
@@ -506,6 +556,8 @@ int gg_distance_initialisation(gg_ctx* c) {
     // grainhdl::find_correctTimestepSize, 250-274).  Slot 0 is the boundary.
     std::vector<double>& stored_scaled = c->stored_scaled;
     stored_scaled.clear();
+    double energy_delta_max = 0;  // grainhdl::m_Energy_deltaMAX
+    bool correct_dt = false;
     if (P.use_stored_elastic_energy) {
         if (c->stored.size() != (size_t)c->N) return fail(c, GG_E_STATE, "no stored energies loaded");
         const double D = P.dislocation_energy_per_m, H = P.hagb_energy, L = P.physical_domain_size;
@@ -523,7 +575,36 @@ int gg_distance_initialisation(gg_ctx* c) {
         if (std::fabs(stored_scaled[0]) / D * H / L < lo) lo = std::fabs(stored_scaled[0]) / D * H / L;
         if (std::fabs(stored_scaled[0]) / D * H / L > hi) hi = std::fabs(stored_scaled[0]) / D * H / L;
         if (c->N == 1) lo = 0.0;
-        const double energy_delta_max = D * (hi - lo) / H * L;
+        energy_delta_max = D * (hi - lo) / H * L;
+        correct_dt = true;
+    }
+    // Magnetic energies (UseMagneticField): per grain from its orientation,
+    // slot 0 the boundary's (identity orientation, src/box.cpp:35-49); their
+    // range over grains 1 .. N-1 present (the reference's loop bound) replaces
+    // the stored-energy difference (find_correctTimestepSize,
+    // src/grainhdl.cpp:250-265).
+    std::vector<double>& magnetic = c->magnetic;
+    magnetic.clear();
+    if (P.use_magnetic_field) {
+        magnetic.assign((size_t)c->N + 1, 0.0);
+        const double identity[4] = {1.0, 0.0, 0.0, 0.0};
+        magnetic[0] = magnetic_energy(identity, P);
+        for (int g = 1; g <= c->N; ++g) {
+            double q[4];
+            euler2quaternion(&c->euler[3 * (size_t)(g - 1)], q);
+            magnetic[g] = magnetic_energy(q, P);
+        }
+        double lo = 1000000, hi = 0;
+        for (int g = 1; g < c->N; ++g) {
+            if (c->bbox[5 * (size_t)(g - 1) + 4] == 0) continue;  // absent grain (no LSbox)
+            if (magnetic[g] < lo) lo = magnetic[g];
+            if (magnetic[g] > hi) hi = magnetic[g];
+        }
+        if (c->N == 1) lo = 0.0;
+        energy_delta_max = hi - lo;
+        correct_dt = true;
+    }
+    if (correct_dt) {
         const double vmax = energy_delta_max * c->dt;
         double correction = 0.5 / (vmax / c->h);
         if (correction > 1.0) correction = 1.0;
@@ -629,6 +710,7 @@ int gg_distance_initialisation(gg_ctx* c) {
     ALLOC(C.gone_loop, N + 1);
     C.time_slope = P.time_slope;
     if (P.use_stored_elastic_energy) ALLOC(C.stored, N + 1);
+    if (P.use_magnetic_field) ALLOC(C.magnetic, N + 1);
     GG_CUDA(c, cudaMemsetAsync(C.gone_loop, 0xff, sizeof(int32_t) * (N + 1), c->stream));
 
     // tables: twiddles and Gaussian multipliers (plain), separable kernels (batched)
@@ -807,6 +889,7 @@ int gg_distance_initialisation(gg_ctx* c) {
     GG_CUDA(c, h2d(C.regular, ones.data(), sizeof(int32_t) * (N + 1)));
     GG_CUDA(c, h2d(C.quat, quat.data(), sizeof(double) * quat.size()));
     if (C.stored) GG_CUDA(c, h2d(C.stored, stored_scaled.data(), sizeof(double) * stored_scaled.size()));
+    if (C.magnetic) GG_CUDA(c, h2d(C.magnetic, magnetic.data(), sizeof(double) * magnetic.size()));
     GG_CUDA(c, h2d(c->d_ids, c->ids.data(), sizeof(int32_t) * c->ids.size()));
     S.phi_used = a;
     S.spec_used = sp;
@@ -1010,8 +1093,8 @@ int gg_tangent_enable(gg_ctx* c, int32_t enable) {
     if (c->initialised) return fail(c, GG_E_STATE, "tangents must be enabled before gg_distance_initialisation");
     if (enable && c->P.precision != GG_PRECISION_PLAIN)
         return fail(c, GG_E_INVALID, "tangents need the plain (FP64) form");
-    if (enable && c->P.use_stored_elastic_energy)
-        return fail(c, GG_E_INVALID, "tangents do not cover the stored-energy driving force");
+    if (enable && (c->P.use_stored_elastic_energy || c->P.use_magnetic_field))
+        return fail(c, GG_E_INVALID, "tangents do not cover the stored-energy or magnetic driving force");
     c->tangents = enable != 0;
     return GG_OK;
 }
@@ -1102,7 +1185,8 @@ int gg_write_analysis(gg_ctx* c, const char* directory, int32_t loop) {
         }
         tex << g << '\t' << nbn[g] << '\t' << (bnd[g] != 0) << '\t' << vol[g] << '\t'
             << mda[g] / (double)c->P.analysis_timestep << '\t' << per[g] << '\t' << en[g] << '\t'
-            << (c->stored_scaled.empty() ? 0.0 : c->stored_scaled[g]) << '\t' << eul[0] << '\t' << eul[1] << '\t' << eul[2] << std::endl;
+            << (!c->magnetic.empty() ? c->magnetic[g] : c->stored_scaled.empty() ? 0.0 : c->stored_scaled[g])
+            << '\t' << eul[0] << '\t' << eul[1] << '\t' << eul[2] << std::endl;
         double sum = 0.0;
         for (int i = 0; i < nbins; ++i) sum += modf[i];
         for (int i = 0; i < nbins; ++i)

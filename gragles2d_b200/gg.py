@@ -61,7 +61,9 @@ class Params(ctypes.Structure):
         ("hagb_mobility", ctypes.c_double), ("physical_domain_size", ctypes.c_double),
         ("time_slope", ctypes.c_double), ("theta_ref_deg", ctypes.c_double), ("gamma_hagb", ctypes.c_double),
         ("m_hagb", ctypes.c_double), ("dislocation_energy_per_m", ctypes.c_double),
-        ("box_default_stored_elastic_energy", ctypes.c_double), ("reserved_d", ctypes.c_double * 4),
+        ("box_default_stored_elastic_energy", ctypes.c_double), ("vacuum_permeability", ctypes.c_double),
+        ("magnetic_vector", ctypes.c_double * 3), ("delta_mag_sys", ctypes.c_double),
+        ("magnetic_force_field", ctypes.c_double), ("reserved_d", ctypes.c_double * 2),
         ("read_from_filename", ctypes.c_char * 512), ("additional_filename", ctypes.c_char * 512),
     ]
 

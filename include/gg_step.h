@@ -88,7 +88,7 @@ typedef struct gg_params {
     int32_t decouple_grains;          /* DecoupleGrains */
     int32_t grid_coarsement;          /* GridCoarsement (0 supported) */
     int32_t use_stored_elastic_energy;/* UseStoredElasticEnergy (0, 1) */
-    int32_t use_magnetic_field;       /* UseMagneticField (0 supported) */
+    int32_t use_magnetic_field;       /* UseMagneticField (0, 1; parameters from the MagneticParams file) */
     int32_t discrete_sampling_rate;   /* DiscreteSamplingRate (bins of the MODF output) */
     int32_t reserved_i[4];
     double triple_point_drag;         /* TriplePointDrag */
@@ -103,7 +103,13 @@ typedef struct gg_params {
     double m_hagb;                    /* relative high-angle boundary mobility */
     double dislocation_energy_per_m;  /* DislocEnPerM (scales the stored energies) */
     double box_default_stored_elastic_energy; /* BoxDefaultStoredElasticEnergy (domain boundary) */
-    double reserved_d[4];
+    /* magnetic field: the tags of the file that MagneticParams names
+     * (Settings::readMagneticFieldParams, src/Settings.cpp:291-347) */
+    double vacuum_permeability;       /* VacuumPermeability */
+    double magnetic_vector[3];        /* MagneticVector_x, _y, _z (unit field direction) */
+    double delta_mag_sys;             /* deltaMagSys (susceptibility difference) */
+    double magnetic_force_field;      /* MagneticForceField */
+    double reserved_d[2];
     char read_from_filename[512];     /* ReadFromFilename (.bin ID field) */
     char additional_filename[512];    /* AdditionalFilename (.uds header) */
 } gg_params;

@@ -55,6 +55,20 @@ def quaternion2euler(q):
     return phi1, phi, phi2
 
 
+def magnetic_energy(euler, vacuum_permeability, vector, delta_mag_sys, force_field, hagb_energy=1.0,
+                    physical_domain_size=1.0):
+    """LSbox::calculateMagneticEnergy (src/box.cpp:2238-2292) of a grain with
+    the given input Bunge angles: the c axis (the sample normal rotated by the
+    quaternion round trip of the angles) against the field direction."""
+    p1, t, _ = quaternion2euler(euler2quaternion(euler))
+    axis = (0.0 + math.sin(p1) * math.sin(t), 0.0 + -math.cos(p1) * math.sin(t), 0.0 + math.cos(t))
+    cosine = (vector[0] * axis[0]) + (vector[1] * axis[1]) + (vector[2] * axis[2])
+    if cosine > 1:
+        cosine = 1.0
+    e = 0.5 * vacuum_permeability * delta_mag_sys * force_field * force_field * cosine * cosine
+    return e / hagb_energy * physical_domain_size
+
+
 def g6(x) -> str:
     """A double through an ostream with default flags."""
     return "%.6g" % x

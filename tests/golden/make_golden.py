@@ -47,10 +47,19 @@ CASES = {
     "se_v30": ("voronoi", 30, 120, 6, 20, 5,
                {"IsIsotropicNetwork": 0, "UseStoredElasticEnergy": 1, "DislocEnPerM": 1.0,
                 "BoxDefaultStoredElasticEnergy": 500.0, "AnalysisTimestep": 5}),
+    # magnetic driving force: field direction (0.6, 0, 0.8), 1/2 mu0 dchi B^2 = 800,
+    # read from magnetic.xml beside the parameters; analysis files every 5 steps
+    "mag_v30": ("voronoi", 30, 120, 7, 20, 5,
+                {"IsIsotropicNetwork": 0, "UseMagneticField": 1, "MagneticParams": "magnetic.xml",
+                 "AnalysisTimestep": 5}),
     "ana_mob_v80": ("voronoi", 80, 100, 12, 40, 0,
                     {"IsIsotropicNetwork": 0, "UseMobilityModel": 1, "TriplePointDrag": 2.0,
                      "AnalysisTimestep": 5}),
 }
+
+
+MAGNETIC = {"VacuumPermeability": 1.0, "MagneticVector_x": 0.6, "MagneticVector_y": 0.0, "MagneticVector_z": 0.8,
+            "deltaMagSys": 1.0, "MagneticForceField": 40.0}
 
 
 def make_case(name: str, spec) -> dict:
@@ -62,6 +71,12 @@ def make_case(name: str, spec) -> dict:
     if over.get("UseStoredElasticEnergy"):
         micro.stored = np.random.default_rng(1000 + seed).uniform(0.0, 3000.0, n)
     xml = ms.make_case(d, name, micro, NumberOfTimesteps=steps, **over)
+    if over.get("UseMagneticField"):
+        with open(os.path.join(d, over["MagneticParams"]), "w") as f:
+            f.write('<?xml version="1.0" encoding="utf-8"?>\n<Parameters>\n')
+            for k, v in MAGNETIC.items():
+                f.write(f"   <{k}> {v} </{k}>\n")
+            f.write("</Parameters>\n")
     dump = os.path.join(d, "reference.dump")
     cmd = [GG_REF, os.path.basename(xml), "reference.dump", str(every), "1"]
     if name.startswith("ana_") or "AnalysisTimestep" in over:

@@ -16,7 +16,7 @@ sys.path.insert(0, ROOT)
 from oracle import analysis  # noqa: E402
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-CASES = ["ana_iso_v80", "ana_mob_v80", "se_v30"]
+CASES = ["ana_iso_v80", "ana_mob_v80", "se_v30", "mag_v30"]
 
 
 def _case(name):
@@ -45,6 +45,13 @@ def test_last_texture_and_modf_restated_from_the_final_state(name):
         # m_StoredElasticEnergy = value * DislocEnPerM / HAGB_Energy * Physical_Domain_Size (all 1 here)
         stored = {g: v * (info["overrides"]["DislocEnPerM"] / 1.0 * 1.0)
                   for g, v in analysis.read_uds_stored(os.path.join(d, name + ".uds")).items()}
+    if info["overrides"].get("UseMagneticField"):
+        # the magnetic energy takes the stored energy's column
+        import re
+        M = {k: float(v) for k, v in re.findall(r"<(\w+)>\s*([^<]+?)\s*</\1>", _read(os.path.join(d, "magnetic.xml")))}
+        vec = (M["MagneticVector_x"], M["MagneticVector_y"], M["MagneticVector_z"])
+        stored = {g: analysis.magnetic_energy(e, M["VacuumPermeability"], vec, M["deltaMagSys"], M["MagneticForceField"])
+                  for g, e in euler.items()}
     text, modf, _ = analysis.texture(final, euler, info["overrides"]["AnalysisTimestep"], 31, stored)
     assert text == _read(os.path.join(d, "analysis", f"Texture_{steps}.ori"))
     assert analysis.modf_text(modf, iso) == _read(os.path.join(d, "analysis", f"MODF_{steps}.txt"))

@@ -15,7 +15,7 @@ from gragles2d_b200 import gg
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["ana_iso_v80", "ana_mob_v80", "se_v30"]
+CASES = ["ana_iso_v80", "ana_mob_v80", "se_v30", "mag_v30"]
 
 
 def _run(golden_dir, name, precision, out, run_sim=False):
@@ -57,7 +57,8 @@ def _text(path):
         return f.read()
 
 
-@pytest.mark.parametrize("name,run_sim", [(CASES[0], False), (CASES[1], False), (CASES[2], False), (CASES[0], True)])
+@pytest.mark.parametrize("name,run_sim", [(CASES[0], False), (CASES[1], False), (CASES[2], False), (CASES[3], False),
+                                          (CASES[0], True)])
 def test_plain_form_writes_the_reference_files(golden_dir, name, run_sim, tmp_path):
     d, info, loops = _run(golden_dir, name, gg.PRECISION_PLAIN, tmp_path, run_sim)
     ref_dir = os.path.join(d, "analysis")

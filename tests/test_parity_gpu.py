@@ -20,7 +20,7 @@ from tests.parity import compare_records, ownership_mismatch
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 ISO = ["iso_v20", "iso_v60"]
-ANISO = ["rs_v30", "mob_v30", "se_v30"]
+ANISO = ["rs_v30", "mob_v30", "se_v30", "mag_v30"]
 
 
 def _run_against_reference(case, tmp_path, *, exact, inject=True, precision=0):
@@ -89,7 +89,7 @@ def _areas(h):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["iso_v60", "rs_v30", "mob_v30", "se_v30"])
+@pytest.mark.parametrize("case", ["iso_v60", "rs_v30", "mob_v30", "se_v30", "mag_v30"])
 def test_batched_fp32_area_error_vs_plain(case):
     """The batched FP32 form (graph-captured steps) against the plain FP64
     form from the same initial state: per-grain relative area error <= 1e-3
@@ -122,16 +122,17 @@ def test_batched_fp32_area_error_vs_plain(case):
 
 
 @pytest.mark.gpu
-def test_stored_energy_time_step_and_tangent_guard():
-    """UseStoredElasticEnergy: the time step is the reference's, shortened by
-    the largest stored-energy difference (find_correctTimestepSize), and the
-    parameter derivatives, which do not cover the stored-energy term, are
-    refused."""
+@pytest.mark.parametrize("case", ["se_v30", "mag_v30"])
+def test_driving_force_time_step_and_tangent_guard(case):
+    """UseStoredElasticEnergy / UseMagneticField: the time step is the
+    reference's, shortened by the largest energy difference
+    (find_correctTimestepSize), and the parameter derivatives, which do not
+    cover these terms, are refused."""
     from gragles2d_b200 import gg
 
-    d = os.path.join(GOLDEN, "se_v30")
+    d = os.path.join(GOLDEN, case)
     ref = dumpfile.read(os.path.join(d, "reference.dump.gz"))
-    h = gg.GrainHandler(gg.Settings(os.path.join(d, "se_v30.xml")))
+    h = gg.GrainHandler(gg.Settings(os.path.join(d, case + ".xml")))
     try:
         h.load_voxel_files()
         with pytest.raises(gg.GGError):
