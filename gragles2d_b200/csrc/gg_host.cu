@@ -280,6 +280,7 @@ int gg_params_default(gg_params* p) {
     p->struct_size = (int32_t)sizeof(gg_params);
     p->precision = GG_PRECISION_PLAIN;
     p->analysis_timestep = 1;
+    p->grid_coarsement_gradient = 0.95;
     p->domain_border_size = 7;
     p->microstructure_gen_mode = 4;
     p->convolution_mode = 2;
@@ -350,6 +351,13 @@ int gg_params_from_xml(const char* path, gg_params* p) {
         getd("DislocEnPerM", &p->dislocation_energy_per_m);
         getd("BoxDefaultStoredElasticEnergy", &p->box_default_stored_elastic_energy);
         geti("Precision", &p->precision);
+        geti("PlotInterval", &p->plot_interval);
+        geti("UseTexture", &p->use_texture);
+        geti("ExecuteInParallel", &p->execute_in_parallel);
+        geti("MaximumNumberOfThreads", &p->maximum_number_of_threads);
+        geti("NeighbourTracking", &p->neighbour_tracking);
+        geti("GrainScheduler", &p->grain_scheduler);
+        getd("GridCoarsementGradient", &p->grid_coarsement_gradient);
         // magnetic field parameters from the file MagneticParams names
         // (Settings::readMagneticFieldParams, src/Settings.cpp:291-347); a
         // relative name is looked up beside the parameters file first
@@ -1213,6 +1221,106 @@ int gg_write_analysis(gg_ctx* c, const char* directory, int32_t loop) {
     std::ofstream st(stats_path, loop == 0 ? std::ios::out : std::ios::app);
     if (!st) return fail(c, GG_E_IO, "cannot write " + stats_path);
     st << realtime << "\t" << nr << "\t" << 0.5 * total_energy << "\t" << c->nn << std::endl;
+    return GG_OK;
+}
+
+int gg_write_restart(gg_ctx* c, const char* directory, int32_t loop) {
+    if (!c || !directory) return GG_E_INVALID;
+    if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
+    int rc = refresh_state(c);
+    if (rc) return rc;
+    if (loop < c->P.start_time || c->hS.loop != loop + 1)
+        return fail(c, GG_E_STATE, "loop is not the last completed step");
+    const int N = c->N;
+    const NetState& S = c->hS;
+    std::vector<int32_t> state(N + 1), gone(N + 1), cn(N + 1);
+    std::vector<int64_t> coff(N + 1);
+    auto d2h = [&](void* dst, const void* src, size_t bytes) {
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream);
+    };
+    GG_CUDA(c, d2h(state.data(), c->C.state, 4 * (N + 1)));
+    GG_CUDA(c, d2h(gone.data(), c->C.gone_loop, 4 * (N + 1)));
+    GG_CUDA(c, d2h(cn.data(), S.cn_prev, 4 * (N + 1)));
+    GG_CUDA(c, d2h(coff.data(), S.coff_prev, 8 * (N + 1)));
+    GG_CUDA(c, cudaStreamSynchronize(c->stream));
+    // the latest contours (rotated into the previous-contour arena at the end
+    // of the step), copied as one range
+    int64_t lo = INT64_MAX, hi = 0;
+    for (int g = 1; g <= N; ++g)
+        if (state[g] == G_EXISTS && cn[g] > 0) {
+            lo = std::min(lo, coff[g]);
+            hi = std::max(hi, coff[g] + cn[g]);
+        }
+    std::vector<CPoint> pts(hi > lo ? (size_t)(hi - lo) : 0);
+    if (!pts.empty()) {
+        GG_CUDA(c, d2h(pts.data(), S.contPrev + lo, sizeof(CPoint) * pts.size()));
+        GG_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    int nr = 0;  // grains present when the step began (as in gg_write_analysis)
+    for (int g = 1; g <= N; ++g) nr += (state[g] != G_GONE || gone[g] == loop) ? 1 : 0;
+    const std::string tail = "_TIMESTEP_" + std::to_string(loop) + "_GRAINS_" + std::to_string(nr);
+    const std::string dat_name = "NETWORK_NONAME" + tail + ".dat";
+    const std::string dir(directory);
+    // LSbox::plot_full_grain (src/box.cpp:1552-1596), absolute coordinates
+    std::ofstream dat(dir + "/" + dat_name);
+    if (!dat) return fail(c, GG_E_IO, "cannot write " + dir + "/" + dat_name);
+    const double h = c->h;
+    const int blowup = c->b;
+    for (int g = 1; g <= N; ++g) {
+        if (state[g] != G_EXISTS) continue;
+        double q[4];
+        euler2quaternion(&c->euler[3 * (size_t)(g - 1)], q);
+        dat << g << "\t" << cn[g] << "\t" << q[0] << "\t" << q[1] << "\t" << q[2] << "\t" << q[3] << std::endl;
+        for (int k = 0; k < cn[g]; ++k) {
+            const CPoint& p = pts[(size_t)(coff[g] - lo + k)];
+            dat << (p.x - blowup) * h << "\t" << (p.y - blowup) * h << std::endl;
+        }
+        dat << std::endl;
+    }
+    dat.close();
+    // Settings::generateXMLParametersNode (src/Settings.cpp:363-400), printed
+    // as rapidxml prints a document: one tab-indented element per line
+    const gg_params& P = c->P;
+    std::ostringstream x;
+    auto tag = [&](const char* name, const auto& value) { x << "\t<" << name << ">" << value << "</" << name << ">\n"; };
+    auto flag = [](int v) { return v != 0 ? 1 : 0; };
+    x << "<?xml version=\"1.0\" encoding=\"utf-8\"?>\n<Parameters>\n";
+    tag("StartTime", loop);
+    tag("NumberOfParticles", nr);
+    tag("NumberOfPointsPerGrain", c->ppg);  // set from the grid in mode 4 (src/grainhdl.cpp:331)
+    tag("AnalysisTimestep", P.analysis_timestep);
+    tag("PlotInterval", P.plot_interval);
+    tag("NumberOfTimesteps", P.number_of_timesteps);
+    tag("BreakupNumber", P.breakup_number);
+    tag("DiscreteSamplingRate", P.discrete_sampling_rate);
+    tag("DomainBorderSize", P.domain_border_size);
+    tag("MicrostructureGenMode", 0);
+    tag("ReadFromFilename", dat_name);
+    tag("HAGB_Energy", P.hagb_energy);
+    tag("HAGB_Mobility", P.hagb_mobility);
+    tag("Physical_Domain_Size", P.physical_domain_size);
+    tag("TriplePointDrag", P.triple_point_drag);
+    tag("UseMobilityModel", P.use_mobility_model);
+    tag("IdentifyTwins", flag(P.identify_twins));
+    tag("IsIsotropicNetwork", flag(P.is_isotropic_network));
+    tag("UseTexture", flag(P.use_texture));
+    tag("ExecuteInParallel", flag(P.execute_in_parallel));
+    tag("MaximumNumberOfThreads", P.maximum_number_of_threads);
+    tag("GridCoarsement", flag(P.grid_coarsement));
+    tag("GridCoarsementGradient", P.grid_coarsement_gradient);
+    tag("ConvolutionMode", P.convolution_mode);
+    tag("ResearchMode", flag(P.research_mode));
+    tag("ResearchProject", P.research_project);
+    tag("ConstantSectorRadius", P.constant_sector_radius * c->h);  // scaled at set-up (src/grainhdl.cpp:130-131)
+    tag("InterpolatingSectorRadius", P.interpolating_sector_radius * c->h);
+    tag("NeighbourTracking", P.neighbour_tracking);
+    tag("UseStoredElasticEnergy", flag(P.use_stored_elastic_energy));
+    tag("GrainScheduler", P.grain_scheduler);
+    x << "</Parameters>\n\n";
+    const std::string xml_name = dir + "/PARAMETERS_SIM_NONAME" + tail + ".xml";
+    std::ofstream xf(xml_name);
+    if (!xf) return fail(c, GG_E_IO, "cannot write " + xml_name);
+    xf << x.str();
     return GG_OK;
 }
 

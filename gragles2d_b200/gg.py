@@ -28,7 +28,7 @@ EXPORTS = (
     "gg_load_voxel_files", "gg_load_stored_energy", "gg_distance_initialisation", "gg_find_neighbors", "gg_set_neighbours",
     "gg_convolution", "gg_update_second_order_neighbors", "gg_comparison", "gg_level_set", "gg_redistancing",
     "gg_grain_count", "gg_step", "gg_status", "gg_read_grain_stats", "gg_tangent_enable", "gg_read_area_tangents",
-    "gg_write_analysis", "gg_dims", "gg_dump", "gg_last_step_ms",
+    "gg_write_analysis", "gg_write_restart", "gg_dims", "gg_dump", "gg_last_step_ms",
     "gg_grain_updates", "gg_profile_steps", "gg_traffic", "gg_convolve_box_static",
 )
 STATIC_CONV_MAX_N = 128
@@ -55,7 +55,9 @@ class Params(ctypes.Structure):
         ("research_mode", ctypes.c_int32), ("research_project", ctypes.c_int32),
         ("decouple_grains", ctypes.c_int32), ("grid_coarsement", ctypes.c_int32),
         ("use_stored_elastic_energy", ctypes.c_int32), ("use_magnetic_field", ctypes.c_int32),
-        ("discrete_sampling_rate", ctypes.c_int32), ("reserved_i", ctypes.c_int32 * 4),
+        ("discrete_sampling_rate", ctypes.c_int32), ("plot_interval", ctypes.c_int32), ("use_texture", ctypes.c_int32),
+        ("execute_in_parallel", ctypes.c_int32), ("maximum_number_of_threads", ctypes.c_int32),
+        ("neighbour_tracking", ctypes.c_int32), ("grain_scheduler", ctypes.c_int32), ("reserved_i", ctypes.c_int32 * 2),
         ("triple_point_drag", ctypes.c_double), ("constant_sector_radius", ctypes.c_double),
         ("interpolating_sector_radius", ctypes.c_double), ("hagb_energy", ctypes.c_double),
         ("hagb_mobility", ctypes.c_double), ("physical_domain_size", ctypes.c_double),
@@ -63,7 +65,8 @@ class Params(ctypes.Structure):
         ("m_hagb", ctypes.c_double), ("dislocation_energy_per_m", ctypes.c_double),
         ("box_default_stored_elastic_energy", ctypes.c_double), ("vacuum_permeability", ctypes.c_double),
         ("magnetic_vector", ctypes.c_double * 3), ("delta_mag_sys", ctypes.c_double),
-        ("magnetic_force_field", ctypes.c_double), ("reserved_d", ctypes.c_double * 2),
+        ("magnetic_force_field", ctypes.c_double), ("grid_coarsement_gradient", ctypes.c_double),
+        ("reserved_d", ctypes.c_double * 1),
         ("read_from_filename", ctypes.c_char * 512), ("additional_filename", ctypes.c_char * 512),
     ]
 
@@ -113,6 +116,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "gg_tangent_enable": (I, [V, I]),
         "gg_read_area_tangents": (I, [V, P(D), I]),
         "gg_write_analysis": (I, [V, ctypes.c_char_p, I]),
+        "gg_write_restart": (I, [V, ctypes.c_char_p, I]),
         "gg_dims": (I, [V, P(I), P(I), P(D), P(D), P(D)]),
         "gg_dump": (I, [V, ctypes.c_char_p, I, I]),
         "gg_last_step_ms": (I, [V, P(D)]),
@@ -296,6 +300,8 @@ class GrainHandler:
             if analysis_dir is not None and ((loop - p.start_time) % p.analysis_timestep == 0
                                              or loop == p.number_of_timesteps):
                 self.write_analysis(analysis_dir, loop)
+                if (p.microstructure_gen_mode == 4 and loop == 0) or loop == p.number_of_timesteps:
+                    self.write_restart(analysis_dir, loop)
             live, _ = self.get_biggestGrainVol()
             if live < self.settings.p.breakup_number:
                 break
@@ -340,6 +346,11 @@ class GrainHandler:
         """save_Texture + save_NrGrainsStats of the completed step `loop`
         (default: the last one) into `directory`."""
         self._check(self.lib.gg_write_analysis(self.ctx, directory.encode(), self.loop - 1 if loop is None else loop))
+
+    def write_restart(self, directory: str, loop: int | None = None):
+        """save_Full_Microstructure_for_Restart of the completed step `loop`
+        (default: the last one) into `directory`."""
+        self._check(self.lib.gg_write_restart(self.ctx, directory.encode(), self.loop - 1 if loop is None else loop))
 
     def grain_updates(self) -> int:
         v = ctypes.c_int64()

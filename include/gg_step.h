@@ -90,7 +90,15 @@ typedef struct gg_params {
     int32_t use_stored_elastic_energy;/* UseStoredElasticEnergy (0, 1) */
     int32_t use_magnetic_field;       /* UseMagneticField (0, 1; parameters from the MagneticParams file) */
     int32_t discrete_sampling_rate;   /* DiscreteSamplingRate (bins of the MODF output) */
-    int32_t reserved_i[4];
+    /* control settings the step does not use; kept to be written back into
+     * restart parameter files */
+    int32_t plot_interval;            /* PlotInterval */
+    int32_t use_texture;              /* UseTexture */
+    int32_t execute_in_parallel;      /* ExecuteInParallel */
+    int32_t maximum_number_of_threads;/* MaximumNumberOfThreads */
+    int32_t neighbour_tracking;       /* NeighbourTracking */
+    int32_t grain_scheduler;          /* GrainScheduler */
+    int32_t reserved_i[2];
     double triple_point_drag;         /* TriplePointDrag */
     double constant_sector_radius;    /* ConstantSectorRadius (grid points) */
     double interpolating_sector_radius; /* InterpolatingSectorRadius (grid points) */
@@ -109,7 +117,8 @@ typedef struct gg_params {
     double magnetic_vector[3];        /* MagneticVector_x, _y, _z (unit field direction) */
     double delta_mag_sys;             /* deltaMagSys (susceptibility difference) */
     double magnetic_force_field;      /* MagneticForceField */
-    double reserved_d[2];
+    double grid_coarsement_gradient;  /* GridCoarsementGradient (written back only) */
+    double reserved_d[1];
     char read_from_filename[512];     /* ReadFromFilename (.bin ID field) */
     char additional_filename[512];    /* AdditionalFilename (.uds header) */
 } gg_params;
@@ -227,6 +236,23 @@ int gg_read_area_tangents(gg_ctx* ctx, double* out, int32_t capacity);
  * HAGB_Mobility) over the steps before `loop`.
  */
 int gg_write_analysis(gg_ctx* ctx, const char* directory, int32_t loop);
+
+/*
+ * Restart files of one timestep, as grainhdl::save_Full_Microstructure_for_Restart
+ * writes them (src/grainhdl.cpp:1179-1223, LSbox::plot_full_grain with
+ * absolute coordinates, src/box.cpp:1552-1596), into `directory`:
+ *  - NETWORK_NONAME_TIMESTEP_<loop>_GRAINS_<n>.dat: per existing grain, its ID,
+ *    contour length and orientation quaternion, then its contour points in
+ *    domain coordinates, then an empty line;
+ *  - PARAMETERS_SIM_NONAME_TIMESTEP_<loop>_GRAINS_<n>.xml: the parameters
+ *    (Settings::generateXMLParametersNode, src/Settings.cpp:363-400) with
+ *    StartTime <loop>, NumberOfParticles <n>, MicrostructureGenMode 0 and the
+ *    contour file as ReadFromFilename.
+ * <n> is the grain count at the start of step `loop`, as for the statistics
+ * file.  The reference writes them after step 0 of a voxelized input and after
+ * step NumberOfTimesteps.  Call after step `loop` has completed.
+ */
+int gg_write_restart(gg_ctx* ctx, const char* directory, int32_t loop);
 
 /* Number of grain slots N and the grid size (ngridpoints). */
 int gg_dims(gg_ctx* ctx, int32_t* n_grains, int32_t* ngridpoints, double* h, double* delta, double* dt);

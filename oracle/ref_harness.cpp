@@ -17,9 +17,9 @@
  *     stage by stage, skipping the analysis file writers (save_Texture /
  *     save_NetworkPlot / save_NrGrainsStats / restart files), which change
  *     no grain state, unless an analysis directory is given: then
- *     save_Texture and save_NrGrainsStats run on the reference's schedule
- *     (src/grainhdl.cpp:1098-1105) with that directory as the working
- *     directory;
+ *     save_Texture, save_NrGrainsStats and save_Full_Microstructure_for_Restart
+ *     run on the reference's schedule (src/grainhdl.cpp:1098-1112) with that
+ *     directory as the working directory;
  *   - writes a binary dump of every LSbox after initialisation and after
  *     chosen steps (format below), and the loop's wall time.
  *
@@ -255,6 +255,9 @@ int main(int argc, char** argv) {
                              sim->loop == Settings::NumberOfTimesteps)) {
             sim->save_Texture();
             sim->save_NrGrainsStats();
+            if ((Settings::MicrostructureGenMode == E_READ_VOXELIZED_MICROSTRUCTURE && sim->loop == 0) ||
+                sim->loop == Settings::NumberOfTimesteps)
+                sim->save_Full_Microstructure_for_Restart();
         }
         sim->Realtime += (sim->get_dt() * (Settings::Physical_Domain_Size * Settings::Physical_Domain_Size) /
                           (sim->TimeSlope * Settings::HAGB_Energy * Settings::HAGB_Mobility));

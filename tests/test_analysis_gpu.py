@@ -1,7 +1,8 @@
-"""The analysis writer (gg_write_analysis) against the files GraGLeS2D itself
-wrote in the same run (ana_* fixtures): Texture_<loop>.ori, MODF_<loop>.txt
-and NrGrains&EnergyStatistics.txt on the reference's schedule (every
-AnalysisTimestep steps and after the last).  The plain FP64 form must write
+"""The analysis writers (gg_write_analysis, gg_write_restart) against the
+files GraGLeS2D itself wrote in the same run: Texture_<loop>.ori,
+MODF_<loop>.txt and NrGrains&EnergyStatistics.txt on the reference's schedule
+(every AnalysisTimestep steps and after the last), and where the fixture has
+them (se_v30) the restart files written after step 0 and after the last step.  The plain FP64 form must write
 the same bytes; the batched FP32 form the same grains and counts with areas,
 energies and MODF values within FP32 tolerances.
 """
@@ -38,6 +39,8 @@ def _run(golden_dir, name, precision, out, run_sim=False):
                 h.step(1)
                 if loop in written:
                     h.write_analysis(str(out), loop)
+                    if loop in (0, info["steps"]):
+                        h.write_restart(str(out), loop)
         assert h.loop == info["steps"] + 1
         assert h.status() == 0
     finally:
@@ -62,9 +65,14 @@ def _text(path):
 def test_plain_form_writes_the_reference_files(golden_dir, name, run_sim, tmp_path):
     d, info, loops = _run(golden_dir, name, gg.PRECISION_PLAIN, tmp_path, run_sim)
     ref_dir = os.path.join(d, "analysis")
-    assert sorted(os.listdir(ref_dir)) == sorted(_files(loops))
-    for fn in _files(loops):
+    expected = sorted(os.listdir(ref_dir))
+    restart = [f for f in expected if f.startswith(("NETWORK_", "PARAMETERS_"))]
+    assert sorted(set(expected) - set(restart)) == sorted(_files(loops))
+    assert set(expected) <= set(os.listdir(tmp_path))
+    for fn in expected:
         assert _text(tmp_path / fn) == _text(os.path.join(ref_dir, fn)), fn
+    if name == "se_v30":
+        assert len(restart) == 4
 
 
 def _table(path):
