@@ -499,6 +499,12 @@ void launch_corrector_f(const NetConst& C, NetState* dS, cudaStream_t s) {
         k_corrector_f<false><<<C.N, 128, 0, s>>>(C, dS);
 }
 
+cudaError_t batched_resample(const NetConst& C, NetState* dS, double h_old, double hn, double delta_old,
+                             cudaStream_t s) {
+    if (C.N > 0) k_resample<float><<<C.N, 256, 0, s>>>(C, dS, h_old, hn, delta_old);
+    return cudaGetLastError();
+}
+
 cudaError_t batched_prepare(int tmax) {
     return cudaFuncSetAttribute(k_conv_sep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conv_sep_smem(tmax));
 }

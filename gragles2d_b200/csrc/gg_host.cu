@@ -43,6 +43,9 @@ struct gg_ctx {
     double h = 0, dt = 0, delta = 0, ds = 0;
     bool loaded = false, initialised = false;
     bool tangents = false;  // carry d phi / d p_k (plain form; set before distance initialisation)
+    double energy_delta_max = 0;  // grainhdl::m_Energy_deltaMAX (time-step bound of the driving forces)
+    int ngrains_ref = 0;          // grainhdl::ngrains: the grain count the coarsening trigger compares with
+    std::vector<std::pair<int, double>> dt_from;  // (first loop, dt) after every change of the time step
 
     std::vector<int32_t> ids;     // nn*nn
     std::vector<double> euler;    // 3 per grain
@@ -263,11 +266,203 @@ int set_loop(gg_ctx* c, int loop) {
     return GG_OK;
 }
 
+// grainhdl::gridCoarsement (src/grainhdl.cpp:1396-1478), checked at the start
+// of step `loop`: when the grains present have fallen below
+// GridCoarsementGradient of the count at the last coarsening, every grain's
+// field is resampled onto a grid of sqrt(count) x NumberOfPointsPerGrain
+// points, the grid constants and the time step are recomputed, IDLocal is
+// rebuilt by a comparison of the resampled fields and the contours are
+// extracted from them; the step then runs on the new grid.  Returns whether
+// the grid changed in *changed.
+int launch_stages(gg_ctx* c, int stages);
+void conv_tables(const gg_ctx* c, int tmax, const std::vector<int64_t>& gk_off, const std::vector<int64_t>& ck_off,
+                 std::vector<double>& gk, std::vector<float>& ck);
+
+int coarsen_if_due(gg_ctx* c, int loop, bool* changed) {
+    *changed = false;
+    const gg_params& P = c->P;
+    if (!P.grid_coarsement || loop == 0) return GG_OK;
+    int rc = refresh_state(c);
+    if (rc) return rc;
+    NetState& S = c->hS;
+    NetConst& C = c->C;
+    const int current = S.live;
+    if (!((double)current / (double)c->ngrains_ref < P.grid_coarsement_gradient)) return GG_OK;
+    const int N = c->N;
+    const int new_size = (int)(std::sqrt((double)current) * (double)c->ppg);
+    if (new_size < 1) return fail(c, GG_E_INVALID, "grid coarsening to an empty grid");
+    const int m_new = new_size + 2 * c->b;
+    const double h_old = c->h, hn = 1.0 / (double)new_size, delta_old = c->delta;
+    std::vector<Box> bcur(N + 1), bnew(N + 1, Box{0, 0, 0, 0});
+    std::vector<int32_t> state(N + 1), newbb(4 * (size_t)(N + 1), 0);
+    auto d2h = [&](void* dst, const void* src, size_t bytes) {
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream);
+    };
+    auto h2d = [&](void* dst, const void* src, size_t bytes) {
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream);
+    };
+    GG_CUDA(c, d2h(bcur.data(), S.box_cur, sizeof(Box) * (N + 1)));
+    GG_CUDA(c, d2h(state.data(), C.state, 4 * (N + 1)));
+    GG_CUDA(c, cudaStreamSynchronize(c->stream));
+    // LSbox::resizeGrid (src/box.cpp:1408-1436): the old box scaled by h / hn
+    // (kept unsquared as m_newXMin ..), the input box made square on the new grid
+    std::vector<int64_t> off(N + 1, 0), coff(N + 1, 0);
+    std::vector<int32_t> ccap(N + 1, 0);
+    int64_t a = 0, cc = 0;
+    for (int g = 1; g <= N; ++g) {
+        off[g] = a;
+        coff[g] = cc;
+        if (state[g] == G_GONE) continue;
+        const Box& o = bcur[g];
+        const int x0 = o.x0 * (h_old / hn) + 0.5, x1 = o.x1 * (h_old / hn) + 0.5;
+        const int y0 = o.y0 * (h_old / hn) + 0.5, y1 = o.y1 * (h_old / hn) + 0.5;
+        newbb[4 * (size_t)g] = x0;
+        newbb[4 * (size_t)g + 1] = x1;
+        newbb[4 * (size_t)g + 2] = y0;
+        newbb[4 * (size_t)g + 3] = y1;
+        bnew[g] = host_resize_to_square(Box{x0, x1, y0, y1}, m_new);
+        a += box_area(bnew[g]);
+        ccap[g] = contour_capacity(box_w(bnew[g]));
+        cc += ccap[g];
+    }
+    if (a > S.phi_cap || cc > S.cont_cap) return fail(c, GG_E_CAPACITY, "coarsened grid does not fit the arenas");
+    GG_CUDA(c, h2d(S.box_new, bnew.data(), sizeof(Box) * (N + 1)));
+    GG_CUDA(c, h2d(S.off_new, off.data(), sizeof(int64_t) * (N + 1)));
+    cudaError_t e = P.precision == GG_PRECISION_PLAIN ? plain_resample(C, c->dS, h_old, hn, delta_old, c->stream)
+                                                      : batched_resample(C, c->dS, h_old, hn, delta_old, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "resample");
+    // new grid constants and time step (src/grainhdl.cpp:1414-1451)
+    c->nn = new_size;
+    c->m = m_new;
+    c->delta = (unsigned long)P.domain_border_size * 1 / double(new_size);
+    c->h = 1.0 / new_size;
+    const unsigned long ppg_used =
+        P.decouple_grains == 1 ? (unsigned long)P.number_of_points_per_grain : (unsigned long)c->ppg;
+    c->dt = 0.8 / double(new_size * new_size) * ppg_used / 2 / 5.0;
+    double correction = 0.5 / new_size / c->energy_delta_max / c->dt;
+    if (correction > 1.0) correction = 1.0;
+    c->dt *= correction;
+    c->ngrains_ref = current;
+    c->dt_from.emplace_back(loop, c->dt);
+    C.m = c->m;
+    C.nn = c->nn;
+    C.h = c->h;
+    C.delta = c->delta;
+    C.dt = c->dt;
+    {
+        const int tmax = C.tmax;
+        std::vector<int64_t> gk_off(tmax + 1, 0), ck_off(tmax + 1, 0);
+        int64_t gkn = 0, ckn = 0;
+        for (int n = 1; n <= tmax; ++n) {
+            gk_off[n] = gkn;
+            gkn += (int64_t)(n / 2 + 1) * (n / 2 + 1);
+            ck_off[n] = ckn;
+            ckn += n + 1;
+        }
+        const bool plain = P.precision == GG_PRECISION_PLAIN;
+        std::vector<double> gk(plain ? gkn : 1);
+        std::vector<float> ck(plain ? 1 : ckn);
+        conv_tables(c, tmax, gk_off, ck_off, gk, ck);
+        if (plain)
+            GG_CUDA(c, h2d(const_cast<double*>(C.gk), gk.data(), sizeof(double) * gk.size()));
+        else
+            GG_CUDA(c, h2d(const_cast<float*>(C.ck), ck.data(), sizeof(float) * ck.size()));
+        GG_CUDA(c, cudaStreamSynchronize(c->stream));  // host tables leave scope
+    }
+    // LSbox::recalculateIDLocal (src/box.cpp:1487-1495): a comparison of the
+    // resampled fields (read where the convolution would be: phiB at the new
+    // offsets) into the new IDLocal; the old IDLocal stays in idPrev for the
+    // buffer-keeping resize
+    std::swap(S.box_cur, S.box_new);
+    std::swap(S.off_cur, S.off_new);
+    GG_CUDA(c, h2d(c->dS, &S, sizeof(NetState)));
+    e = P.precision == GG_PRECISION_PLAIN ? plain_stage_kernel(C, c->dS, 3, c->stream, c->cfg)
+                                          : batched_stage_kernel(C, c->dS, 3, c->stream, c->cfg);
+    if (e != cudaSuccess) return cuda_fail(c, e, "coarsening comparison");
+    // LSbox::extractContour (src/box.cpp:1089-1153) of the resampled fields
+    // (phiA), with the scaled boxes as m_newXMin .. (not the set comparison's)
+    GG_CUDA(c, h2d(C.newbb, newbb.data(), sizeof(int32_t) * newbb.size()));
+    std::swap(S.phiA, S.phiB);
+    GG_CUDA(c, h2d(c->dS, &S, sizeof(NetState)));
+    e = P.precision == GG_PRECISION_PLAIN ? plain_stage_kernel(C, c->dS, 4, c->stream, c->cfg)
+                                          : batched_stage_kernel(C, c->dS, 4, c->stream, c->cfg);
+    if (e != cudaSuccess) return cuda_fail(c, e, "coarsening contours");
+    // the contour extraction does not delete grains that had vanished before
+    for (int g = 1; g <= N; ++g)
+        if (state[g] == G_VANISHED) {
+            const int32_t vanished = G_VANISHED, none = -1;
+            GG_CUDA(c, h2d(C.state + g, &vanished, 4));
+            GG_CUDA(c, h2d(C.gone_loop + g, &none, 4));
+        }
+    // the step then starts from the resampled field (phiA, box_cur), the new
+    // IDLocal and contour as the previous ones, and fresh contour slots
+    std::swap(S.idPrev, S.idCur);
+    GG_CUDA(c, cudaMemcpyAsync(S.box_prev, S.box_cur, sizeof(Box) * (N + 1), cudaMemcpyDeviceToDevice, c->stream));
+    GG_CUDA(c, cudaMemcpyAsync(S.off_prev, S.off_cur, sizeof(int64_t) * (N + 1), cudaMemcpyDeviceToDevice, c->stream));
+    std::swap(S.contPrev, S.contCur);
+    std::swap(S.coff_prev, S.coff_cur);
+    std::swap(S.ccap_prev, S.ccap_cur);
+    std::swap(S.cn_prev, S.cn_cur);
+    std::swap(S.jPrev, S.jCur);
+    std::swap(S.jn_prev, S.jn_cur);
+    GG_CUDA(c, h2d(S.coff_cur, coff.data(), sizeof(int64_t) * (N + 1)));
+    GG_CUDA(c, h2d(S.ccap_cur, ccap.data(), sizeof(int32_t) * (N + 1)));
+    GG_CUDA(c, h2d(c->dS, &S, sizeof(NetState)));
+    GG_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (c->graph) {  // the captured step holds the old constants
+        cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+    }
+    *changed = true;
+    return check_status(c);
+}
+
 int launch_stages(gg_ctx* c, int stages) {
     cudaError_t e = c->P.precision == GG_PRECISION_PLAIN ? plain_stages(c->C, c->dS, stages, c->stream, c->cfg)
                                                          : batched_stages(c->C, c->dS, stages, c->stream, c->cfg);
     if (e != cudaSuccess) return cuda_fail(c, e, "stage launch");
     return GG_OK;
+}
+
+// Gaussian multipliers (plain form) or separable real-space kernels with their
+// band radius (batched form) of every box edge up to tmax, for the context's
+// current dt and grid size (both change when the grid is coarsened).
+void conv_tables(const gg_ctx* c, int tmax, const std::vector<int64_t>& gk_off, const std::vector<int64_t>& ck_off,
+                 std::vector<double>& gk, std::vector<float>& ck) {
+    if (c->P.precision == GG_PRECISION_PLAIN) {
+        for (int n = 1; n <= tmax; ++n) {
+            const int half = n / 2 + 1;
+            for (int i2 = 0; i2 < half; ++i2)
+                for (int j2 = 0; j2 < half; ++j2)
+                    gk[gk_off[n] + i2 * half + j2] = gaussian_multiplier(n, i2, j2, c->dt, c->nn);
+        }
+        return;
+    }
+        // k_n[r] = (1/n) sum_f g(min(f, n-f)) cos(2 pi f r / n), g(f) = exp(-kappa f^2),
+        // kappa = sqrt(2/pi) 4 dt nn^2 / n^2 pi^2 (the 1/n^2 of G split over both axes)
+        std::vector<double> gf;
+        for (int n = 1; n <= tmax; ++n) {
+            const double kappa = sqrt(2 / kPiH) * 4.0 * c->dt * (double)c->nn * (double)c->nn / ((double)n * n) *
+                                 kPiH * kPiH;
+            gf.assign(n, 0.0);
+            for (int f = 0; f < n; ++f) {
+                const int f2 = std::min(f, n - f);
+                gf[f] = exp(-kappa * (double)f2 * f2);
+            }
+            for (int r = 0; r < n; ++r) {
+                double acc = 0;
+                for (int f = 0; f < n; ++f) acc += gf[f] * cos(2.0 * kPiH * (double)((int64_t)f * r % n) / n);
+                ck[ck_off[n] + r] = (float)(acc / n);
+            }
+            // band radius: every entry at circular distance > R is below 2^-26 k_n[0]
+            // (under half an FP32 ulp of the centre tap; the dropped tail is the
+            // flat aliasing floor of the truncated Gaussian, ~7e-9 k_n[0])
+            int R = 0;
+            const double tiny = std::ldexp(std::fabs((double)ck[ck_off[n]]), -26);
+            for (int r = 1; r < n; ++r)
+                if (std::fabs((double)ck[ck_off[n] + r]) > tiny) R = std::max(R, std::min(r, n - r));
+            ck[ck_off[n] + n] = (float)R;
+        }
 }
 
 }  // namespace
@@ -409,7 +604,8 @@ int gg_create(const gg_params* p, int device, gg_ctx** out) {
     if (p->convolution_mode != 2) return bad("only ConvolutionMode 2 (Gaussian) is supported");
     if (p->lattice_type != 0) return bad("only LatticeType 0 (cubic) is supported");
     if (p->research_mode != 0) return bad("only ResearchMode 0 is supported");
-    if (p->grid_coarsement != 0) return bad("GridCoarsement must be 0");
+    if (p->grid_coarsement < 0 || p->grid_coarsement > 1) return bad("GridCoarsement must be 0 or 1");
+    if (p->grid_coarsement && p->decouple_grains == 1) return bad("GridCoarsement with DecoupleGrains is not supported");
     if (p->use_magnetic_field < 0 || p->use_magnetic_field > 1) return bad("UseMagneticField must be 0 or 1");
     if (p->use_stored_elastic_energy < 0 || p->use_stored_elastic_energy > 1)
         return bad("UseStoredElasticEnergy must be 0 or 1");
@@ -612,6 +808,8 @@ int gg_distance_initialisation(gg_ctx* c) {
         energy_delta_max = hi - lo;
         correct_dt = true;
     }
+    c->energy_delta_max = energy_delta_max;
+    c->ngrains_ref = c->N;
     if (correct_dt) {
         const double vmax = energy_delta_max * c->dt;
         double correction = 0.5 / (vmax / c->h);
@@ -735,41 +933,10 @@ int gg_distance_initialisation(gg_ctx* c) {
     const bool plain = P.precision == GG_PRECISION_PLAIN;
     std::vector<double> tw(plain ? 2 * twn : 2), gk(plain ? gkn : 1);
     std::vector<float> ck(plain ? 1 : ckn);
-    if (plain) {
-        for (int n = 1; n <= tmax; ++n) {
+    if (plain)
+        for (int n = 1; n <= tmax; ++n)
             for (int k = 0; k < n; ++k) twiddle(n, k, &tw[2 * (tw_off[n] + k)], &tw[2 * (tw_off[n] + k) + 1]);
-            const int half = n / 2 + 1;
-            for (int i2 = 0; i2 < half; ++i2)
-                for (int j2 = 0; j2 < half; ++j2)
-                    gk[gk_off[n] + i2 * half + j2] = gaussian_multiplier(n, i2, j2, c->dt, c->nn);
-        }
-    } else {
-        // k_n[r] = (1/n) sum_f g(min(f, n-f)) cos(2 pi f r / n), g(f) = exp(-kappa f^2),
-        // kappa = sqrt(2/pi) 4 dt nn^2 / n^2 pi^2 (the 1/n^2 of G split over both axes)
-        std::vector<double> gf;
-        for (int n = 1; n <= tmax; ++n) {
-            const double kappa = sqrt(2 / kPiH) * 4.0 * c->dt * (double)c->nn * (double)c->nn / ((double)n * n) *
-                                 kPiH * kPiH;
-            gf.assign(n, 0.0);
-            for (int f = 0; f < n; ++f) {
-                const int f2 = std::min(f, n - f);
-                gf[f] = exp(-kappa * (double)f2 * f2);
-            }
-            for (int r = 0; r < n; ++r) {
-                double acc = 0;
-                for (int f = 0; f < n; ++f) acc += gf[f] * cos(2.0 * kPiH * (double)((int64_t)f * r % n) / n);
-                ck[ck_off[n] + r] = (float)(acc / n);
-            }
-            // band radius: every entry at circular distance > R is below 2^-26 k_n[0]
-            // (under half an FP32 ulp of the centre tap; the dropped tail is the
-            // flat aliasing floor of the truncated Gaussian, ~7e-9 k_n[0])
-            int R = 0;
-            const double tiny = std::ldexp(std::fabs((double)ck[ck_off[n]]), -26);
-            for (int r = 1; r < n; ++r)
-                if (std::fabs((double)ck[ck_off[n] + r]) > tiny) R = std::max(R, std::min(r, n - r));
-            ck[ck_off[n] + n] = (float)R;
-        }
-    }
+    conv_tables(c, tmax, gk_off, ck_off, gk, ck);
     double* d_tw;
     double* d_gk;
     float* d_ck;
@@ -910,6 +1077,7 @@ int gg_distance_initialisation(gg_ctx* c) {
     rc = check_status(c);
     if (rc != GG_OK) return rc;
     c->initialised = true;
+    c->dt_from.assign(1, std::make_pair((int)P.start_time, c->dt));
     return refresh_state(c);
 }
 
@@ -969,7 +1137,14 @@ int run_stage(gg_ctx* c, int stages, bool setloop, int loop) {
 }
 }  // namespace
 
-int gg_convolution(gg_ctx* c, int32_t loop) { return run_stage(c, ST_CONV, true, loop); }
+int gg_convolution(gg_ctx* c, int32_t loop) {
+    if (!c) return GG_E_INVALID;
+    if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
+    bool coarsened = false;
+    const int rc = coarsen_if_due(c, loop, &coarsened);  // the first stage of a loop (src/grainhdl.cpp:1053)
+    if (rc) return rc;
+    return run_stage(c, ST_CONV, true, loop);
+}
 int gg_update_second_order_neighbors(gg_ctx* c) { return run_stage(c, ST_SECOND, false, 0); }
 int gg_comparison(gg_ctx* c) { return run_stage(c, ST_COMPARE, false, 0); }
 int gg_level_set(gg_ctx* c, int32_t loop) { return run_stage(c, ST_LEVELSET, true, loop); }
@@ -989,7 +1164,21 @@ int gg_step(gg_ctx* c, int32_t loop, int32_t nsteps) {
     if (!c) return GG_E_INVALID;
     if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
     if (nsteps <= 0) return GG_OK;
-    int rc = set_loop(c, loop);
+    if (c->P.grid_coarsement && nsteps > 1) {
+        // the coarsening test needs the grain count between steps
+        double total = 0;
+        for (int s = 0; s < nsteps; ++s) {
+            const int rs = gg_step(c, loop + s, 1);
+            if (rs) return rs;
+            total += c->last_ms;
+        }
+        c->last_ms = total;
+        return GG_OK;
+    }
+    bool coarsened = false;
+    int rc = coarsen_if_due(c, loop, &coarsened);
+    if (rc) return rc;
+    rc = set_loop(c, loop);
     if (rc) return rc;
     if (c->P.precision == GG_PRECISION_BATCHED) {
         if (!c->graph) {
@@ -1103,6 +1292,7 @@ int gg_tangent_enable(gg_ctx* c, int32_t enable) {
         return fail(c, GG_E_INVALID, "tangents need the plain (FP64) form");
     if (enable && (c->P.use_stored_elastic_energy || c->P.use_magnetic_field))
         return fail(c, GG_E_INVALID, "tangents do not cover the stored-energy or magnetic driving force");
+    if (enable && c->P.grid_coarsement) return fail(c, GG_E_INVALID, "tangents do not cover grid coarsening");
     c->tangents = enable != 0;
     return GG_OK;
 }
@@ -1214,10 +1404,15 @@ int gg_write_analysis(gg_ctx* c, const char* directory, int32_t loop) {
     // set deletes them), total energy, grid size
     int nr = 0;
     for (int g = 1; g <= N; ++g) nr += (state[g] != G_GONE || gone[g] == loop) ? 1 : 0;
-    const double inc = (c->dt * (c->P.physical_domain_size * c->P.physical_domain_size) /
-                        (c->P.time_slope * c->P.hagb_energy * c->P.hagb_mobility));
+    // each step adds the increment of its own time step (which a coarsening changes)
     double realtime = 0.0;
-    for (int l = c->P.start_time; l < loop; ++l) realtime += inc;
+    for (int l = c->P.start_time; l < loop; ++l) {
+        double dt = c->dt_from.front().second;
+        for (const auto& seg : c->dt_from)
+            if (seg.first <= l) dt = seg.second;
+        realtime += (dt * (c->P.physical_domain_size * c->P.physical_domain_size) /
+                     (c->P.time_slope * c->P.hagb_energy * c->P.hagb_mobility));
+    }
     std::ofstream st(stats_path, loop == 0 ? std::ios::out : std::ios::app);
     if (!st) return fail(c, GG_E_IO, "cannot write " + stats_path);
     st << realtime << "\t" << nr << "\t" << 0.5 * total_energy << "\t" << c->nn << std::endl;
@@ -1311,8 +1506,9 @@ int gg_write_restart(gg_ctx* c, const char* directory, int32_t loop) {
     tag("ConvolutionMode", P.convolution_mode);
     tag("ResearchMode", flag(P.research_mode));
     tag("ResearchProject", P.research_project);
-    tag("ConstantSectorRadius", P.constant_sector_radius * c->h);  // scaled at set-up (src/grainhdl.cpp:130-131)
-    tag("InterpolatingSectorRadius", P.interpolating_sector_radius * c->h);
+    // scaled by h at set-up (src/grainhdl.cpp:130-131), not again when the grid is coarsened
+    tag("ConstantSectorRadius", c->C.csr);
+    tag("InterpolatingSectorRadius", c->C.isr);
     tag("NeighbourTracking", P.neighbour_tracking);
     tag("UseStoredElasticEnergy", flag(P.use_stored_elastic_energy));
     tag("GrainScheduler", P.grain_scheduler);

@@ -731,6 +731,42 @@ __global__ void __launch_bounds__(256) k_redistance(NetConst C, NetState* S) {
     redistance_grain<R>(in, S->box_cur[g], out, S->box_new[g], (R)C.h, (R)C.delta);
 }
 
+// LSbox::resizeGrid (src/box.cpp:1408-1485) of one grain (not removed) per
+// block: its distance function on the coarser grid, by bilinear
+// interpolation of the old field (box_cur / off_cur of phiA) at the new grid's
+// points, into box_new / off_new of phiB (boxes laid out by the host).  A
+// point whose interpolation cell reaches the old box's last two rows or
+// columns, or lies before its first, takes -delta_old.  The arithmetic is the
+// reference's, term for term.
+template <typename R>
+__global__ void __launch_bounds__(256) k_resample(NetConst C, NetState* S, double h_old, double hn, double delta_old) {
+    const int g = blockIdx.x + 1;
+    if (g > C.N || C.state[g] == G_GONE) return;
+    const Box ob = S->box_cur[g];
+    const Box nb = S->box_new[g];
+    const R* src = phiA_of<R>(S) + S->off_cur[g];
+    R* dst = phiB_of<R>(S) + S->off_new[g];
+    const int ow = ob.x1 - ob.x0, nw = nb.x1 - nb.x0;
+    if (nw <= 0 || nb.y1 <= nb.y0) return;
+    const int64_t cnt = (int64_t)nw * (nb.y1 - nb.y0);
+    for (int64_t p = threadIdx.x; p < cnt; p += blockDim.x) {
+        const int i = nb.y0 + (int)(p / nw), j = nb.x0 + (int)(p % nw);
+        const double pointx = j * (hn / h_old);
+        const double pointy = i * (hn / h_old);
+        const double xl = (int)pointx, xr = (int)(pointx + 1), yo = (int)(pointy + 1), yu = (int)pointy;
+        if (xr > ob.x1 - 2 || yo > ob.y1 - 2 || yu < ob.y0 || xl < ob.x0) {
+            dst[p] = (R)(-delta_old);
+            continue;
+        }
+        auto at = [&](double row, double col) {
+            return (double)src[(int64_t)((int)row - ob.y0) * ow + ((int)col - ob.x0)];
+        };
+        const double ro = 1 / (xr - xl) * ((xr - pointx) * at(yo, xl) + (pointx - xl) * at(yo, xr));
+        const double ru = 1 / (xr - xl) * ((xr - pointx) * at(yu, xl) + (pointx - xl) * at(yu, xr));
+        dst[p] = (R)(1 / (yo - yu) * ((yo - pointy) * ru + (pointy - yu) * ro));
+    }
+}
+
 // ---------------------------------------------------------------------------
 // End of step: grainhdl::get_biggestGrainVol (src/grainhdl.cpp:1744-1754) and
 // the buffer switches; rotates per-step roles in NetState.

@@ -40,6 +40,11 @@ size_t conv_sep_smem(int tmax);
 cudaError_t batched_prepare(int tmax);
 cudaError_t batched_init(const NetConst& C, NetState* dS, const int32_t* d_ids, cudaStream_t s);
 cudaError_t finalize_only(const NetConst& C, NetState* dS, int rotate, cudaStream_t s);
+// Grid coarsening: every grain's field resampled onto the coarser grid.
+cudaError_t plain_resample(const NetConst& C, NetState* dS, double h_old, double hn, double delta_old,
+                           cudaStream_t s);
+cudaError_t batched_resample(const NetConst& C, NetState* dS, double h_old, double hn, double delta_old,
+                             cudaStream_t s);
 cudaError_t swap_phi(NetState* dS, cudaStream_t s);
 cudaError_t find_neighbors_launch(const NetConst& C, NetState* dS, cudaStream_t s);
 cudaError_t traffic_launch(const NetConst& C, NetState* dS, cudaStream_t s);

@@ -23,6 +23,12 @@ cudaError_t swap_phi(NetState* dS, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+cudaError_t plain_resample(const NetConst& C, NetState* dS, double h_old, double hn, double delta_old,
+                           cudaStream_t s) {
+    if (C.N > 0) k_resample<double><<<C.N, 256, 0, s>>>(C, dS, h_old, hn, delta_old);
+    return cudaGetLastError();
+}
+
 cudaError_t finalize_only(const NetConst& C, NetState* dS, int rotate, cudaStream_t s) {
     k_finalize<<<1, 1024, 0, s>>>(C, dS, rotate);
     return cudaGetLastError();

@@ -86,7 +86,7 @@ typedef struct gg_params {
     int32_t research_mode;            /* ResearchMode (0 supported) */
     int32_t research_project;         /* ResearchProject */
     int32_t decouple_grains;          /* DecoupleGrains */
-    int32_t grid_coarsement;          /* GridCoarsement (0 supported) */
+    int32_t grid_coarsement;          /* GridCoarsement (0, 1: gg_step and gg_convolution coarsen the grid when due) */
     int32_t use_stored_elastic_energy;/* UseStoredElasticEnergy (0, 1) */
     int32_t use_magnetic_field;       /* UseMagneticField (0, 1; parameters from the MagneticParams file) */
     int32_t discrete_sampling_rate;   /* DiscreteSamplingRate (bins of the MODF output) */
@@ -117,7 +117,7 @@ typedef struct gg_params {
     double magnetic_vector[3];        /* MagneticVector_x, _y, _z (unit field direction) */
     double delta_mag_sys;             /* deltaMagSys (susceptibility difference) */
     double magnetic_force_field;      /* MagneticForceField */
-    double grid_coarsement_gradient;  /* GridCoarsementGradient (written back only) */
+    double grid_coarsement_gradient;  /* GridCoarsementGradient */
     double reserved_d[1];
     char read_from_filename[512];     /* ReadFromFilename (.bin ID field) */
     char additional_filename[512];    /* AdditionalFilename (.uds header) */

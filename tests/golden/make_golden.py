@@ -47,6 +47,11 @@ CASES = {
     "se_v30": ("voronoi", 30, 120, 6, 20, 5,
                {"IsIsotropicNetwork": 0, "UseStoredElasticEnergy": 1, "DislocEnPerM": 1.0,
                 "BoxDefaultStoredElasticEnergy": 500.0, "AnalysisTimestep": 5}),
+    # grid coarsening: every time the grain count falls below 0.99 of the
+    # count at the last coarsening the grid shrinks (first at loop 12: 100 -> 97)
+    "gc_v80": ("voronoi", 80, 100, 11, 24, 4,
+               {"IsIsotropicNetwork": 1, "GridCoarsement": 1, "GridCoarsementGradient": 0.99,
+                "AnalysisTimestep": 4}),
     # magnetic driving force: field direction (0.6, 0, 0.8), 1/2 mu0 dchi B^2 = 800,
     # read from magnetic.xml beside the parameters; analysis files every 5 steps
     "mag_v30": ("voronoi", 30, 120, 7, 20, 5,

@@ -2,7 +2,9 @@
 files GraGLeS2D itself wrote in the same run: Texture_<loop>.ori,
 MODF_<loop>.txt and NrGrains&EnergyStatistics.txt on the reference's schedule
 (every AnalysisTimestep steps and after the last), and where the fixture has
-them (se_v30) the restart files written after step 0 and after the last step.  The plain FP64 form must write
+them (se_v30, gc_v80) the restart files written after step 0 and after the last
+step; gc_v80 coarsens its grid twice in between, so its simulated time adds
+increments of three different time steps.  The plain FP64 form must write
 the same bytes; the batched FP32 form the same grains and counts with areas,
 energies and MODF values within FP32 tolerances.
 """
@@ -16,7 +18,7 @@ from gragles2d_b200 import gg
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["ana_iso_v80", "ana_mob_v80", "se_v30", "mag_v30"]
+CASES = ["ana_iso_v80", "ana_mob_v80", "se_v30", "mag_v30", "gc_v80"]
 
 
 def _run(golden_dir, name, precision, out, run_sim=False):
@@ -61,7 +63,7 @@ def _text(path):
 
 
 @pytest.mark.parametrize("name,run_sim", [(CASES[0], False), (CASES[1], False), (CASES[2], False), (CASES[3], False),
-                                          (CASES[0], True)])
+                                          (CASES[4], False), (CASES[0], True)])
 def test_plain_form_writes_the_reference_files(golden_dir, name, run_sim, tmp_path):
     d, info, loops = _run(golden_dir, name, gg.PRECISION_PLAIN, tmp_path, run_sim)
     ref_dir = os.path.join(d, "analysis")
@@ -71,7 +73,7 @@ def test_plain_form_writes_the_reference_files(golden_dir, name, run_sim, tmp_pa
     assert set(expected) <= set(os.listdir(tmp_path))
     for fn in expected:
         assert _text(tmp_path / fn) == _text(os.path.join(ref_dir, fn)), fn
-    if name == "se_v30":
+    if name in ("se_v30", "gc_v80"):
         assert len(restart) == 4
 
 

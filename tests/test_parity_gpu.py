@@ -19,7 +19,7 @@ from gragles2d_b200 import dumpfile
 from tests.parity import compare_records, ownership_mismatch
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
-ISO = ["iso_v20", "iso_v60"]
+ISO = ["iso_v20", "iso_v60", "gc_v80"]
 ANISO = ["rs_v30", "mob_v30", "se_v30", "mag_v30"]
 
 
@@ -89,7 +89,7 @@ def _areas(h):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["iso_v60", "rs_v30", "mob_v30", "se_v30", "mag_v30"])
+@pytest.mark.parametrize("case", ["iso_v60", "rs_v30", "mob_v30", "se_v30", "mag_v30", "gc_v80"])
 def test_batched_fp32_area_error_vs_plain(case):
     """The batched FP32 form (graph-captured steps) against the plain FP64
     form from the same initial state: per-grain relative area error <= 1e-3
@@ -140,5 +140,34 @@ def test_driving_force_time_step_and_tangent_guard(case):
         h.distanceInitialisation()
         assert h.dims().dt == ref.dt
         assert ref.dt < 0.8 / 120**2 * 21 / 2 / 5.0 / 10  # shortened well below the uncorrected step
+    finally:
+        h.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1])
+def test_grid_coarsening_shrinks_the_grid(precision):
+    """GridCoarsement: the gc_v80 run coarsens at the starts of loops 12
+    (100 -> 97 points: 79 of 80 grains left, below 0.99), 13 (78 of 79:
+    97 -> 97) and 22 (77 of 78: 97 -> 96), as the reference's run does; the
+    time step follows the grid (NumberOfPointsPerGrain 11)."""
+    from gragles2d_b200 import gg
+
+    d = os.path.join(GOLDEN, "gc_v80")
+    ref = dumpfile.read(os.path.join(d, "reference.dump.gz"))
+    h = gg.GrainHandler(gg.Settings(os.path.join(d, "gc_v80.xml"), precision=precision))
+    try:
+        h.load_voxel_files()
+        h.distanceInitialisation()
+        h.set_neighbours({gid: g.sec for gid, g in ref.records[0].grains.items() if g.state})
+        sizes = []
+        for _ in range(25):
+            h.step(1)
+            sizes.append(h.dims().ngridpoints)
+        assert sizes[:12] == [114] * 12
+        assert sizes[12:22] == [111] * 10
+        assert sizes[22:] == [110] * 3
+        assert h.dims().dt == 0.8 / (96 * 96) * 11 / 2 / 5.0
+        assert h.status() == 0
     finally:
         h.close()
