@@ -420,17 +420,30 @@ __global__ void __launch_bounds__(128, 8) k_corrector_f(NetConst C, NetState* S)
             se = (float)f;
         }
         if (inside && !valid) out[k] = -delta - se;
-        if (__ballot_sync(0xffffffffu, valid) == 0u) continue;
+        // A pixel whose field and convolved value lie on the same side beyond
+        // 0.3 delta (2.1 cells) keeps that side for every weight up to 2 (the
+        // result lies between val and 2 conv - val, and |val| <= delta), and
+        // it is not next to a sign change of these near-distance fields; only
+        // signs and the values next to sign changes reach the comparison's
+        // zero crossings and the redistancing that replaces the field.  It
+        // takes weight 1 (the convolved value) without the projection.  (On
+        // the 20,000-grain workload the areas stay bit-identical for 10 steps
+        // and within 1.3e-7 relative, in a few dozen grains, after 40.)
+        const float far_level = 0.3f * delta;
+        const bool far = valid && ((val >= far_level && conv >= far_level) || (val <= -far_level && conv <= -far_level));
+        if (far) out[k] = conv - se;
+        const bool need = valid && !far;
+        if (__ballot_sync(0xffffffffu, need) == 0u) continue;
         float lambda = 0.f;
         int segment;
         if (staged) {
-            segment = project_warp(sp, cbb, size, j, i, valid, &lambda, &wseed);
+            segment = project_warp(sp, cbb, size, j, i, need, &lambda, &wseed);
         } else {
             double dl = 0;
             segment = project_to_boundary(P, size, (double)j, (double)i, &dl);
             lambda = (float)dl;
         }
-        if (!valid) continue;
+        if (!need) continue;
         int sid = -1;
         float interpolator = 0.f;
         if (tabled) {
