@@ -991,7 +991,7 @@ constexpr int kRedistSmemBytes = 24 * 1024;
 // out[(i - bo.y0) * so + (j - bo.x0)].  One thread per column (y sweeps) or
 // row (x sweeps), carrying the running value in a register.
 template <typename R>
-__device__ void redistance_sweeps(const R* __restrict__ in, int in_x0, int in_y0, int si, const Box bi,
+__device__ void redistance_sweeps_indexed(const R* __restrict__ in, int in_x0, int in_y0, int si, const Box bi,
                                   R* __restrict__ out, int so, const Box bo, R h) {
     const int ixmin = (bi.x0 < bo.x0) ? bo.x0 : bi.x0;
     const int iymin = (bi.y0 < bo.y0) ? bo.y0 : bi.y0;
@@ -1124,6 +1124,217 @@ __device__ void redistance_sweeps(const R* __restrict__ in, int in_x0, int in_y0
 #undef GG_IN
 #undef GG_OUT
     __syncthreads();
+}
+
+// The four directional sweeps of LSbox::executeRedistancing
+// (src/box.cpp:1259-1399) over the new box bo.  The input is read through
+// IN(i, j) = in[(i - in_y0) * si + (j - in_x0)] and is only touched inside
+// the intersection of bi and bo; the output through OUT(i, j) =
+// out[(i - bo.y0) * so + (j - bo.x0)].  One thread per column (y sweeps) or
+// row (x sweeps), carrying the running value in a register.
+template <typename R>
+__device__ void redistance_sweeps_walk(const R* __restrict__ in, int in_x0, int in_y0, int si, const Box bi,
+                                  R* __restrict__ out, int so, const Box bo, R h) {
+    const int ixmin = (bi.x0 < bo.x0) ? bo.x0 : bi.x0;
+    const int iymin = (bi.y0 < bo.y0) ? bo.y0 : bi.y0;
+    const int ixmax = (bi.x1 < bo.x1) ? bi.x1 : bo.x1;
+    const int iymax = (bi.y1 < bo.y1) ? bi.y1 : bo.y1;
+    // Each recurrence carries its running value in a register and walks the
+    // output (and, inside the intersection, the input) with a pointer; the
+    // loads of the next step (which no store of the current step touches) are
+    // issued one step ahead so their latency overlaps the current step.  Each
+    // sweep is split where the input's region ends, so the loop bodies carry
+    // no per-step region test.
+    // y sweeps: one thread per column, stride so / si between steps
+    for (int j = ixmin + (int)threadIdx.x; j < bo.x1; j += blockDim.x) {
+        const bool col_in = j < ixmax;
+        R* const ocol = out + (j - bo.x0);
+        const R* const icol = in + (j - in_x0);
+        if (iymin < bo.y1 - 1) {  // y forward
+            const int a_end = col_in ? min(iymax - 1, bo.y1 - 1) : iymin;  // steps that see the input
+            R* po = ocol + (iymin - bo.y0) * so;
+            const R* pi = icol + (iymin - in_y0) * si;
+            R cur = po[0];
+            R nxt = po[so];
+            int i = iymin;
+            if (i < a_end) {
+                R a = pi[0], c = pi[si];
+                for (; i < a_end; i++) {
+                    const R nxt_n = i + 2 < bo.y1 ? po[2 * so] : (R)0;
+                    const R c_n = i + 1 < iymax - 1 ? pi[2 * si] : (R)0;
+                    if (a * c <= (R)0.0) {
+                        const R slope = (c - a) / h;
+                        const R dz = -a / slope;
+                        if (fabs(cur) > fabs(dz)) {
+                            cur = -dz * (R)sgn(slope);
+                            po[0] = cur;
+                        }
+                    }
+                    const R cand = cur + ((R)sgn(c) * h);
+                    if (fabs(cand) < fabs(nxt)) {
+                        nxt = cand;
+                        po[so] = nxt;
+                    }
+                    cur = nxt;
+                    nxt = nxt_n;
+                    a = c;
+                    c = c_n;
+                    po += so;
+                    pi += si;
+                }
+            }
+            for (; i < bo.y1 - 1; i++) {
+                const R nxt_n = i + 2 < bo.y1 ? po[2 * so] : (R)0;
+                const R cand = cur + ((R)sgn(nxt) * h);
+                if (fabs(cand) < fabs(nxt)) {
+                    nxt = cand;
+                    po[so] = nxt;
+                }
+                cur = nxt;
+                nxt = nxt_n;
+                po += so;
+            }
+        }
+        if (iymax - 1 > bo.y0) {  // y backward
+            const int a_end = col_in ? iymin : iymax - 1;  // steps i > a_end see the input
+            R* po = ocol + (iymax - 1 - bo.y0) * so;
+            R cur = po[0];
+            R prv = po[-so];
+            int i = iymax - 1;
+            if (i > a_end) {
+                const R* pi = icol + (iymax - 2 - in_y0) * si;  // IN(i - 1)
+                R ip = pi[0];
+                for (; i > a_end; i--) {
+                    const R prv_n = i - 2 >= bo.y0 ? po[-2 * so] : (R)0;
+                    const R ip_n = i - 1 > iymin ? pi[-si] : (R)0;
+                    const R cand = cur + ((R)sgn(ip) * h);
+                    if (fabs(cand) < fabs(prv)) {
+                        prv = cand;
+                        po[-so] = prv;
+                    }
+                    cur = prv;
+                    prv = prv_n;
+                    ip = ip_n;
+                    po -= so;
+                    pi -= si;
+                }
+            }
+            for (; i > bo.y0; i--) {
+                const R prv_n = i - 2 >= bo.y0 ? po[-2 * so] : (R)0;
+                const R cand = cur + ((R)sgn(prv) * h);
+                if (fabs(cand) < fabs(prv)) {
+                    prv = cand;
+                    po[-so] = prv;
+                }
+                cur = prv;
+                prv = prv_n;
+                po -= so;
+            }
+        }
+    }
+    __syncthreads();
+    // x sweeps: one thread per row, unit stride between steps
+    for (int i = iymin + (int)threadIdx.x; i < bo.y1; i += blockDim.x) {
+        const bool row_in = i < iymax;
+        R* const orow = out + (int64_t)(i - bo.y0) * so;
+        const R* const irow = in + (int64_t)(i - in_y0) * si;
+        if (ixmin < bo.x1 - 1) {  // x forward
+            const int a_end = row_in ? min(ixmax - 1, bo.x1 - 1) : ixmin;
+            R* po = orow + (ixmin - bo.x0);
+            const R* pi = irow + (ixmin - in_x0);
+            R cur = po[0];
+            R nxt = po[1];
+            int j = ixmin;
+            if (j < a_end) {
+                R a = pi[0], c = pi[1];
+                for (; j < a_end; j++) {
+                    const R nxt_n = j + 2 < bo.x1 ? po[2] : (R)0;
+                    const R c_n = j + 1 < ixmax - 1 ? pi[2] : (R)0;
+                    if (a * c <= (R)0.0) {
+                        const R slope = (c - a) / h;
+                        const R dz = -a / slope;
+                        if (fabs(cur) > fabs(dz)) {
+                            cur = -dz * (R)sgn(slope);
+                            po[0] = cur;
+                        }
+                    }
+                    const R cand = cur + ((R)sgn(c) * h);
+                    if (fabs(cand) < fabs(nxt)) {
+                        nxt = cand;
+                        po[1] = nxt;
+                    }
+                    cur = nxt;
+                    nxt = nxt_n;
+                    a = c;
+                    c = c_n;
+                    ++po;
+                    ++pi;
+                }
+            }
+            for (; j < bo.x1 - 1; j++) {
+                const R nxt_n = j + 2 < bo.x1 ? po[2] : (R)0;
+                const R cand = cur + ((R)sgn(nxt) * h);
+                if (fabs(cand) < fabs(nxt)) {
+                    nxt = cand;
+                    po[1] = nxt;
+                }
+                cur = nxt;
+                nxt = nxt_n;
+                ++po;
+            }
+        }
+        if (ixmax - 1 > bo.x0) {  // x backward
+            const int a_end = row_in ? ixmin : ixmax - 1;
+            R* po = orow + (ixmax - 1 - bo.x0);
+            R cur = po[0];
+            R prv = po[-1];
+            int j = ixmax - 1;
+            if (j > a_end) {
+                const R* pi = irow + (ixmax - 2 - in_x0);  // IN(i, j - 1)
+                R ip = pi[0];
+                for (; j > a_end; j--) {
+                    const R prv_n = j - 2 >= bo.x0 ? po[-2] : (R)0;
+                    const R ip_n = j - 1 > ixmin ? pi[-1] : (R)0;
+                    const R cand = cur + ((R)sgn(ip) * h);
+                    if (fabs(cand) < fabs(prv)) {
+                        prv = cand;
+                        po[-1] = prv;
+                    }
+                    cur = prv;
+                    prv = prv_n;
+                    ip = ip_n;
+                    --po;
+                    --pi;
+                }
+            }
+            for (; j > bo.x0; j--) {
+                const R prv_n = j - 2 >= bo.x0 ? po[-2] : (R)0;
+                const R cand = cur + (R)sgn(prv) * h;
+                if (fabs(cand) < fabs(prv)) {
+                    prv = cand;
+                    po[-1] = prv;
+                }
+                cur = prv;
+                prv = prv_n;
+                --po;
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// The FP32 (batched) form walks pointers with each sweep split where the
+// input's region ends (fewer instructions: 0.75 -> 0.68 ms on the 20,000-grain
+// workload); the FP64 (plain) form keeps indexed accesses with per-step region
+// tests, which the compiler schedules better for doubles (1.75 ms against
+// 2.33 ms).  Both evaluate the same expressions in the same order.
+template <typename R>
+__device__ __forceinline__ void redistance_sweeps(const R* __restrict__ in, int in_x0, int in_y0, int si, const Box bi,
+                                                  R* __restrict__ out, int so, const Box bo, R h) {
+    if constexpr (sizeof(R) == 4)
+        redistance_sweeps_walk<R>(in, in_x0, in_y0, si, bi, out, so, bo, h);
+    else
+        redistance_sweeps_indexed<R>(in, in_x0, in_y0, si, bi, out, so, bo, h);
 }
 
 // LSbox::executeRedistancing, one CTA of 64 threads per grain.  When both
