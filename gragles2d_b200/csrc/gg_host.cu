@@ -11,6 +11,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <mutex>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -47,7 +48,7 @@ struct gg_ctx {
     int ngrains_ref = 0;          // grainhdl::ngrains: the grain count the coarsening trigger compares with
     std::vector<std::pair<int, double>> dt_from;  // (first loop, dt) after every change of the time step
 
-    std::vector<int32_t> ids;     // nn*nn
+    size_t d_ids_count = 0;       // elements of d_ids
     std::vector<double> euler;    // 3 per grain
     std::vector<int32_t> bbox;    // 5 per grain
     std::vector<double> stored;   // .uds stored energy per grain (empty: none given)
@@ -57,7 +58,7 @@ struct gg_ctx {
     NetConst C{};
     NetState hS{};               // host copy of the device NetState (pointers)
     NetState* dS = nullptr;
-    int32_t* d_ids = nullptr;
+    int32_t* d_ids = nullptr;     // ID field of the loaded microstructure (device)
     std::vector<void*> allocs;
     LaunchCfg cfg{256, 256, 128, 64};
 
@@ -69,7 +70,10 @@ struct gg_ctx {
 
     ~gg_ctx() {
         if (graph) cudaGraphExecDestroy(graph);
-        for (void* p : allocs) cudaFree(p);
+        if (stream) {
+            for (void* p : allocs) cudaFreeAsync(p, stream);  // back to the library's pool
+            cudaStreamSynchronize(stream);
+        }
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         for (cudaEvent_t e : fork)
@@ -96,12 +100,44 @@ int cuda_fail(gg_ctx* c, cudaError_t e, const char* where) {
         if (e_ != cudaSuccess) return cuda_fail((ctx), e_, #call);   \
     } while (0)
 
+// Device memory of the contexts comes from a stream-ordered pool of the
+// library's own, one per device, which keeps the memory a destroyed context
+// gave back for the next context of the process: creating and destroying a
+// network then maps and unmaps no memory after the first (cudaMalloc and
+// cudaFree of the arenas took 30-110 ms and up to 1 s on the 20,000-grain
+// workload).  The pool holds at most what the largest set of contexts alive
+// together used, until the process exits.
+int library_pool(gg_ctx* c, cudaMemPool_t* out) {
+    constexpr int kMaxDevices = 64;
+    static std::mutex mutex;
+    static cudaMemPool_t pools[kMaxDevices] = {};
+    const int dev = c->device;
+    if (dev < 0 || dev >= kMaxDevices) return fail(c, GG_E_INVALID, "device index out of range");
+    std::lock_guard<std::mutex> lock(mutex);
+    if (!pools[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        GG_CUDA(c, cudaMemPoolCreate(&pool, &props));
+        uint64_t keep = UINT64_MAX;
+        GG_CUDA(c, cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+        pools[dev] = pool;
+    }
+    *out = pools[dev];
+    return GG_OK;
+}
+
 template <typename T>
 int dalloc(gg_ctx* c, T** out, size_t count) {
     void* p = nullptr;
     const size_t bytes = sizeof(T) * (count > 0 ? count : 1);
-    cudaError_t e = cudaMalloc(&p, bytes);
-    if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc");
+    cudaMemPool_t pool = nullptr;
+    int rc = library_pool(c, &pool);
+    if (rc) return rc;
+    cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, pool, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaMallocFromPoolAsync");
     e = cudaMemsetAsync(p, 0, bytes, c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaMemset");
     c->allocs.push_back(p);
@@ -433,14 +469,15 @@ void conv_tables(const gg_ctx* c, int tmax, const std::vector<int64_t>& gk_off, 
         for (int n = 1; n <= tmax; ++n) {
             const int half = n / 2 + 1;
             for (int i2 = 0; i2 < half; ++i2)
-                for (int j2 = 0; j2 < half; ++j2)
-                    gk[gk_off[n] + i2 * half + j2] = gaussian_multiplier(n, i2, j2, c->dt, c->nn);
+                for (int j2 = i2; j2 < half; ++j2)  // G(i2, j2) = G(j2, i2): i2^2 + j2^2 is the argument
+                    gk[gk_off[n] + i2 * half + j2] = gk[gk_off[n] + j2 * half + i2] =
+                        gaussian_multiplier(n, i2, j2, c->dt, c->nn);
         }
         return;
     }
         // k_n[r] = (1/n) sum_f g(min(f, n-f)) cos(2 pi f r / n), g(f) = exp(-kappa f^2),
         // kappa = sqrt(2/pi) 4 dt nn^2 / n^2 pi^2 (the 1/n^2 of G split over both axes)
-        std::vector<double> gf;
+        std::vector<double> gf, cs;
         for (int n = 1; n <= tmax; ++n) {
             const double kappa = sqrt(2 / kPiH) * 4.0 * c->dt * (double)c->nn * (double)c->nn / ((double)n * n) *
                                  kPiH * kPiH;
@@ -449,9 +486,17 @@ void conv_tables(const gg_ctx* c, int tmax, const std::vector<int64_t>& gk_off, 
                 const int f2 = std::min(f, n - f);
                 gf[f] = exp(-kappa * (double)f2 * f2);
             }
+            // cos(2 pi k / n) once per k (the same expression the sum would
+            // evaluate for k = f r mod n)
+            cs.resize(n);
+            for (int k = 0; k < n; ++k) cs[k] = cos(2.0 * kPiH * (double)k / n);
             for (int r = 0; r < n; ++r) {
                 double acc = 0;
-                for (int f = 0; f < n; ++f) acc += gf[f] * cos(2.0 * kPiH * (double)((int64_t)f * r % n) / n);
+                for (int f = 0, k = 0; f < n; ++f) {  // k = f r mod n
+                    acc += gf[f] * cs[k];
+                    k += r;
+                    if (k >= n) k -= n;
+                }
                 ck[ck_off[n] + r] = (float)(acc / n);
             }
             // band radius: every entry at circular distance > R is below 2^-26 k_n[0]
@@ -650,7 +695,16 @@ int gg_load_voxels(gg_ctx* c, int32_t nn, const int32_t* ids, int32_t n_grains, 
     if (c->initialised) return fail(c, GG_E_STATE, "network already initialised");
     c->nn = nn;
     c->N = n_grains;
-    c->ids.assign(ids, ids + (size_t)nn * nn);
+    // the ID field goes straight to the device (it is read only by the
+    // distance initialisation)
+    GG_CUDA(c, cudaSetDevice(c->device));
+    if (c->d_ids_count != (size_t)nn * nn) {
+        int rc;
+        if ((rc = dalloc(c, &c->d_ids, (size_t)nn * nn)) != GG_OK) return rc;
+        c->d_ids_count = (size_t)nn * nn;
+    }
+    GG_CUDA(c, cudaMemcpyAsync(c->d_ids, ids, sizeof(int32_t) * (size_t)nn * nn, cudaMemcpyHostToDevice, c->stream));
+    GG_CUDA(c, cudaStreamSynchronize(c->stream));
     c->euler.assign(euler, euler + 3 * (size_t)n_grains);
     c->bbox.assign(bbox, bbox + 5 * (size_t)n_grains);
     c->stored.clear();
@@ -1042,7 +1096,7 @@ int gg_distance_initialisation(gg_ctx* c) {
     S.cont_cap = cont_cap;
     S.loop = P.start_time;
     ALLOC(c->dS, 1);
-    ALLOC(c->d_ids, (size_t)c->nn * c->nn);
+
 #undef ALLOC
 
     // initial per-grain data
@@ -1065,7 +1119,7 @@ int gg_distance_initialisation(gg_ctx* c) {
     GG_CUDA(c, h2d(C.quat, quat.data(), sizeof(double) * quat.size()));
     if (C.stored) GG_CUDA(c, h2d(C.stored, stored_scaled.data(), sizeof(double) * stored_scaled.size()));
     if (C.magnetic) GG_CUDA(c, h2d(C.magnetic, magnetic.data(), sizeof(double) * magnetic.size()));
-    GG_CUDA(c, h2d(c->d_ids, c->ids.data(), sizeof(int32_t) * c->ids.size()));
+
     S.phi_used = a;
     S.spec_used = sp;
     S.cont_used = cc;
