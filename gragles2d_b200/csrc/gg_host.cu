@@ -60,6 +60,8 @@ struct gg_ctx {
     NetState* dS = nullptr;
     int32_t* d_ids = nullptr;     // ID field of the loaded microstructure (device)
     std::vector<void*> allocs;
+    gg_grain_stats* d_stats = nullptr;  // packed statistics (device) and their pinned host copy
+    gg_grain_stats* h_stats = nullptr;
     LaunchCfg cfg{256, 256, 128, 64};
 
     cudaGraphExec_t graph = nullptr;
@@ -74,6 +76,7 @@ struct gg_ctx {
             for (void* p : allocs) cudaFreeAsync(p, stream);  // back to the library's pool
             cudaStreamSynchronize(stream);
         }
+        if (h_stats) cudaFreeHost(h_stats);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         for (cudaEvent_t e : fork)
@@ -1578,43 +1581,18 @@ int gg_read_grain_stats(gg_ctx* c, gg_grain_stats* out, int32_t capacity) {
     if (!c || !out) return GG_E_INVALID;
     if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
     if (capacity < c->N) return fail(c, GG_E_INVALID, "capacity smaller than the grain count");
-    int rc = refresh_state(c);
-    if (rc) return rc;
     const int N = c->N;
-    std::vector<int32_t> state(N + 1), reg(N + 1), bnd(N + 1), nbn(N + 1), cn(N + 1);
-    std::vector<double> vol(N + 1), en(N + 1), per(N + 1), mda(N + 1);
-    std::vector<Box> box(N + 1);
-    auto d2h = [&](void* dst, const void* src, size_t bytes) {
-        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream);
-    };
-    GG_CUDA(c, d2h(state.data(), c->C.state, 4 * (N + 1)));
-    GG_CUDA(c, d2h(reg.data(), c->C.regular, 4 * (N + 1)));
-    GG_CUDA(c, d2h(bnd.data(), c->C.inter_bnd, 4 * (N + 1)));
-    GG_CUDA(c, d2h(nbn.data(), c->C.nb_n, 4 * (N + 1)));
-    GG_CUDA(c, d2h(cn.data(), c->hS.cn_prev, 4 * (N + 1)));
-    GG_CUDA(c, d2h(vol.data(), c->C.volume, 8 * (N + 1)));
-    GG_CUDA(c, d2h(en.data(), c->C.energy, 8 * (N + 1)));
-    GG_CUDA(c, d2h(per.data(), c->C.perimeter, 8 * (N + 1)));
-    GG_CUDA(c, d2h(mda.data(), c->C.meanda, 8 * (N + 1)));
-    GG_CUDA(c, d2h(box.data(), c->hS.box_cur, sizeof(Box) * (N + 1)));
-    GG_CUDA(c, cudaStreamSynchronize(c->stream));
-    for (int g = 1; g <= N; ++g) {
-        gg_grain_stats& s = out[g - 1];
-        s.id = g;
-        s.state = state[g];
-        s.motion_regular = reg[g];
-        s.intersects_boundary = bnd[g];
-        s.n_neighbours = nbn[g];
-        s.contour_points = cn[g];
-        s.box[0] = box[g].x0;
-        s.box[1] = box[g].x1;
-        s.box[2] = box[g].y0;
-        s.box[3] = box[g].y1;
-        s.area = vol[g];
-        s.energy = en[g];
-        s.perimeter = per[g];
-        s.mean_da = mda[g];
+    // gathered on the device, one copy through a pinned buffer
+    if (!c->d_stats) {
+        int rc = dalloc(c, &c->d_stats, (size_t)N);
+        if (rc) return rc;
+        GG_CUDA(c, cudaMallocHost(&c->h_stats, sizeof(gg_grain_stats) * (size_t)(N > 0 ? N : 1)));
     }
+    GG_CUDA(c, pack_stats(c->C, c->dS, c->d_stats, c->stream));
+    GG_CUDA(c, cudaMemcpyAsync(c->h_stats, c->d_stats, sizeof(gg_grain_stats) * (size_t)N, cudaMemcpyDeviceToHost,
+                               c->stream));
+    GG_CUDA(c, cudaStreamSynchronize(c->stream));
+    std::memcpy(out, c->h_stats, sizeof(gg_grain_stats) * (size_t)N);
     return GG_OK;
 }
 

@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include "../../include/gg_step.h"
 #include "gg_device.cuh"
 
 namespace gg {
@@ -40,6 +41,8 @@ size_t conv_sep_smem(int tmax);
 cudaError_t batched_prepare(int tmax);
 cudaError_t batched_init(const NetConst& C, NetState* dS, const int32_t* d_ids, cudaStream_t s);
 cudaError_t finalize_only(const NetConst& C, NetState* dS, int rotate, cudaStream_t s);
+// Every grain's gg_grain_stats into out[0 .. N-1] (device memory).
+cudaError_t pack_stats(const NetConst& C, const NetState* dS, gg_grain_stats* out, cudaStream_t s);
 // Grid coarsening: every grain's field resampled onto the coarser grid.
 cudaError_t plain_resample(const NetConst& C, NetState* dS, double h_old, double hn, double delta_old,
                            cudaStream_t s);

@@ -29,6 +29,34 @@ cudaError_t plain_resample(const NetConst& C, NetState* dS, double h_old, double
     return cudaGetLastError();
 }
 
+// The per-grain statistics of gg_read_grain_stats, gathered into one array.
+__global__ void k_pack_stats(NetConst C, const NetState* S, gg_grain_stats* out) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (g > C.N) return;
+    gg_grain_stats s;
+    s.id = g;
+    s.state = C.state[g];
+    s.motion_regular = C.regular[g];
+    s.intersects_boundary = C.inter_bnd[g];
+    s.n_neighbours = C.nb_n[g];
+    s.contour_points = S->cn_prev[g];
+    const Box b = S->box_cur[g];
+    s.box[0] = b.x0;
+    s.box[1] = b.x1;
+    s.box[2] = b.y0;
+    s.box[3] = b.y1;
+    s.area = C.volume[g];
+    s.energy = C.energy[g];
+    s.perimeter = C.perimeter[g];
+    s.mean_da = C.meanda[g];
+    out[g - 1] = s;
+}
+
+cudaError_t pack_stats(const NetConst& C, const NetState* dS, gg_grain_stats* out, cudaStream_t s) {
+    if (C.N > 0) k_pack_stats<<<(C.N + 255) / 256, 256, 0, s>>>(C, dS, out);
+    return cudaGetLastError();
+}
+
 cudaError_t finalize_only(const NetConst& C, NetState* dS, int rotate, cudaStream_t s) {
     k_finalize<<<1, 1024, 0, s>>>(C, dS, rotate);
     return cudaGetLastError();
