@@ -397,6 +397,7 @@ __global__ void __launch_bounds__(128, 8) k_corrector_f(NetConst C, NetState* S)
     const int ntx = (w + 7) >> 3, ntiles = ntx * ((hgt + 3) >> 2);
     uint32_t st = 0;
     int wseed = 0;
+    const bool far_ok = C.gamma_hagb <= 1.0 && C.m_hagb <= 1.0;
     // one warp per 8 x 4 tile; pixels at or below -delta are set to -delta
     for (int t = warp; t < ntiles; t += nwarps) {
         const int x = (t % ntx) * 8 + (lane & 7), y = (t / ntx) * 4 + (lane >> 3);
@@ -420,17 +421,23 @@ __global__ void __launch_bounds__(128, 8) k_corrector_f(NetConst C, NetState* S)
             se = (float)f;
         }
         if (inside && !valid) out[k] = -delta - se;
-        // A pixel whose field and convolved value lie on the same side beyond
-        // 0.3 delta (2.1 cells) keeps that side for every weight up to 2 (the
-        // result lies between val and 2 conv - val, and |val| <= delta), and
-        // it is not next to a sign change of these near-distance fields; only
-        // signs and the values next to sign changes reach the comparison's
-        // zero crossings and the redistancing that replaces the field.  It
-        // takes weight 1 (the convolved value) without the projection.  (On
-        // the 20,000-grain workload the areas stay bit-identical for 10 steps
-        // and within 1.3e-7 relative, in a few dozen grains, after 40.)
-        const float far_level = 0.3f * delta;
-        const bool far = valid && ((val >= far_level && conv >= far_level) || (val <= -far_level && conv <= -far_level));
+        // The corrected value val + (conv - val) w lies between val and
+        // 2 conv - val for every weight w in [0, 2]; with the relative
+        // high-angle energy and mobility at most 1 the weights (energy x
+        // mobility products, junction sums of three energies, their blends)
+        // stay below 2 (far_ok).  When val, conv and
+        // 2 conv - val all lie on the same side beyond 0.3 delta (2.1 cells),
+        // the pixel keeps that side whatever its weight, and it is not next to
+        // a sign change of these near-distance fields; only signs and the
+        // values next to sign changes reach the comparison's zero crossings
+        // and the redistancing that replaces the field.  Such a pixel takes
+        // weight 1 (the convolved value) without the projection.  (On the
+        // 20,000-grain workload the areas stay bit-identical for 10 steps and
+        // within 1.3e-7 relative, in 18 grains, after 40.)
+        const float far_level = 0.3f * delta, stretched = 2.f * conv - val;
+        const bool far = far_ok && valid &&
+                         ((val >= far_level && conv >= far_level && stretched >= far_level) ||
+                          (val <= -far_level && conv <= -far_level && stretched <= -far_level));
         if (far) out[k] = conv - se;
         const bool need = valid && !far;
         if (__ballot_sync(0xffffffffu, need) == 0u) continue;
