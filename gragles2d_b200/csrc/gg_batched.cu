@@ -540,6 +540,12 @@ cudaError_t batched_init(const NetConst& C, NetState* dS, const int32_t* d_ids, 
     return cudaGetLastError();
 }
 
+cudaError_t batched_init_polygon(const NetConst& C, NetState* dS, cudaStream_t s) {
+    if (C.N <= 0) return cudaSuccess;
+    k_polygon_phi<float><<<C.N, 256, 0, s>>>(C, dS);
+    return cudaGetLastError();
+}
+
 cudaError_t batched_stage_kernel(const NetConst& C, NetState* dS, int which, cudaStream_t s, const LaunchCfg& cfg) {
     const int gt = cfg.grain_threads;
     const int gblocks = (C.N + gt - 1) / gt;

@@ -54,6 +54,11 @@ struct gg_ctx {
     std::vector<double> stored;   // .uds stored energy per grain (empty: none given)
     std::vector<double> stored_scaled;  // UseStoredElasticEnergy: scaled values, slot 0 = boundary
     std::vector<double> magnetic;       // UseMagneticField: magnetic energies, slot 0 = boundary
+    bool contour_input = false;         // MicrostructureGenMode 0: grains loaded as polygons
+    std::vector<int32_t> poly_off;      // contour input: point range of grain k at [k-1, k]
+    std::vector<double> poly_xy;        // contour input: points in domain coordinates
+    std::vector<double> poly_quat;      // contour input: 4 per grain, as given
+    std::vector<double> quat;           // orientation quaternion per grain, slot 0 = boundary
 
     NetConst C{};
     NetState hS{};               // host copy of the device NetState (pointers)
@@ -649,6 +654,8 @@ int gg_create(const gg_params* p, int device, gg_ctx** out) {
         *out = c;
         return GG_E_INVALID;
     };
+    if (p->microstructure_gen_mode != 0 && p->microstructure_gen_mode != 4)
+        return bad("only MicrostructureGenMode 0 (contour file) and 4 (voxelized) are supported");
     if (p->convolution_mode != 2) return bad("only ConvolutionMode 2 (Gaussian) is supported");
     if (p->lattice_type != 0) return bad("only LatticeType 0 (cubic) is supported");
     if (p->research_mode != 0) return bad("only ResearchMode 0 is supported");
@@ -711,8 +718,74 @@ int gg_load_voxels(gg_ctx* c, int32_t nn, const int32_t* ids, int32_t n_grains, 
     c->euler.assign(euler, euler + 3 * (size_t)n_grains);
     c->bbox.assign(bbox, bbox + 5 * (size_t)n_grains);
     c->stored.clear();
+    c->contour_input = false;
     c->loaded = true;
     return GG_OK;
+}
+
+int gg_load_contours(gg_ctx* c, int32_t n_grains, const int32_t* offsets, const double* xy, const double* quat) {
+    if (!c || !offsets || !quat || n_grains <= 0) return fail(c, GG_E_INVALID, "bad contour input");
+    if (c->initialised) return fail(c, GG_E_STATE, "network already initialised");
+    if (offsets[0] != 0) return fail(c, GG_E_INVALID, "contour offsets must start at 0");
+    for (int k = 0; k < n_grains; ++k) {
+        const int32_t np = offsets[k + 1] - offsets[k];
+        if (np < 0) return fail(c, GG_E_INVALID, "contour offsets must not decrease");
+        if (np > 0 && np < 3) return fail(c, GG_E_INVALID, "a present grain needs a polygon of 3 or more points");
+    }
+    if (offsets[n_grains] > 0 && !xy) return fail(c, GG_E_INVALID, "no contour points");
+    c->N = n_grains;
+    c->poly_off.assign(offsets, offsets + n_grains + 1);
+    c->poly_xy.resize(2 * (size_t)offsets[n_grains]);
+    // grainhdl::readMicrostructure clamps every point to the unit square
+    // (src/grainhdl.cpp:639-646)
+    for (size_t q = 0; q < c->poly_xy.size(); ++q) {
+        double v = xy[q];
+        if (v < 0) v = 0;
+        if (v > 1) v = 1;
+        c->poly_xy[q] = v;
+    }
+    c->poly_quat.assign(quat, quat + 4 * (size_t)n_grains);
+    c->euler.clear();
+    c->bbox.clear();
+    c->stored.clear();
+    c->contour_input = true;
+    c->loaded = true;
+    return GG_OK;
+}
+
+int gg_load_contour_file(gg_ctx* c, const char* base_dir) {
+    if (!c) return GG_E_INVALID;
+    std::string path(c->P.read_from_filename);
+    if (!path.empty() && path[0] != '/' && base_dir && base_dir[0]) path = std::string(base_dir) + "/" + path;
+    std::ifstream f(path);
+    if (!f) return fail(c, GG_E_IO, "cannot open " + path);
+    // grainhdl::readMicrostructure (src/grainhdl.cpp:605-654): records in file
+    // order become grains 1, 2, ...; a record ID at least the grain count
+    // raises the count, and the loop reads that many records
+    int ngrains = c->P.number_of_particles;
+    if (ngrains <= 0) return fail(c, GG_E_INVALID, "NumberOfParticles must be > 0");
+    std::vector<int32_t> off(1, 0);
+    std::vector<double> xy, quat;
+    for (int k = 1; k <= ngrains; ++k) {
+        long id = 0, nv = 0;
+        double q[4];
+        if (!(f >> id)) break;  // fewer records than grains: the rest are absent
+        if (id >= ngrains) ngrains = (int)id;
+        if (!(f >> nv >> q[0] >> q[1] >> q[2] >> q[3]) || nv < 0)
+            return fail(c, GG_E_IO, "truncated contour record in " + path);
+        for (long v = 0; v < 2 * nv; ++v) {
+            double t;
+            if (!(f >> t)) return fail(c, GG_E_IO, "truncated contour points in " + path);
+            xy.push_back(t);
+        }
+        off.push_back(off.back() + (int32_t)nv);
+        quat.insert(quat.end(), q, q + 4);
+    }
+    while ((int)off.size() < ngrains + 1) {
+        off.push_back(off.back());
+        quat.insert(quat.end(), {1.0, 0.0, 0.0, 0.0});
+    }
+    return gg_load_contours(c, ngrains, off.data(), xy.data(), quat.data());
 }
 
 int gg_load_stored_energy(gg_ctx* c, const double* stored, int32_t n_grains) {
@@ -800,9 +873,34 @@ int gg_distance_initialisation(gg_ctx* c) {
     if (c->initialised) return fail(c, GG_E_STATE, "already initialised");
     GG_CUDA(c, cudaSetDevice(c->device));
     const gg_params& P = c->P;
-    // grainhdl::read_HeaderCPG / setSimulationParameter (src/grainhdl.cpp:56-136, 275-334)
-    c->ppg = (int)(c->nn / sqrt(c->N));
+    const bool poly = c->contour_input;
+    if (poly) {
+        // grainhdl::setSimulationParameter for file input (src/grainhdl.cpp:74-78):
+        // the grid follows the parameters, not the loaded grains
+        c->nn = (int)(std::sqrt((double)(unsigned)P.number_of_particles) * (double)P.number_of_points_per_grain);
+        if (c->nn <= 0) return fail(c, GG_E_INVALID, "NumberOfParticles and NumberOfPointsPerGrain give no grid");
+        c->ppg = P.number_of_points_per_grain;
+    } else {
+        // grainhdl::read_HeaderCPG / setSimulationParameter (src/grainhdl.cpp:56-136, 275-334)
+        c->ppg = (int)(c->nn / sqrt(c->N));
+    }
     const int realDomainSize = c->nn;
+    // orientation quaternions, slot 0 the boundary (Euler (0,0,0),
+    // src/grainhdl.cpp:137): converted from the Euler angles of a voxelized
+    // input (src/box.cpp:156-217), used as given for contour input
+    // (src/box.cpp:112)
+    c->quat.assign(4 * (size_t)(c->N + 1), 0.0);
+    c->quat[0] = 1.0;
+    for (int g = 1; g <= c->N; ++g) {
+        double* q = &c->quat[4 * (size_t)g];
+        if (poly)
+            for (int k = 0; k < 4; ++k) q[k] = c->poly_quat[4 * (size_t)(g - 1) + k];
+        else
+            euler2quaternion(&c->euler[3 * (size_t)(g - 1)], q);
+    }
+    auto present = [&](int g) {
+        return poly ? c->poly_off[g] > c->poly_off[g - 1] : c->bbox[5 * (size_t)(g - 1) + 4] != 0;
+    };
     const double csr_raw = P.constant_sector_radius, isr_raw = P.interpolating_sector_radius;
     c->ds = (csr_raw * 2 + isr_raw * 2) / double(realDomainSize);
     const unsigned long ppg_used =
@@ -819,7 +917,16 @@ int gg_distance_initialisation(gg_ctx* c) {
     stored_scaled.clear();
     double energy_delta_max = 0;  // grainhdl::m_Energy_deltaMAX
     bool correct_dt = false;
-    if (P.use_stored_elastic_energy) {
+    if (P.use_stored_elastic_energy && poly) {
+        // the contour constructor sets every grain's stored energy to 0
+        // (src/box.cpp:115); the boundary keeps its default, and
+        // m_Energy_deltaMAX is not computed for this input (it stays 0)
+        const double D = P.dislocation_energy_per_m, H = P.hagb_energy, L = P.physical_domain_size;
+        stored_scaled.assign((size_t)c->N + 1, 0.0);
+        stored_scaled[0] = P.box_default_stored_elastic_energy;
+        stored_scaled[0] *= D / H * L;
+        correct_dt = true;
+    } else if (P.use_stored_elastic_energy) {
         if (c->stored.size() != (size_t)c->N) return fail(c, GG_E_STATE, "no stored energies loaded");
         const double D = P.dislocation_energy_per_m, H = P.hagb_energy, L = P.physical_domain_size;
         stored_scaled.assign((size_t)c->N + 1, 0.0);
@@ -850,14 +957,10 @@ int gg_distance_initialisation(gg_ctx* c) {
         magnetic.assign((size_t)c->N + 1, 0.0);
         const double identity[4] = {1.0, 0.0, 0.0, 0.0};
         magnetic[0] = magnetic_energy(identity, P);
-        for (int g = 1; g <= c->N; ++g) {
-            double q[4];
-            euler2quaternion(&c->euler[3 * (size_t)(g - 1)], q);
-            magnetic[g] = magnetic_energy(q, P);
-        }
+        for (int g = 1; g <= c->N; ++g) magnetic[g] = magnetic_energy(&c->quat[4 * (size_t)g], P);
         double lo = 1000000, hi = 0;
         for (int g = 1; g < c->N; ++g) {
-            if (c->bbox[5 * (size_t)(g - 1) + 4] == 0) continue;  // absent grain (no LSbox)
+            if (!present(g)) continue;  // absent grain (no LSbox)
             if (magnetic[g] < lo) lo = magnetic[g];
             if (magnetic[g] > hi) hi = magnetic[g];
         }
@@ -878,13 +981,33 @@ int gg_distance_initialisation(gg_ctx* c) {
     c->m = realDomainSize + 2 * c->b;
     const int N = c->N, m = c->m, b = c->b;
 
-    // boxes of the voxel constructor (src/box.cpp:156-217)
+    // boxes of the voxel constructor (src/box.cpp:156-217) or of the contour
+    // constructor (src/box.cpp:108-159)
     std::vector<Box> box0(N + 1, Box{0, 0, 0, 0});
     std::vector<int32_t> state(N + 1, G_GONE);
     int maxn = 1;
     for (int g = 1; g <= N; ++g) {
+        if (!present(g)) continue;  // zero-pixel grains and missing contours are skipped
+        if (poly) {
+            const double h = c->h;
+            int xmax = 0, xmin = m, ymax = 0, ymin = xmin;
+            for (int32_t k = c->poly_off[g - 1]; k < c->poly_off[g]; ++k) {
+                const double x = c->poly_xy[2 * (size_t)k], y = c->poly_xy[2 * (size_t)k + 1];
+                if (y / h < ymin) ymin = (int)(y / h);
+                if (y / h > ymax) ymax = (int)(y / h);
+                if (x / h < xmin) xmin = (int)(x / h);
+                if (x / h > xmax) xmax = (int)(x / h);
+            }
+            xmax += 2 * b;
+            ymax += 2 * b;
+            if (ymax > m) ymax = m;
+            if (xmax > m) xmax = m;
+            box0[g] = host_resize_to_square(Box{xmin, xmax, ymin, ymax}, m);
+            state[g] = G_EXISTS;
+            maxn = std::max(maxn, box_w(box0[g]));
+            continue;
+        }
         const int32_t* q = &c->bbox[5 * (size_t)(g - 1)];
-        if (q[4] == 0) continue;  // zero-pixel grains are skipped
         int xmin = m, xmax = 0, ymin = m, ymax = 0;
         const int vx[4] = {q[0], q[0], q[1], q[1]}, vy[4] = {q[2], q[3], q[2], q[3]};
         for (int k = 0; k < 4; ++k) {
@@ -919,6 +1042,7 @@ int gg_distance_initialisation(gg_ctx* c) {
             a += box_area(box0[g]);
             sp += (int64_t)spc * 2 * (int64_t)n * (n / 2 + 1);
             ccap[g] = contour_capacity(n);
+            if (poly) ccap[g] = std::max(ccap[g], c->poly_off[g] - c->poly_off[g - 1]);
             cc += ccap[g];
         }
     }
@@ -1103,9 +1227,7 @@ int gg_distance_initialisation(gg_ctx* c) {
 #undef ALLOC
 
     // initial per-grain data
-    std::vector<double> quat(4 * (size_t)(N + 1), 0.0);
-    quat[0] = 1.0;  // boundary grain: Euler (0,0,0) (src/grainhdl.cpp:137)
-    for (int g = 1; g <= N; ++g) euler2quaternion(&c->euler[3 * (size_t)(g - 1)], &quat[4 * (size_t)g]);
+    const std::vector<double>& quat = c->quat;
     std::vector<int32_t> ones(N + 1, 1);
     auto h2d = [&](void* dst, const void* src, size_t bytes) {
         return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream);
@@ -1129,7 +1251,35 @@ int gg_distance_initialisation(gg_ctx* c) {
     GG_CUDA(c, h2d(c->dS, &S, sizeof(NetState)));
 
     if (!plain) GG_CUDA(c, batched_prepare(tmax));
-    GG_CUDA(c, plain ? plain_init(C, c->dS, c->d_ids, c->stream) : batched_init(C, c->dS, c->d_ids, c->stream));
+    if (poly) {
+        // the loaded polygon is the grain's contour until the first level-set
+        // stage (energy and mobility 0, no junctions); its area is
+        // computeVolume / h^2 (src/box.cpp:396-397, src/grainBoundary.cpp:201-213)
+        std::vector<CPoint> pts((size_t)std::max<int64_t>(cc, 1), CPoint{0, 0, 0, 0});
+        std::vector<int32_t> cn(N + 1, 0);
+        std::vector<double> vol(N + 1, 0.0);
+        for (int g = 1; g <= N; ++g) {
+            if (state[g] != G_EXISTS) continue;
+            const int32_t k0 = c->poly_off[g - 1], np = c->poly_off[g] - k0;
+            for (int32_t k = 0; k < np; ++k)
+                pts[coff[g] + k] = CPoint{c->poly_xy[2 * (size_t)(k0 + k)], c->poly_xy[2 * (size_t)(k0 + k) + 1], 0, 0};
+            cn[g] = np;
+            double v = 0;
+            for (int32_t k = 0; k + 1 < np; ++k) {
+                const CPoint& p0 = pts[coff[g] + k];
+                const CPoint& p1 = pts[coff[g] + k + 1];
+                v += (p0.y + p1.y) * (p0.x - p1.x);
+            }
+            v = std::fabs(v) * c->h * c->h * 0.5;
+            vol[g] = v / (c->h * c->h);
+        }
+        GG_CUDA(c, h2d(S.contPrev, pts.data(), sizeof(CPoint) * (size_t)cc));
+        GG_CUDA(c, h2d(S.cn_prev, cn.data(), sizeof(int32_t) * (N + 1)));
+        GG_CUDA(c, h2d(C.volume, vol.data(), sizeof(double) * (N + 1)));
+        GG_CUDA(c, plain ? plain_init_polygon(C, c->dS, c->stream) : batched_init_polygon(C, c->dS, c->stream));
+    } else {
+        GG_CUDA(c, plain ? plain_init(C, c->dS, c->d_ids, c->stream) : batched_init(C, c->dS, c->d_ids, c->stream));
+    }
     GG_CUDA(c, finalize_only(C, c->dS, 0, c->stream));
     rc = check_status(c);
     if (rc != GG_OK) return rc;
@@ -1419,9 +1569,8 @@ int gg_write_analysis(gg_ctx* c, const char* directory, int32_t loop) {
     for (int g = 1; g <= N; ++g) {
         if (state[g] != G_EXISTS || reg[g] == 0) continue;
         total_energy += en[g];
-        double eul[3], q[4];
-        euler2quaternion(&c->euler[3 * (size_t)(g - 1)], q);
-        quaternion2euler(q, eul);
+        double eul[3];
+        quaternion2euler(&c->quat[4 * (size_t)g], eul);
         if (nbins > 0) {
             // ExplicitGrainBoundary::calculateDiscreteEnergyDistribution
             // (src/grainBoundary.cpp:578-598): lengths summed per bin in
@@ -1513,19 +1662,24 @@ int gg_write_restart(gg_ctx* c, const char* directory, int32_t loop) {
     const std::string tail = "_TIMESTEP_" + std::to_string(loop) + "_GRAINS_" + std::to_string(nr);
     const std::string dat_name = "NETWORK_NONAME" + tail + ".dat";
     const std::string dir(directory);
-    // LSbox::plot_full_grain (src/box.cpp:1552-1596), absolute coordinates
+    // LSbox::plot_full_grain (src/box.cpp:1552-1596): domain coordinates,
+    // except after step 0 of a contour input, where the reference prints the
+    // grid coordinates as they are (src/grainhdl.cpp:1194-1198)
     std::ofstream dat(dir + "/" + dat_name);
     if (!dat) return fail(c, GG_E_IO, "cannot write " + dir + "/" + dat_name);
     const double h = c->h;
     const int blowup = c->b;
+    const bool absolute = loop != 0 || !c->contour_input;
     for (int g = 1; g <= N; ++g) {
         if (state[g] != G_EXISTS) continue;
-        double q[4];
-        euler2quaternion(&c->euler[3 * (size_t)(g - 1)], q);
+        const double* q = &c->quat[4 * (size_t)g];
         dat << g << "\t" << cn[g] << "\t" << q[0] << "\t" << q[1] << "\t" << q[2] << "\t" << q[3] << std::endl;
         for (int k = 0; k < cn[g]; ++k) {
             const CPoint& p = pts[(size_t)(coff[g] - lo + k)];
-            dat << (p.x - blowup) * h << "\t" << (p.y - blowup) * h << std::endl;
+            if (absolute)
+                dat << (p.x - blowup) * h << "\t" << (p.y - blowup) * h << std::endl;
+            else
+                dat << p.x << "\t" << p.y << std::endl;
         }
         dat << std::endl;
     }
@@ -1539,7 +1693,7 @@ int gg_write_restart(gg_ctx* c, const char* directory, int32_t loop) {
     x << "<?xml version=\"1.0\" encoding=\"utf-8\"?>\n<Parameters>\n";
     tag("StartTime", loop);
     tag("NumberOfParticles", nr);
-    tag("NumberOfPointsPerGrain", c->ppg);  // set from the grid in mode 4 (src/grainhdl.cpp:331)
+    tag("NumberOfPointsPerGrain", c->ppg);  // from the grid in mode 4 (src/grainhdl.cpp:331), else as given
     tag("AnalysisTimestep", P.analysis_timestep);
     tag("PlotInterval", P.plot_interval);
     tag("NumberOfTimesteps", P.number_of_timesteps);

@@ -911,6 +911,76 @@ __global__ void k_init_contour(NetConst C, NetState* S) {
     C.volume[g] = contour_volume(o.pts, o.n, C.h);
 }
 
+// ---------------------------------------------------------------------------
+// Initialisation for contour input (LSbox::calculateDistanceFunction,
+// src/box.cpp:342-400): every pixel (i, j) of the grain's box, at domain
+// point ((j - b) h, (i - b) h), takes the distance to the nearest edge of the
+// loaded polygon (point-to-segment, the end points where the foot falls
+// outside), clamped to delta, positive inside by the crossing-number test.
+// Both loops run over the edges (p[k-1], p[k]) in order with the reference's
+// expressions, so the FP64 result is the reference's bit for bit; a
+// zero-length edge gives NaN and leaves the minimum unchanged, as std::min
+// does.  One CTA per grain; the polygon is staged in shared memory when it
+// fits, else read from the contour arena.  The other field buffer is zeroed:
+// the reference's input buffer is never written in this mode.
+// ---------------------------------------------------------------------------
+constexpr int kPolySmem = 1024;
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_polygon_phi(NetConst C, NetState* S) {
+    const int g = blockIdx.x + 1;
+    if (g > C.N || C.state[g] != G_EXISTS || halted(S)) return;
+    __shared__ double s_x[kPolySmem], s_y[kPolySmem];
+    const int np = S->cn_prev[g];
+    const CPoint* pts = S->contPrev + S->coff_prev[g];
+    const bool staged = np <= kPolySmem;
+    if (staged)
+        for (int k = threadIdx.x; k < np; k += blockDim.x) {
+            s_x[k] = pts[k].x;
+            s_y[k] = pts[k].y;
+        }
+    __syncthreads();
+    const Box bx = S->box_cur[g];
+    const int w = box_w(bx);
+    const int64_t area = box_area(bx);
+    R* phi = phiA_of<R>(S) + S->off_cur[g];
+    R* other = phiB_of<R>(S) + S->off_cur[g];
+    const double h = C.h, delta = C.delta;
+    const int b = C.b;
+    for (int64_t p = threadIdx.x; p < area; p += blockDim.x) {
+        const int i = bx.y0 + (int)(p / w), j = bx.x0 + (int)(p % w);
+        const double tx = (j - b) * h, ty = (i - b) * h;
+        bool inside = false;
+        double min_dist = 1000000.0;
+        double lx = staged ? s_x[0] : pts[0].x, ly = staged ? s_y[0] : pts[0].y;
+        for (int k = 1; k < np; ++k) {
+            const double kx = staged ? s_x[k] : pts[k].x, ky = staged ? s_y[k] : pts[k].y;
+            if (((ly > ty) != (ky > ty)) && (tx < (kx - lx) * (ty - ly) / (ky - ly) + lx)) inside = !inside;
+            const double ux = kx - lx, uy = ky - ly;
+            double lambda = (tx - lx) * ux + (ty - ly) * uy;
+            lambda /= ux * ux + uy * uy;
+            double dist;
+            if (lambda <= 0) {
+                const double dx = tx - lx, dy = ty - ly;
+                dist = sqrt(dx * dx + dy * dy);
+            } else if (lambda >= 1) {
+                const double dx = kx - tx, dy = ky - ty;
+                dist = sqrt(dx * dx + dy * dy);
+            } else {
+                const double fx = lx + ux * lambda, fy = ly + uy * lambda;
+                const double dx = tx - fx, dy = ty - fy;
+                dist = sqrt(dx * dx + dy * dy);
+            }
+            if (dist < min_dist) min_dist = dist;
+            lx = kx;
+            ly = ky;
+        }
+        if (min_dist > delta) min_dist = delta;
+        phi[p] = (R)(inside ? min_dist : -min_dist);
+        other[p] = (R)0;
+    }
+}
+
 // grainhdl::find_neighbors + LSbox::computeDirectNeighbours
 // (src/grainhdl.cpp:1258-1283, src/box.cpp:2220-2237): every other grain whose
 // closed box overlaps (RTree::Overlap, src/RTree.h:1092-1105), ascending ID.

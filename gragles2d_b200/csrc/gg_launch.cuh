@@ -30,6 +30,8 @@ struct LaunchCfg {
 // Declared per form; defined in gg_plain.cu / gg_batched.cu.
 cudaError_t plain_stages(const NetConst& C, NetState* dS, int stages, cudaStream_t s, const LaunchCfg& cfg);
 cudaError_t plain_init(const NetConst& C, NetState* dS, const int32_t* d_ids, cudaStream_t s);
+// distance initialisation from the loaded polygons (contour input)
+cudaError_t plain_init_polygon(const NetConst& C, NetState* dS, cudaStream_t s);
 cudaError_t plain_corrector(const NetConst& C, NetState* dS, cudaStream_t s);
 cudaError_t batched_stages(const NetConst& C, NetState* dS, int stages, cudaStream_t s, const LaunchCfg& cfg);
 // The whole batched step for graph capture on s, with the independent stages
@@ -40,6 +42,7 @@ cudaError_t batched_step_graph(const NetConst& C, NetState* dS, cudaStream_t s, 
 size_t conv_sep_smem(int tmax);
 cudaError_t batched_prepare(int tmax);
 cudaError_t batched_init(const NetConst& C, NetState* dS, const int32_t* d_ids, cudaStream_t s);
+cudaError_t batched_init_polygon(const NetConst& C, NetState* dS, cudaStream_t s);
 cudaError_t finalize_only(const NetConst& C, NetState* dS, int rotate, cudaStream_t s);
 // Every grain's gg_grain_stats into out[0 .. N-1] (device memory).
 cudaError_t pack_stats(const NetConst& C, const NetState* dS, gg_grain_stats* out, cudaStream_t s);

@@ -78,6 +78,12 @@ cudaError_t plain_init(const NetConst& C, NetState* dS, const int32_t* d_ids, cu
     return cudaGetLastError();
 }
 
+cudaError_t plain_init_polygon(const NetConst& C, NetState* dS, cudaStream_t s) {
+    if (C.N <= 0) return cudaSuccess;
+    k_polygon_phi<double><<<C.N, 256, 0, s>>>(C, dS);
+    return cudaGetLastError();
+}
+
 cudaError_t traffic_launch(const NetConst& C, NetState* dS, cudaStream_t s) {
     const int gt = 128;
     k_traffic<<<(C.N + gt - 1) / gt, gt, 0, s>>>(C, dS);

@@ -25,7 +25,8 @@ ERRORS = {1: "invalid", 2: "cuda", 3: "io", 4: "state", 5: "capacity", 6: "numer
 # Entry points declared in include/gg_step.h, in declaration order.
 EXPORTS = (
     "gg_params_default", "gg_params_from_xml", "gg_create", "gg_destroy", "gg_last_error", "gg_load_voxels",
-    "gg_load_voxel_files", "gg_load_stored_energy", "gg_distance_initialisation", "gg_find_neighbors", "gg_set_neighbours",
+    "gg_load_voxel_files", "gg_load_stored_energy", "gg_load_contours", "gg_load_contour_file",
+    "gg_distance_initialisation", "gg_find_neighbors", "gg_set_neighbours",
     "gg_convolution", "gg_update_second_order_neighbors", "gg_comparison", "gg_level_set", "gg_redistancing",
     "gg_grain_count", "gg_step", "gg_status", "gg_read_grain_stats", "gg_tangent_enable", "gg_read_area_tangents",
     "gg_write_analysis", "gg_write_restart", "gg_dims", "gg_dump", "gg_last_step_ms",
@@ -101,6 +102,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "gg_load_voxels": (I, [V, I, P(I), I, P(D), P(I)]),
         "gg_load_voxel_files": (I, [V, ctypes.c_char_p]),
         "gg_load_stored_energy": (I, [V, P(D), I]),
+        "gg_load_contours": (I, [V, I, P(I), P(D), P(D)]),
+        "gg_load_contour_file": (I, [V, ctypes.c_char_p]),
         "gg_distance_initialisation": (I, [V]),
         "gg_find_neighbors": (I, [V]),
         "gg_set_neighbours": (I, [V, P(I), P(I)]),
@@ -223,8 +226,33 @@ class GrainHandler:
             self._check(self.lib.gg_load_stored_energy(self.ctx, stored.ctypes.data_as(P(ctypes.c_double)),
                                                        stored.shape[0]))
 
+    def load_contour_file(self):
+        """MicrostructureGenMode 0: the contour file ReadFromFilename names
+        (grainhdl::readMicrostructure, src/grainhdl.cpp:605-654)."""
+        self._check(self.lib.gg_load_contour_file(self.ctx, self.settings.base_dir.encode()))
+
+    def load_contours(self, contours, quats):
+        """Contour input from host arrays: `contours[k]` is grain k+1's polygon
+        (points x, y in domain coordinates; empty = absent grain) and
+        `quats[k]` its orientation quaternion."""
+        offs = np.zeros(len(contours) + 1, np.int32)
+        for k, c in enumerate(contours):
+            offs[k + 1] = offs[k] + len(c)
+        xy = np.ascontiguousarray(np.concatenate([np.asarray(c, np.float64).reshape(-1, 2) for c in contours])
+                                  if offs[-1] else np.zeros((1, 2)), dtype=np.float64)
+        q = np.ascontiguousarray(quats, dtype=np.float64).reshape(len(contours), 4)
+        P = ctypes.POINTER
+        self._check(self.lib.gg_load_contours(
+            self.ctx, len(contours), offs.ctypes.data_as(P(ctypes.c_int32)), xy.ctypes.data_as(P(ctypes.c_double)),
+            q.ctypes.data_as(P(ctypes.c_double))))
+
     def setSimulationParameter(self):
-        self.load_voxel_files()
+        """Reads the microstructure the parameters name: a contour file for
+        MicrostructureGenMode 0, the .uds/.bin pair for mode 4."""
+        if self.settings.p.microstructure_gen_mode == 0:
+            self.load_contour_file()
+        else:
+            self.load_voxel_files()
 
     # -- run_sim prologue --
     def distanceInitialisation(self):

@@ -77,7 +77,7 @@ typedef struct gg_params {
     int32_t number_of_particles;      /* NumberOfParticles */
     int32_t number_of_points_per_grain; /* NumberOfPointsPerGrain */
     int32_t domain_border_size;       /* DomainBorderSize */
-    int32_t microstructure_gen_mode;  /* MicrostructureGenMode (4 supported) */
+    int32_t microstructure_gen_mode;  /* MicrostructureGenMode (0 and 4 supported) */
     int32_t convolution_mode;         /* ConvolutionMode (2 = Gaussian supported) */
     int32_t lattice_type;             /* LatticeType (0 = cubic supported) */
     int32_t is_isotropic_network;     /* IsIsotropicNetwork */
@@ -171,8 +171,30 @@ int gg_load_voxel_files(gg_ctx* ctx, const char* base_dir);
  * file.  Call after gg_load_voxels, before gg_distance_initialisation. */
 int gg_load_stored_energy(gg_ctx* ctx, const double* stored, int32_t n_grains);
 
-/* grainhdl::distanceInitialisation for mode-4 input (src/grainhdl.cpp:728-753,
- * src/box.cpp:322-341): +-h field, redistancing, contour. */
+/* Loads grain contours, MicrostructureGenMode 0 (replaces
+ * grainhdl::readMicrostructure, src/grainhdl.cpp:605-654, and the LSbox
+ * read-from-file constructor, src/box.cpp:108-159).  Grain k (k = 1 ..
+ * n_grains) is the k-th contour: offsets[k-1] .. offsets[k]-1 index its
+ * points, xy[2p], xy[2p+1] in domain coordinates (clamped to [0, 1] as the
+ * reference clamps them), and quat[4(k-1)] .. quat[4(k-1)+3] its
+ * orientation quaternion, used as given.  A grain with no points is
+ * absent; one with 1 or 2 points is refused.  The grid is
+ * int(sqrt(NumberOfParticles) x NumberOfPointsPerGrain) points, as the
+ * reference computes it for this mode (src/grainhdl.cpp:74-78). */
+int gg_load_contours(gg_ctx* ctx, int32_t n_grains, const int32_t* offsets, const double* xy, const double* quat);
+/* Same, reading the contour file ReadFromFilename names (a NETWORK_*.dat
+ * restart file as gg_write_restart writes it; relative to base_dir when not
+ * absolute).  Grains are numbered in file order, as the reference numbers
+ * them; a record whose ID is at least the grain count raises the count to
+ * that ID, and grains without a record are absent (the reference reads past
+ * the end of the file there). */
+int gg_load_contour_file(gg_ctx* ctx, const char* base_dir);
+
+/* grainhdl::distanceInitialisation (src/grainhdl.cpp:728-753).  Mode-4 input
+ * (src/box.cpp:322-341): +-h field, redistancing, contour.  Contour input
+ * (src/box.cpp:342-400): the signed distance to the grain's polygon, clamped
+ * to +-delta, sign from the crossing-number point-in-polygon test; the
+ * contour stays the loaded polygon until the first level-set stage. */
 int gg_distance_initialisation(gg_ctx* ctx);
 /* grainhdl::find_neighbors (src/grainhdl.cpp:1258-1283): every grain whose box
  * intersects, in ascending ID order. */

@@ -154,3 +154,30 @@ def realtime(loop: int, start_time: int, dt: float, physical_domain_size: float,
 
 def stats_line(time: float, nr_grains: int, total_energy: float, nn: int) -> str:
     return "%s\t%d\t%s\t%d\n" % (g6(time), nr_grains, g6(0.5 * total_energy), nn)
+
+
+def read_network(path: str, number_of_particles: int):
+    """(polygons, quaternions) of a contour file as grainhdl::readMicrostructure
+    reads it (src/grainhdl.cpp:605-654): records in file order become grains
+    1, 2, ...; a record ID at least the grain count raises the count; points
+    clamped to [0, 1].  Grains without a record get an empty polygon."""
+    with open(path) as f:
+        tok = f.read().split()
+    pos, ngrains, polys, quats = 0, number_of_particles, [], []
+    k = 1
+    while k <= ngrains:
+        if pos >= len(tok):
+            polys.append(np.zeros((0, 2)))
+            quats.append((1.0, 0.0, 0.0, 0.0))
+            k += 1
+            continue
+        gid = int(tok[pos])
+        if gid >= ngrains:
+            ngrains = gid
+        nv = int(tok[pos + 1])
+        quats.append(tuple(float(t) for t in tok[pos + 2:pos + 6]))
+        pts = np.array([float(t) for t in tok[pos + 6:pos + 6 + 2 * nv]]).reshape(nv, 2)
+        polys.append(np.clip(pts, 0.0, 1.0))
+        pos += 6 + 2 * nv
+        k += 1
+    return polys, quats

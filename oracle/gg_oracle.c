@@ -532,3 +532,56 @@ int gg_or_motion_regular(int old_contour, int new_contour, double old_volume, do
     *flagged = 1;
     return 1;
 }
+
+/* ---- contour input ------------------------------------------------------------ */
+
+void gg_or_polygon_phi(const double* pts, int n, const int* bo, int blowup, double h, double delta, double* out) {
+    const int w = bo[1] - bo[0];
+    for (int i = bo[2]; i < bo[3]; ++i)
+        for (int j = bo[0]; j < bo[1]; ++j) {
+            const double tx = (j - blowup) * h, ty = (i - blowup) * h;
+            int inside = 0;
+            for (int k = 1, l = 0; k < n; l = k++) {
+                const double lx = pts[2 * l], ly = pts[2 * l + 1], kx = pts[2 * k], ky = pts[2 * k + 1];
+                if (((ly > ty) != (ky > ty)) && (tx < (kx - lx) * (ty - ly) / (ky - ly) + lx)) inside = !inside;
+            }
+            double best = 1000000.0;
+            for (int k = 1, l = 0; k < n; l = k++) {
+                const double lx = pts[2 * l], ly = pts[2 * l + 1], kx = pts[2 * k], ky = pts[2 * k + 1];
+                const double ux = kx - lx, uy = ky - ly;
+                double lambda = (tx - lx) * ux + (ty - ly) * uy;
+                lambda /= ux * ux + uy * uy;
+                double d;
+                if (lambda <= 0)
+                    d = sqrt((tx - lx) * (tx - lx) + (ty - ly) * (ty - ly));
+                else if (lambda >= 1)
+                    d = sqrt((kx - tx) * (kx - tx) + (ky - ty) * (ky - ty));
+                else {
+                    const double fx = lx + ux * lambda, fy = ly + uy * lambda;
+                    d = sqrt((tx - fx) * (tx - fx) + (ty - fy) * (ty - fy));
+                }
+                if (d < best) best = d; /* std::min(best, d): NaN leaves best */
+            }
+            if (best > delta) best = delta;
+            out[(i - bo[2]) * w + (j - bo[0])] = inside ? best : -best;
+        }
+}
+
+void gg_or_polygon_box(const double* pts, int n, int m, int blowup, double h, int* out) {
+    int xmax = 0, xmin = m, ymax = 0, ymin = m;
+    for (int k = 0; k < n; ++k) {
+        const double x = pts[2 * k], y = pts[2 * k + 1];
+        if (y / h < ymin) ymin = (int)(y / h);
+        if (y / h > ymax) ymax = (int)(y / h);
+        if (x / h < xmin) xmin = (int)(x / h);
+        if (x / h > xmax) xmax = (int)(x / h);
+    }
+    xmax += 2 * blowup;
+    ymax += 2 * blowup;
+    if (ymax > m) ymax = m;
+    if (xmax > m) xmax = m;
+    out[0] = xmin;
+    out[1] = xmax;
+    out[2] = ymin;
+    out[3] = ymax;
+}

@@ -57,6 +57,16 @@ void gg_or_new_box(const int* newbb, int m, int* out);
 /* LSbox::executeRedistancing (src/box.cpp:1259-1399). */
 void gg_or_redistance(const double* in, const int* bi, double* out, const int* bo, double h, double delta);
 
+/* LSbox::calculateDistanceFunction for contour input (src/box.cpp:342-400):
+ * the signed distance of every pixel of box `bo` (xmin, xmax, ymin, ymax) to
+ * the polygon pts[2k], pts[2k+1] (k < n, domain coordinates), clamped to
+ * delta, positive inside by the crossing-number test. */
+void gg_or_polygon_phi(const double* pts, int n, const int* bo, int blowup, double h, double delta, double* out);
+
+/* The box of the contour constructor (src/box.cpp:108-159) before it is made
+ * square: out = xmin, xmax, ymin, ymax. */
+void gg_or_polygon_box(const double* pts, int n, int m, int blowup, double h, int* out);
+
 #ifdef __cplusplus
 }
 #endif

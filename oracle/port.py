@@ -36,6 +36,8 @@ def load():
                                   ctypes.c_int, ctypes.c_double, ctypes.c_double, _D, _U, _I]
     lib.gg_or_contour.restype = ctypes.c_int
     lib.gg_or_contour.argtypes = [_D, _I, _U, ctypes.c_uint, _D, ctypes.c_int, _I, _U, _I, _D, _D, ctypes.c_int, _I]
+    lib.gg_or_polygon_phi.argtypes = [_D, ctypes.c_int, _I, ctypes.c_int, ctypes.c_double, ctypes.c_double, _D]
+    lib.gg_or_polygon_box.argtypes = [_D, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _I]
     lib.gg_or_area.restype = ctypes.c_double
     lib.gg_or_area.argtypes = [_D, ctypes.c_int, ctypes.c_double]
     lib.gg_or_perimeter.restype = ctypes.c_double
@@ -149,3 +151,20 @@ def redistance(phi_in, box_in, box_out, h, delta):
     out = np.empty((bo[3] - bo[2], bo[1] - bo[0]))
     lib.gg_or_redistance(_p(phi_in, _D), _p(bi, _I), _p(out, _D), _p(bo, _I), h, delta)
     return out
+
+
+def polygon_phi(pts, box, blowup, h, delta):
+    """Signed distance to a polygon, clamped to delta (src/box.cpp:342-400)."""
+    pts = np.ascontiguousarray(np.asarray(pts, np.float64)[:, :2])
+    bo = _box(box)
+    out = np.empty((bo[3] - bo[2], bo[1] - bo[0]))
+    load().gg_or_polygon_phi(_p(pts, _D), pts.shape[0], _p(bo, _I), blowup, h, delta, _p(out, _D))
+    return out
+
+
+def polygon_box(pts, m, blowup, h):
+    """The contour constructor's box before squaring (src/box.cpp:108-159)."""
+    pts = np.ascontiguousarray(np.asarray(pts, np.float64)[:, :2])
+    out = np.zeros(4, np.int32)
+    load().gg_or_polygon_box(_p(pts, _D), pts.shape[0], m, blowup, h, _p(out, _I))
+    return tuple(int(v) for v in out)

@@ -19,8 +19,19 @@ from gragles2d_b200 import dumpfile
 from tests.parity import compare_records, ownership_mismatch
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
-ISO = ["iso_v20", "iso_v60", "gc_v80"]
-ANISO = ["rs_v30", "mob_v30", "se_v30", "mag_v30"]
+# rst_*: contour input (MicrostructureGenMode 0) from the reference's own
+# restart files, starting at the restart loop
+ISO = ["iso_v20", "iso_v60", "gc_v80", "rst_iso_v60"]
+ANISO = ["rs_v30", "mob_v30", "se_v30", "mag_v30", "rst_rs_v30", "rst_se_v30"]
+
+
+def _parameters(case):
+    """The case's parameters file: the restart parameters of a contour-input
+    case, else <case>.xml."""
+    d = os.path.join(GOLDEN, case)
+    with open(os.path.join(d, "case.json")) as f:
+        info = json.load(f)
+    return os.path.join(d, info.get("parameters", case + ".xml"))
 
 
 def _run_against_reference(case, tmp_path, *, exact, inject=True, precision=0):
@@ -28,9 +39,9 @@ def _run_against_reference(case, tmp_path, *, exact, inject=True, precision=0):
 
     d = os.path.join(GOLDEN, case)
     ref = dumpfile.read(os.path.join(d, "reference.dump.gz"))
-    s = gg.Settings(os.path.join(d, case + ".xml"), precision=precision)
+    s = gg.Settings(_parameters(case), precision=precision)
     h = gg.GrainHandler(s)
-    h.load_voxel_files()
+    h.setSimulationParameter()
     h.distanceInitialisation()
     if inject:
         h.set_neighbours({gid: g.sec for gid, g in ref.records[0].grains.items() if g.state})
@@ -46,7 +57,9 @@ def _run_against_reference(case, tmp_path, *, exact, inject=True, precision=0):
         if steps in want:
             h.dump(path, steps)
             got = dumpfile.read(path).records[0]
-            p = compare_records(want[steps], got, exact=exact, delta=ref.delta, check_idlocal=inject)
+            # contour input: the reference's initial set-comparison box is unset
+            p = compare_records(want[steps], got, exact=exact, delta=ref.delta, check_idlocal=inject,
+                                check_newbb=not (steps == 0 and case.startswith("rst_")))
             if not inject:
                 # own (ascending-ID) initial order: list order and the initial
                 # placeholder neighbour order differ by construction
@@ -89,7 +102,8 @@ def _areas(h):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["iso_v60", "rs_v30", "mob_v30", "se_v30", "mag_v30", "gc_v80"])
+@pytest.mark.parametrize("case", ["iso_v60", "rs_v30", "mob_v30", "se_v30", "mag_v30", "gc_v80", "rst_iso_v60",
+                                  "rst_rs_v30"])
 def test_batched_fp32_area_error_vs_plain(case):
     """The batched FP32 form (graph-captured steps) against the plain FP64
     form from the same initial state: per-grain relative area error <= 1e-3
@@ -101,8 +115,8 @@ def test_batched_fp32_area_error_vs_plain(case):
     lists = {gid: g.sec for gid, g in ref.records[0].grains.items() if g.state}
     hs = []
     for prec in (gg.PRECISION_PLAIN, gg.PRECISION_BATCHED):
-        h = gg.GrainHandler(gg.Settings(os.path.join(d, case + ".xml"), precision=prec))
-        h.load_voxel_files()
+        h = gg.GrainHandler(gg.Settings(_parameters(case), precision=prec))
+        h.setSimulationParameter()
         h.distanceInitialisation()
         h.set_neighbours(lists)
         hs.append(h)
@@ -171,3 +185,37 @@ def test_grid_coarsening_shrinks_the_grid(precision):
         assert h.status() == 0
     finally:
         h.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["rst_iso_v60", "rst_rs_v30", "rst_se_v30"])
+def test_restart_files_round_trip(case, tmp_path):
+    """The library's own restart files of the voxelized run the rst_* case
+    was cut from (rebuilt from its seed) are the reference's byte for byte:
+    the files the contour-input parity runs start from are the ones the
+    library writes."""
+    from gragles2d_b200 import gg
+    from gragles2d_b200 import microstructure as ms
+
+    d = os.path.join(GOLDEN, case)
+    with open(os.path.join(d, "case.json")) as f:
+        info = json.load(f)
+    loop, over = info["restart_loop"], info["overrides"]
+    micro = ms.voronoi(info["grains"], info["grid"], info["seed"])
+    if over.get("UseStoredElasticEnergy"):
+        micro.stored = np.random.default_rng(1000 + info["seed"]).uniform(0.0, 3000.0, info["grains"])
+    xml = ms.make_case(str(tmp_path / "src"), case + "_src", micro, NumberOfTimesteps=loop, AnalysisTimestep=loop,
+                       **over)
+    out = tmp_path / "out"
+    out.mkdir()
+    h = gg.GrainHandler(gg.Settings(xml))
+    try:
+        h.setSimulationParameter()
+        h.run_sim(analysis_dir=str(out))
+        assert h.status() == 0
+    finally:
+        h.close()
+    for name in os.listdir(d):
+        if name.startswith(("NETWORK_", "PARAMETERS_")):
+            with open(out / name) as f, open(os.path.join(d, name)) as g:
+                assert f.read() == g.read(), name
