@@ -337,7 +337,10 @@ def run_ours(args, rank, world, local_rank):
         "area_rel_err_max_ge_25px": area_err_big,
         "area_err_detail": area_diag,
         "clocks": clk.summary(),
-        "gpu_launches": (9 if aniso else 8) * K,
+        # per step: second-order lists, convolution, corrector (anisotropic),
+        # comparison, level set, arena allocation, neighbours, redistancing,
+        # end of step, work queue
+        "gpu_launches": (10 if aniso else 9) * K,
         "status": status_b,
     }
     if not args.no_gradient:

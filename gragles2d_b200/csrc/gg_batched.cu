@@ -135,7 +135,7 @@ __device__ __forceinline__ int kx_len(int n) { return 2 * n + kSepStrip + 1; }
 
 __global__ void __launch_bounds__(128) k_conv_sep(NetConst C, NetState* S) {
     extern __shared__ float sm[];
-    const int g = blockIdx.x + 1;
+    const int g = grain_at(S, blockIdx.x);
     if (g > C.N || C.state[g] != G_EXISTS || halted(S)) return;
     const Box bx = S->box_cur[g];
     const int n = box_w(bx);
@@ -342,7 +342,7 @@ __device__ __forceinline__ int project_warp(const float2* P, const float4* cbb, 
 // kForces: with the stored-energy and / or magnetic driving-force terms.
 template <bool kForces>
 __global__ void __launch_bounds__(128, 8) k_corrector_f(NetConst C, NetState* S) {
-    const int g = blockIdx.x + 1;
+    const int g = grain_at(S, blockIdx.x);
     if (g > C.N || C.state[g] != G_EXISTS || C.regular[g] == 0 || S->loop == 0 || halted(S)) return;
     __shared__ SectorSet sec;
     __shared__ __align__(16) float2 sp[kCorrMaxPts];
@@ -540,6 +540,12 @@ cudaError_t batched_init(const NetConst& C, NetState* dS, const int32_t* d_ids, 
     return cudaGetLastError();
 }
 
+cudaError_t batched_order(const NetConst& C, NetState* dS, cudaStream_t s) {
+    if (C.N <= 0) return cudaSuccess;
+    k_order<<<1, 1024, 0, s>>>(C, dS);
+    return cudaGetLastError();
+}
+
 cudaError_t batched_init_polygon(const NetConst& C, NetState* dS, cudaStream_t s) {
     if (C.N <= 0) return cudaSuccess;
     k_polygon_phi<float><<<C.N, 256, 0, s>>>(C, dS);
@@ -560,7 +566,10 @@ cudaError_t batched_stage_kernel(const NetConst& C, NetState* dS, int which, cud
         case 5: k_alloc<<<1, 1024, 0, s>>>(C, dS, 1); break;
         case 6: k_neighbours_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS, reinterpret_cast<PointInfo*>(C.ptinfo)); break;
         case 7: k_redistance_s<float><<<C.N, kRedistThreads, kRedistSmemBytes, s>>>(C, dS); break;
-        default: k_finalize<<<1, 1024, 0, s>>>(C, dS, 1); break;
+        default:
+            k_finalize<<<1, 1024, 0, s>>>(C, dS, 1);
+            k_order<<<1, 1024, 0, s>>>(C, dS);
+            break;
     }
     return cudaGetLastError();
 }
@@ -583,6 +592,7 @@ cudaError_t batched_stages(const NetConst& C, NetState* dS, int stages, cudaStre
         k_neighbours_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS, reinterpret_cast<PointInfo*>(C.ptinfo));
         k_redistance_s<float><<<C.N, kRedistThreads, kRedistSmemBytes, s>>>(C, dS);
         k_finalize<<<1, 1024, 0, s>>>(C, dS, 1);
+        k_order<<<1, 1024, 0, s>>>(C, dS);
     }
     return cudaGetLastError();
 }
@@ -611,6 +621,7 @@ cudaError_t batched_step_graph(const NetConst& C, NetState* dS, cudaStream_t s, 
     k_redistance_s<float><<<C.N, kRedistThreads, kRedistSmemBytes, s>>>(C, dS);
     if ((e = cudaStreamWaitEvent(s, ev[3], 0)) != cudaSuccess) return e;
     k_finalize<<<1, 1024, 0, s>>>(C, dS, 1);
+    k_order<<<1, 1024, 0, s>>>(C, dS);  // the next step's work queue, from its boxes
     return cudaGetLastError();
 }
 

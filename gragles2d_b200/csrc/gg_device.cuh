@@ -199,7 +199,17 @@ struct NetState {
     // dy / dp_k), same offsets and rotation as contPrev / contCur
     double* dcontPrev;
     double* dcontCur;
+    // batched form: the per-grain launches' work queue, grain IDs by
+    // descending box edge (rebuilt after every change of the boxes); null in
+    // the plain form, whose launches take grains in ID order
+    int32_t* order;
 };
+
+// The grain that work slot `slot` (0-based, < N) of a per-grain launch
+// processes: largest boxes first when the queue exists, else ID order.  Every
+// per-grain kernel writes only its own grain's outputs, so the order changes
+// when a grain runs, never what it computes.
+GG_HD int grain_at(const NetState* S, int slot) { return S->order ? S->order[slot] : slot + 1; }
 
 GG_HD void set_status(NetState* S, uint32_t bits) {
 #ifdef __CUDA_ARCH__

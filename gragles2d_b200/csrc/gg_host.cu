@@ -452,6 +452,7 @@ int coarsen_if_due(gg_ctx* c, int loop, bool* changed) {
     GG_CUDA(c, h2d(S.coff_cur, coff.data(), sizeof(int64_t) * (N + 1)));
     GG_CUDA(c, h2d(S.ccap_cur, ccap.data(), sizeof(int32_t) * (N + 1)));
     GG_CUDA(c, h2d(c->dS, &S, sizeof(NetState)));
+    if (P.precision != GG_PRECISION_PLAIN) GG_CUDA(c, batched_order(C, c->dS, c->stream));
     GG_CUDA(c, cudaStreamSynchronize(c->stream));
     if (c->graph) {  // the captured step holds the old constants
         cudaGraphExecDestroy(c->graph);
@@ -1222,6 +1223,7 @@ int gg_distance_initialisation(gg_ctx* c) {
     S.spec_cap = spec_cap;
     S.cont_cap = cont_cap;
     S.loop = P.start_time;
+    if (!plain) ALLOC(S.order, N + 1);  // the batched step's work queue
     ALLOC(c->dS, 1);
 
 #undef ALLOC
@@ -1281,6 +1283,7 @@ int gg_distance_initialisation(gg_ctx* c) {
         GG_CUDA(c, plain ? plain_init(C, c->dS, c->d_ids, c->stream) : batched_init(C, c->dS, c->d_ids, c->stream));
     }
     GG_CUDA(c, finalize_only(C, c->dS, 0, c->stream));
+    if (!plain) GG_CUDA(c, batched_order(C, c->dS, c->stream));
     rc = check_status(c);
     if (rc != GG_OK) return rc;
     c->initialised = true;

@@ -185,7 +185,7 @@ constexpr int kListMaxSmem = 128;
 
 template <typename R>
 __global__ void __launch_bounds__(256) k_compare(NetConst C, NetState* S) {
-    const int g = blockIdx.x + 1;
+    const int g = grain_at(S, blockIdx.x);
     if (g > C.N || C.state[g] != G_EXISTS || halted(S)) return;
     __shared__ Box s_box[kListMaxSmem];
     __shared__ int64_t s_org[kListMaxSmem];  // arena index of the member's pixel (0, 0)
@@ -844,6 +844,38 @@ __global__ void __launch_bounds__(1024) k_finalize(NetConst C, NetState* S, int 
     S->jn_prev = S->jn_cur;
     S->jn_cur = tjn;
     S->loop += 1;
+}
+
+// The batched form's work queue (NetState::order): existing grains by
+// descending box edge, then the rest, by a counting sort in one CTA.  A
+// per-grain launch then starts its longest blocks first and the short ones
+// fill the last wave.  The order within one edge length is whatever the
+// shared-memory atomics give; no result depends on it.
+constexpr int kOrderBins = 256;
+
+__global__ void __launch_bounds__(1024) k_order(NetConst C, NetState* S) {
+    int32_t* order = S->order;
+    if (!order) return;
+    __shared__ int s_bin[kOrderBins];
+    for (int q = threadIdx.x; q < kOrderBins; q += blockDim.x) s_bin[q] = 0;
+    __syncthreads();
+    auto bin_of = [&](int g) {
+        if (C.state[g] != G_EXISTS) return kOrderBins - 1;
+        const int e = min(max(box_w(S->box_cur[g]), 0), kOrderBins - 2);
+        return kOrderBins - 2 - e;
+    };
+    for (int g = threadIdx.x + 1; g <= C.N; g += blockDim.x) atomicAdd(&s_bin[bin_of(g)], 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int q = 0; q < kOrderBins; ++q) {
+            const int c = s_bin[q];
+            s_bin[q] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    for (int g = threadIdx.x + 1; g <= C.N; g += blockDim.x) order[atomicAdd(&s_bin[bin_of(g)], 1)] = g;
 }
 
 // Traffic model: box areas and comparison-list overlaps of existing grains.

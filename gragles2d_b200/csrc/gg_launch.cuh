@@ -43,6 +43,8 @@ size_t conv_sep_smem(int tmax);
 cudaError_t batched_prepare(int tmax);
 cudaError_t batched_init(const NetConst& C, NetState* dS, const int32_t* d_ids, cudaStream_t s);
 cudaError_t batched_init_polygon(const NetConst& C, NetState* dS, cudaStream_t s);
+// rebuilds the batched form's work queue (NetState::order) from the current boxes
+cudaError_t batched_order(const NetConst& C, NetState* dS, cudaStream_t s);
 cudaError_t finalize_only(const NetConst& C, NetState* dS, int rotate, cudaStream_t s);
 // Every grain's gg_grain_stats into out[0 .. N-1] (device memory).
 cudaError_t pack_stats(const NetConst& C, const NetState* dS, gg_grain_stats* out, cudaStream_t s);

@@ -656,7 +656,8 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_levelset_w(NetConst C,
     __shared__ WalkShared s_walk[kGrainsPerBlock];
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;
-    const int g = blockIdx.x * kGrainsPerBlock + wid + 1;
+    const int slot = blockIdx.x * kGrainsPerBlock + wid;
+    const int g = slot < C.N ? grain_at(S, slot) : C.N + 1;
     if (g > C.N || halted(S)) return;
     const int st = C.state[g];
     const Box bc = S->box_cur[g];
@@ -773,7 +774,8 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_neighbours_w(NetConst 
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;
-    const int g = blockIdx.x * kGrainsPerBlock + wid + 1;
+    const int slot = blockIdx.x * kGrainsPerBlock + wid;
+    const int g = slot < C.N ? grain_at(S, slot) : C.N + 1;
     if (g > C.N || C.state[g] != G_EXISTS || C.regular[g] == 0 || halted(S)) return;
     const int loop = S->loop;
     CPoint* P = S->contCur + S->coff_cur[g];
@@ -916,7 +918,8 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_second_order_w(NetCons
     __shared__ int s_list[kGrainsPerBlock][kL];
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;
-    const int g = blockIdx.x * kGrainsPerBlock + wid + 1;
+    const int slot = blockIdx.x * kGrainsPerBlock + wid;
+    const int g = slot < C.N ? grain_at(S, slot) : C.N + 1;
     if (g > C.N || C.state[g] != G_EXISTS) return;
     const int K = C.kmax < kL ? C.kmax : kL;
     const int* sec = C.sec_ids + (int64_t)g * C.kmax;
@@ -1346,7 +1349,7 @@ __device__ __forceinline__ void redistance_sweeps(const R* __restrict__ in, int 
 template <typename R>
 __global__ void __launch_bounds__(kRedistThreads) k_redistance_s(NetConst C, NetState* S) {
     extern __shared__ __align__(16) unsigned char s_raw[];
-    const int g = blockIdx.x + 1;
+    const int g = grain_at(S, blockIdx.x);
     if (g > C.N || C.state[g] != G_EXISTS || halted(S)) return;
     const R* in_g = phiA_of<R>(S) + S->off_cur[g];
     R* out_g = phiB_of<R>(S) + S->off_new[g];
