@@ -525,8 +525,28 @@ cudaError_t batched_resample(const NetConst& C, NetState* dS, double h_old, doub
     return cudaGetLastError();
 }
 
+// persistent grid of the large-box redistancing bin: one CTA per SM
+int g_big_grid = 148;
+
 cudaError_t batched_prepare(int tmax) {
-    return cudaFuncSetAttribute(k_conv_sep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conv_sep_smem(tmax));
+    cudaError_t e = cudaFuncSetAttribute(k_conv_sep, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)conv_sep_smem(tmax));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_redistance_big, cudaFuncAttributeMaxDynamicSharedMemorySize, kRedistBigSmemBytes);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    g_big_grid = sms > 0 ? sms : 148;
+    return cudaSuccess;
+}
+
+// The redistancing stage: the large-box bin, then the 64-thread kernel for
+// the rest.
+void launch_redistance(const NetConst& C, NetState* dS, cudaStream_t s) {
+    const int grid = C.N < g_big_grid ? C.N : g_big_grid;
+    k_redistance_big<<<grid, kRedistBigThreads, kRedistBigSmemBytes, s>>>(C, dS);
+    k_redistance_s<float><<<C.N, kRedistThreads, kRedistSmemBytes, s>>>(C, dS);
 }
 
 cudaError_t batched_init(const NetConst& C, NetState* dS, const int32_t* d_ids, cudaStream_t s) {
@@ -565,7 +585,7 @@ cudaError_t batched_stage_kernel(const NetConst& C, NetState* dS, int which, cud
         case 4: k_levelset_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS); break;
         case 5: k_alloc<<<1, 1024, 0, s>>>(C, dS, 1); break;
         case 6: k_neighbours_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS, reinterpret_cast<PointInfo*>(C.ptinfo)); break;
-        case 7: k_redistance_s<float><<<C.N, kRedistThreads, kRedistSmemBytes, s>>>(C, dS); break;
+        case 7: launch_redistance(C, dS, s); break;
         default:
             k_finalize<<<1, 1024, 0, s>>>(C, dS, 1);
             k_order<<<1, 1024, 0, s>>>(C, dS);
@@ -590,7 +610,7 @@ cudaError_t batched_stages(const NetConst& C, NetState* dS, int stages, cudaStre
     if (stages & ST_REDIST) {
         k_alloc<<<1, 1024, 0, s>>>(C, dS, 1);
         k_neighbours_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS, reinterpret_cast<PointInfo*>(C.ptinfo));
-        k_redistance_s<float><<<C.N, kRedistThreads, kRedistSmemBytes, s>>>(C, dS);
+        launch_redistance(C, dS, s);
         k_finalize<<<1, 1024, 0, s>>>(C, dS, 1);
         k_order<<<1, 1024, 0, s>>>(C, dS);
     }
@@ -618,7 +638,7 @@ cudaError_t batched_step_graph(const NetConst& C, NetState* dS, cudaStream_t s, 
     if ((e = cudaStreamWaitEvent(s2, ev[2], 0)) != cudaSuccess) return e;
     k_neighbours_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s2>>>(C, dS, reinterpret_cast<PointInfo*>(C.ptinfo));
     if ((e = cudaEventRecord(ev[3], s2)) != cudaSuccess) return e;
-    k_redistance_s<float><<<C.N, kRedistThreads, kRedistSmemBytes, s>>>(C, dS);
+    launch_redistance(C, dS, s);
     if ((e = cudaStreamWaitEvent(s, ev[3], 0)) != cudaSuccess) return e;
     k_finalize<<<1, 1024, 0, s>>>(C, dS, 1);
     k_order<<<1, 1024, 0, s>>>(C, dS);  // the next step's work queue, from its boxes

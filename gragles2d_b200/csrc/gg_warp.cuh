@@ -1340,17 +1340,14 @@ __device__ __forceinline__ void redistance_sweeps(const R* __restrict__ in, int 
         redistance_sweeps_indexed<R>(in, in_x0, in_y0, si, bi, out, so, bo, h);
 }
 
-// LSbox::executeRedistancing, one CTA of 64 threads per grain.  When both
-// fit in kRedistSmemBytes, the input over the intersection of the old and new
-// boxes and the output box are staged in shared memory with odd row strides
-// (so the row-wise sweeps hit distinct banks); a larger box keeps only its
-// output there, and the largest stay in global memory.  clearValues(-1)
-// before, clampValues(-delta, delta) after.
-template <typename R>
-__global__ void __launch_bounds__(kRedistThreads) k_redistance_s(NetConst C, NetState* S) {
-    extern __shared__ __align__(16) unsigned char s_raw[];
-    const int g = grain_at(S, blockIdx.x);
-    if (g > C.N || C.state[g] != G_EXISTS || halted(S)) return;
+// LSbox::executeRedistancing of grain g by the whole CTA (any block size).
+// When both fit in kSmem bytes, the input over the intersection of the old
+// and new boxes and the output box are staged in shared memory with odd row
+// strides (so the row-wise sweeps hit distinct banks); a larger box keeps
+// only its output there, and the largest stay in global memory.
+// clearValues(-1) before, clampValues(-delta, delta) after.
+template <typename R, int kSmem>
+__device__ void redistance_grain_s(const NetConst& C, NetState* S, int g, unsigned char* s_raw) {
     const R* in_g = phiA_of<R>(S) + S->off_cur[g];
     R* out_g = phiB_of<R>(S) + S->off_new[g];
     const Box bi = S->box_cur[g], bo = S->box_new[g];
@@ -1363,7 +1360,7 @@ __global__ void __launch_bounds__(kRedistThreads) k_redistance_s(NetConst C, Net
     const int iymax = (bi.y1 < bo.y1) ? bi.y1 : bo.y1;
     const int wI = ixmax > ixmin ? ixmax - ixmin : 0, hI = iymax > iymin ? iymax - iymin : 0;
     const int so = wo | 1, sI = wI | 1;
-    const bool fits = (int64_t)sizeof(R) * ((int64_t)so * ho + (int64_t)sI * hI) <= kRedistSmemBytes;
+    const bool fits = (int64_t)sizeof(R) * ((int64_t)so * ho + (int64_t)sI * hI) <= kSmem;
     if (fits) {
         R* out = reinterpret_cast<R*>(s_raw);
         R* in = out + so * ho;
@@ -1390,7 +1387,7 @@ __global__ void __launch_bounds__(kRedistThreads) k_redistance_s(NetConst C, Net
                     v = delta;
                 out_g[(int64_t)r * wo + c] = v;
             }
-    } else if ((int64_t)sizeof(R) * so * ho <= kRedistSmemBytes) {  // output staged, input read in place
+    } else if ((int64_t)sizeof(R) * so * ho <= kSmem) {  // output staged, input read in place
         R* out = reinterpret_cast<R*>(s_raw);
         for (int p = threadIdx.x; p < so * ho; p += blockDim.x) out[p] = (R)-1.0;
         __syncthreads();
@@ -1416,6 +1413,45 @@ __global__ void __launch_bounds__(kRedistThreads) k_redistance_s(NetConst C, Net
                 v = delta;
             out_g[p] = v;
         }
+    }
+}
+
+// Large boxes (batched form, size bin above kRedistBigEdge): k_redistance_big
+// takes them with 256 threads and up to 200 KB of shared memory, so a 168^2
+// box is staged whole and a 256^2 one sweeps 4x as many columns at a time.
+// The bin starts above the largest boxes of a uniform-seed Voronoi network
+// (edge <= 98 at 25 cells per grain), so there it is an empty launch.
+constexpr int kRedistBigEdge = 128;
+constexpr int kRedistBigThreads = 256;
+constexpr int kRedistBigSmemBytes = 200 * 1024;
+
+// One CTA of 64 threads per grain: every grain in the plain form; in the
+// batched form those whose box edge is at most kRedistBigEdge.
+template <typename R>
+__global__ void __launch_bounds__(kRedistThreads) k_redistance_s(NetConst C, NetState* S) {
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    const int g = grain_at(S, blockIdx.x);
+    if (g > C.N || C.state[g] != G_EXISTS || halted(S)) return;
+    if (S->order && box_w(S->box_cur[g]) > kRedistBigEdge) return;  // the large-box bin
+    redistance_grain_s<R, kRedistSmemBytes>(C, S, g, s_raw);
+}
+
+// The large-box bin of the batched form: a persistent grid walks the work
+// queue (largest boxes first) and stops at the first existing grain at or
+// below kRedistBigEdge; k_redistance_s follows it on the same stream (run
+// side by side, the two measured slower: the 64-thread kernel's blocks take
+// the SMs first).
+__global__ void __launch_bounds__(kRedistBigThreads) k_redistance_big(NetConst C, NetState* S) {
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    if (!S->order) return;
+    for (int slot = blockIdx.x; slot < C.N; slot += gridDim.x) {
+        const int g = S->order[slot];
+        // a grain that vanished in this step's level set keeps its place in
+        // the queue; existing grains are in descending box edge
+        if (C.state[g] != G_EXISTS || halted(S)) continue;
+        if (box_w(S->box_cur[g]) <= kRedistBigEdge) return;
+        redistance_grain_s<float, kRedistBigSmemBytes>(C, S, g, s_raw);
+        __syncthreads();  // the next grain reuses the shared buffers
     }
 }
 
