@@ -99,6 +99,9 @@ int fail(gg_ctx* c, int code, const std::string& msg) {
 }
 
 int cuda_fail(gg_ctx* c, cudaError_t e, const char* where) {
+    // consume the runtime's last error as well, so that a failure reported
+    // here is not reported again by a later, unrelated call of this thread
+    (void)cudaGetLastError();
     return fail(c, GG_E_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
 

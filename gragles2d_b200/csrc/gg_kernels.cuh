@@ -1016,32 +1016,47 @@ __global__ void __launch_bounds__(256) k_polygon_phi(NetConst C, NetState* S) {
 // grainhdl::find_neighbors + LSbox::computeDirectNeighbours
 // (src/grainhdl.cpp:1258-1283, src/box.cpp:2220-2237): every other grain whose
 // closed box overlaps (RTree::Overlap, src/RTree.h:1092-1105), ascending ID.
-__global__ void k_find_neighbors(NetConst C, NetState* S) {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x + 1;
+// One warp per grain: the lanes test 32 consecutive IDs at a time (coalesced
+// box loads) and a ballot keeps the hits in ascending order.
+constexpr int kFindWarps = 4;
+
+__global__ void __launch_bounds__(32 * kFindWarps) k_find_neighbors(NetConst C, NetState* S) {
+    const int lane = threadIdx.x & 31;
+    const int g = blockIdx.x * kFindWarps + (threadIdx.x >> 5) + 1;
     if (g > C.N || C.state[g] == G_GONE) return;
     const Box a = S->box_cur[g];
-    int ns = 0, nbn = 0;
+    int ns = 0;
     bool overflow = false;
     int* sec = C.sec_ids + (int64_t)g * C.kmax;
     Neighbour* nb = C.nb + (int64_t)g * C.nbmax;
-    for (int k = 1; k <= C.N; ++k) {
-        if (k == g || C.state[k] == G_GONE) continue;
-        const Box b = S->box_cur[k];
-        if (a.x0 > b.x1 || b.x0 > a.x1 || a.y0 > b.y1 || b.y0 > a.y1) continue;
-        if (ns < C.kmax) sec[ns++] = k; else overflow = true;
-        if (nbn < C.nbmax) {
-            nb[nbn].id = k;
-            nb[nbn].length = 0;
-            nb[nbn].energy = 0;
-            nb[nbn].misori = 0;
-            nb[nbn].mobility = 0;
-            nbn++;
+    for (int k0 = 1; k0 <= C.N; k0 += 32) {
+        const int k = k0 + lane;
+        bool hit = false;
+        if (k <= C.N && k != g && C.state[k] != G_GONE) {
+            const Box b = S->box_cur[k];
+            hit = !(a.x0 > b.x1 || b.x0 > a.x1 || a.y0 > b.y1 || b.y0 > a.y1);
         }
+        const unsigned mask = __ballot_sync(0xffffffffu, hit);
+        if (hit) {
+            const int pos = ns + __popc(mask & ((1u << lane) - 1u));
+            if (pos < C.kmax) sec[pos] = k; else overflow = true;
+            if (pos < C.nbmax) {
+                nb[pos].id = k;
+                nb[pos].length = 0;
+                nb[pos].energy = 0;
+                nb[pos].misori = 0;
+                nb[pos].mobility = 0;
+            }
+        }
+        ns += __popc(mask);
     }
-    C.sec_n[g] = ns;
-    C.cmp_n[g] = 0;
-    C.nb_n[g] = nbn;
-    if (overflow) set_status(S, S_LIST_OVERFLOW);
+    overflow = __any_sync(0xffffffffu, overflow);
+    if (lane == 0) {
+        C.sec_n[g] = ns < C.kmax ? ns : C.kmax;
+        C.cmp_n[g] = 0;
+        C.nb_n[g] = ns < C.nbmax ? ns : C.nbmax;
+        if (overflow) set_status(S, S_LIST_OVERFLOW);
+    }
 }
 
 }  // namespace

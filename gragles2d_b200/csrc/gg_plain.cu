@@ -63,8 +63,7 @@ cudaError_t finalize_only(const NetConst& C, NetState* dS, int rotate, cudaStrea
 }
 
 cudaError_t find_neighbors_launch(const NetConst& C, NetState* dS, cudaStream_t s) {
-    const int gt = 128;
-    k_find_neighbors<<<(C.N + gt - 1) / gt, gt, 0, s>>>(C, dS);
+    k_find_neighbors<<<(C.N + kFindWarps - 1) / kFindWarps, 32 * kFindWarps, 0, s>>>(C, dS);
     return cudaGetLastError();
 }
 
