@@ -83,6 +83,10 @@ RESTARTS = {
     # finds no neighbour characteristic for IDLocal (its force term is -1)
     "rst_se_v30": (("voronoi", 30, 120, 6, {"IsIsotropicNetwork": 0, "UseStoredElasticEnergy": 1,
                                              "DislocEnPerM": 1.0, "BoxDefaultStoredElasticEnergy": 500.0}), 5, 5),
+    # grid coarsening on: restarted at loop 8 (80 grains, grid int(sqrt(80) * 11) = 98), the run from the
+    # contour file coarsens its grid as grains vanish
+    "rst_gc_v80": (("voronoi", 80, 100, 11, {"IsIsotropicNetwork": 1, "GridCoarsement": 1,
+                                             "GridCoarsementGradient": 0.99}), 8, 2),
 }
 
 

@@ -127,7 +127,7 @@ def test_rejects_a_loop_that_is_not_the_last_step(golden_dir, tmp_path):
         h.close()
 
 
-@pytest.mark.parametrize("name", ["rst_iso_v60", "rst_rs_v30", "rst_se_v30"])
+@pytest.mark.parametrize("name", ["rst_iso_v60", "rst_rs_v30", "rst_se_v30", "rst_gc_v80"])
 def test_contour_input_run_writes_the_reference_files(golden_dir, name, tmp_path):
     """A run from a contour file (MicrostructureGenMode 0, starting at the
     restart loop): the analysis files on the reference's schedule, counted

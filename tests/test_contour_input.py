@@ -16,7 +16,7 @@ from gragles2d_b200 import dumpfile, gg
 from oracle import analysis, port
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
-CASES = ["rst_iso_v60", "rst_rs_v30", "rst_se_v30"]
+CASES = ["rst_iso_v60", "rst_rs_v30", "rst_se_v30", "rst_gc_v80"]
 
 
 def _case(name):

@@ -21,7 +21,7 @@ from tests.parity import compare_records, ownership_mismatch
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 # rst_*: contour input (MicrostructureGenMode 0) from the reference's own
 # restart files, starting at the restart loop
-ISO = ["iso_v20", "iso_v60", "gc_v80", "rst_iso_v60"]
+ISO = ["iso_v20", "iso_v60", "gc_v80", "rst_iso_v60", "rst_gc_v80"]
 ANISO = ["rs_v30", "mob_v30", "se_v30", "mag_v30", "rst_rs_v30", "rst_se_v30"]
 
 
@@ -103,7 +103,7 @@ def _areas(h):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("case", ["iso_v60", "rs_v30", "mob_v30", "se_v30", "mag_v30", "gc_v80", "rst_iso_v60",
-                                  "rst_rs_v30"])
+                                  "rst_rs_v30", "rst_gc_v80"])
 def test_batched_fp32_area_error_vs_plain(case):
     """The batched FP32 form (graph-captured steps) against the plain FP64
     form from the same initial state: per-grain relative area error <= 1e-3
@@ -188,7 +188,7 @@ def test_grid_coarsening_shrinks_the_grid(precision):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["rst_iso_v60", "rst_rs_v30", "rst_se_v30"])
+@pytest.mark.parametrize("case", ["rst_iso_v60", "rst_rs_v30", "rst_se_v30", "rst_gc_v80"])
 def test_restart_files_round_trip(case, tmp_path):
     """The library's own restart files of the voxelized run the rst_* case
     was cut from (rebuilt from its seed) are the reference's byte for byte:
