@@ -226,9 +226,10 @@ def run_ours(args, rank, world, local_rank):
     hb.distanceInitialisation()
     hb.find_neighbors()
     stats_bytes = 0
+    st = None  # one statistics array, filled again every step
     for _ in range(K):
         hb.step(1)
-        st = hb.grain_stats()
+        st = hb.grain_stats(st)
         stats_bytes += len(st) * ctypes.sizeof(gg.GrainStats)
     t_e2e = time.perf_counter() - t0
     upd_e2e = hb.grain_updates()

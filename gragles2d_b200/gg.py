@@ -347,9 +347,11 @@ class GrainHandler:
         self._check(self.lib.gg_status(self.ctx, ctypes.byref(s), int(clear)))
         return s.value
 
-    def grain_stats(self):
+    def grain_stats(self, out=None):
+        """Every grain's statistics (gg_read_grain_stats); `out`, an array
+        from an earlier call, is filled again instead of a new one."""
         n = self.dims().n_grains
-        arr = (GrainStats * n)()
+        arr = out if out is not None and len(out) >= n else (GrainStats * n)()
         self._check(self.lib.gg_read_grain_stats(self.ctx, arr, n))
         return arr
 
