@@ -72,3 +72,24 @@ def test_create_rejects_generation_modes(mode):
     with pytest.raises(gg.GGError) as e:
         gg.GrainHandler(s)
     assert e.value.code == 1 and "MicrostructureGenMode" in str(e.value)
+
+
+def test_oracle_polygon_distance_known_answers():
+    """A square of side 0.5 centred in the unit domain on a 40-point grid:
+    inside, the distance to the nearest side; outside, to the nearest side or
+    corner; both clamped to delta."""
+    nn, b = 40, 7
+    h, delta = 1.0 / nn, b / nn
+    sq = np.array([[0.25, 0.25], [0.75, 0.25], [0.75, 0.75], [0.25, 0.75], [0.25, 0.25]])
+    m = nn + 2 * b
+    box = (0, m, 0, m)
+    phi = port.polygon_phi(sq, box, b, h, delta)
+    for i in range(m):
+        for j in range(m):
+            x, y = (j - b) * h, (i - b) * h
+            dx = max(0.25 - x, 0.0, x - 0.75)
+            dy = max(0.25 - y, 0.0, y - 0.75)
+            inside = 0.25 < x < 0.75 and 0.25 < y < 0.75
+            d = min(x - 0.25, 0.75 - x, y - 0.25, 0.75 - y) if inside else float(np.hypot(dx, dy))
+            want = min(d, delta) * (1 if inside else -1)
+            assert abs(phi[i, j] - want) <= 1e-15, (i, j, phi[i, j], want)
