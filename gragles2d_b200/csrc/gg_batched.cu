@@ -217,32 +217,38 @@ __device__ __forceinline__ unsigned long long f2_fma(unsigned long long a, unsig
     return r;
 }
 
-// projectToGrainBondary (src/grainBoundary.cpp:365-447) in FP32 for the
-// pixels (px, py) of the 32 lanes of a warp (all lanes call it; `valid` lanes
-// are the warp's real pixels, the others only follow along).  The nearest
-// vertex of each lane is the first one at the smallest distance, with
-// distances compared to 14 mantissa bits: each candidate is one 32-bit key,
-// the squared distance's bits with the low 9 replaced by the vertex index
-// (contours of up to 512 points), so one unsigned minimum keeps the smallest
-// distance and, among equal keys, the lowest index.  Chunks are visited out
-// of index order (first the chunk `*wseed` that held the nearest vertex of
-// the warp's previous tile, then the others that the bound does not rule
-// out).  P holds the contour with a 16-byte aligned start, two points per
-// float4.
-constexpr unsigned kKeyIndexBits = 9;
-constexpr unsigned kKeyIndexMask = (1u << kKeyIndexBits) - 1u;
-static_assert(kCorrMaxPts <= (1 << kKeyIndexBits), "vertex index must fit the key");
+// projectToGrainBondary (src/grainBoundary.cpp:365-447) for the pixels
+// (px, py) of the 32 lanes of a warp (all lanes call it; `valid` lanes are
+// the warp's real pixels, the others only follow along), with the reference's
+// FP64 decisions.  The search runs in FP32 on the contour staged in box-local
+// coordinates (P32, origin (ox, oy), two points per float4; coordinates up to
+// L = the box edge, so each is within 2^-24 L of the exact local value):
+//   pass 1: each lane's smallest FP32 squared distance dmin, chunks of 8
+//           points skipped by all lanes together when their bounding box is
+//           farther from the warp's pixels than every lane's best so far;
+//   pass 2: every vertex whose FP32 distance is within the rounding margin of
+//           dmin (|d32 - d| <= 3 sqrt(d) 2^-24 L + 3e-7 d, taken twice with
+//           room to spare: eps_c = 8 2^-24 L) is measured again in FP64 from
+//           the contour itself (P), in ascending index order with strict <:
+//           the reference's first vertex at the smallest distance.
+// The segment and lambda then follow in FP64 (segment_of_vertex).  A vertex
+// outside the margin is farther than the FP32 minimum's vertex in exact
+// arithmetic, so the FP64 choice is the one the reference makes on this
+// contour.  *wseed: the chunk that held the nearest vertex of the warp's
+// previous tile, searched first.
+constexpr float kFarD = 3.0e38f;
 
-__device__ __forceinline__ int project_warp(const float2* P, const float4* cbb, int asize, int px, int py,
-                                            bool valid, float* out_lambda, int* wseed) {
+__device__ __forceinline__ int project_warp(const float2* P32, const CPoint* P, const float4* cbb, int asize, int px,
+                                            int py, int ox, int oy, float eps_c, bool valid, double* out_lambda,
+                                            int* wseed) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    const float fx = (float)px, fy = (float)py;
+    const float fx = (float)(px - ox), fy = (float)(py - oy);
     const unsigned long long FX = f2_pack(fx, fx), FY = f2_pack(fy, fy);
     const int npts = asize - 1;
     const int nch = (npts + kChunk - 1) / kChunk;
-    const float4* P2 = reinterpret_cast<const float4*>(P);
-    unsigned key = 0xffffffffu;
+    const float4* P2 = reinterpret_cast<const float4*>(P32);
+    float dmin = kFarD;
     auto scan = [&](int ch) {
         const int k0 = ch * kChunk, k1 = min(k0 + kChunk, npts);
         for (int k = k0; k < k1; k += 2) {
@@ -250,29 +256,30 @@ __device__ __forceinline__ int project_warp(const float2* P, const float4* cbb, 
             const unsigned long long DX = f2_sub(FX, f2_pack(v.x, v.z)), DY = f2_sub(FY, f2_pack(v.y, v.w));
             float d0, d1;
             f2_unpack(f2_fma(DY, DY, f2_mul(DX, DX)), d0, d1);
-            key = min(key, (__float_as_uint(d0) & ~kKeyIndexMask) | (unsigned)k);
-            if (k + 1 < k1) key = min(key, (__float_as_uint(d1) & ~kKeyIndexMask) | (unsigned)(k + 1));
+            dmin = fminf(dmin, d0);
+            if (k + 1 < k1) dmin = fminf(dmin, d1);
         }
-    };
-    // an upper bound of the lanes' best squared distances (keys rounded up)
-    auto bound = [&]() {
-        const unsigned up = min(key | kKeyIndexMask, 0x7f7fffffu);
-        return __uint_as_float(__reduce_max_sync(FULL, valid ? up : 0u));
     };
     const int sc = *wseed < nch ? *wseed : 0;
     scan(sc);
-    const int bx0 = __reduce_min_sync(FULL, valid ? px : INT_MAX), bx1 = __reduce_max_sync(FULL, valid ? px : INT_MIN);
-    const int by0 = __reduce_min_sync(FULL, valid ? py : INT_MAX), by1 = __reduce_max_sync(FULL, valid ? py : INT_MIN);
-    float U = bound();
+    const int bx0 = __reduce_min_sync(FULL, valid ? px - ox : INT_MAX);
+    const int bx1 = __reduce_max_sync(FULL, valid ? px - ox : INT_MIN);
+    const int by0 = __reduce_min_sync(FULL, valid ? py - oy : INT_MAX);
+    const int by1 = __reduce_max_sync(FULL, valid ? py - oy : INT_MIN);
+    // squared distance from the warp's pixels to chunk ch's bounding box (a
+    // lower bound of every lane's distance to its points)
+    auto lower = [&](int ch) {
+        const float4 b = cbb[ch];
+        const float gx = fmaxf(fmaxf(b.x - (float)bx1, (float)bx0 - b.y), 0.f);
+        const float gy = fmaxf(fmaxf(b.z - (float)by1, (float)by0 - b.w), 0.f);
+        return gx * gx + gy * gy;
+    };
+    // an upper bound of the valid lanes' values v (non-negative floats)
+    auto wmax = [&](float v) { return __uint_as_float(__reduce_max_sync(FULL, valid ? __float_as_uint(v) : 0u)); };
+    float U = wmax(dmin);
     for (int c0 = 0; c0 < nch; c0 += 32) {
         const int ch = c0 + lane;
-        float lb = 3.0e38f;
-        if (ch < nch) {
-            const float4 b = cbb[ch];
-            const float gx = fmaxf(fmaxf(b.x - (float)bx1, (float)bx0 - b.y), 0.f);
-            const float gy = fmaxf(fmaxf(b.z - (float)by1, (float)by0 - b.w), 0.f);
-            lb = gx * gx + gy * gy;
-        }
+        const float lb = ch < nch ? lower(ch) : kFarD;
         unsigned mask = __ballot_sync(FULL, ch < nch && ch != sc && lb <= U * kBoundSlack);
         while (mask) {
             const int bit = __ffs(mask) - 1;
@@ -280,63 +287,53 @@ __device__ __forceinline__ int project_warp(const float2* P, const float4* cbb, 
             const float lbc = __shfl_sync(FULL, lb, bit);
             if (lbc > U * kBoundSlack) continue;
             scan(c0 + bit);
-            U = bound();
+            U = wmax(dmin);
         }
     }
-    const int nearest = key == 0xffffffffu ? -1 : (int)(key & kKeyIndexMask);
+    // pass 2: the candidates within the margin, in FP64 and index order
+    const float thr = dmin + (sqrtf(dmin) + 1.f) * eps_c + (dmin + 1.f) * 2e-6f;
+    const float T = wmax(thr) * kBoundSlack;
+    const double dpx = (double)px, dpy = (double)py;
+    double best = 1000000.0;  // the reference's initial minDist
+    int nearest = -1;
+    for (int c0 = 0; c0 < nch; c0 += 32) {
+        const int ch = c0 + lane;
+        unsigned mask = __ballot_sync(FULL, ch < nch && lower(ch) <= T);
+        while (mask) {
+            const int bit = __ffs(mask) - 1;
+            mask &= mask - 1;
+            const int k0 = (c0 + bit) * kChunk, k1 = min(k0 + kChunk, npts);
+            for (int k = k0; k < k1; k += 2) {
+                const float4 v = P2[k >> 1];
+                const unsigned long long DX = f2_sub(FX, f2_pack(v.x, v.z)), DY = f2_sub(FY, f2_pack(v.y, v.w));
+                float d0, d1;
+                f2_unpack(f2_fma(DY, DY, f2_mul(DX, DX)), d0, d1);
+                if (valid && d0 <= thr) {
+                    const double ex = dpx - P[k].x, ey = dpy - P[k].y;
+                    const double d = __dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey));
+                    if (d < best) {
+                        best = d;
+                        nearest = k;
+                    }
+                }
+                if (valid && k + 1 < k1 && d1 <= thr) {
+                    const double ex = dpx - P[k + 1].x, ey = dpy - P[k + 1].y;
+                    const double d = __dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey));
+                    if (d < best) {
+                        best = d;
+                        nearest = k + 1;
+                    }
+                }
+            }
+        }
+    }
     {
-        const int src = __ffs(__ballot_sync(FULL, valid)) - 1;
+        const int src = __ffs(__ballot_sync(FULL, valid && nearest >= 0)) - 1;
         const int sn = __shfl_sync(FULL, nearest, src < 0 ? 0 : src);
-        if (sn >= 0) *wseed = sn / kChunk;
+        if (src >= 0) *wseed = sn / kChunk;
     }
-    if (nearest < 0) return 0;
-    float lam_out = 0.f;
-    int seg = nearest;
-    float minDist = 1e30f;
-    {
-        const int next = nearest + 1;
-        const float ux = P[next].x - P[nearest].x, uy = P[next].y - P[nearest].y;
-        float lambda = ((fx - P[nearest].x) * ux + (fy - P[nearest].y) * uy) / (ux * ux + uy * uy);
-        float d;
-        if (lambda < 0) {
-            const float dx = fx - P[nearest].x, dy = fy - P[nearest].y;
-            d = dx * dx + dy * dy;
-        } else if (lambda > 1) {
-            const float dx = P[next].x - fx, dy = P[next].y - fy;
-            d = dx * dx + dy * dy;
-        } else {
-            const float dx = fx - (P[nearest].x + ux * lambda), dy = fy - (P[nearest].y + uy * lambda);
-            d = dx * dx + dy * dy;
-        }
-        if (d < minDist) {
-            seg = nearest;
-            minDist = d;
-            lam_out = lambda;
-        }
-    }
-    const int nb = nearest == 0 ? asize - 1 : nearest;
-    {
-        const int prev = nb - 1;
-        const float ux = P[nb].x - P[prev].x, uy = P[nb].y - P[prev].y;
-        float lambda = ((fx - P[prev].x) * ux + (fy - P[prev].y) * uy) / (ux * ux + uy * uy);
-        float d;
-        if (lambda < 0) {
-            const float dx = fx - P[prev].x, dy = fy - P[prev].y;
-            d = dx * dx + dy * dy;
-        } else if (lambda > 1) {
-            const float dx = P[nb].x - fx, dy = P[nb].y - fy;
-            d = dx * dx + dy * dy;
-        } else {
-            const float dx = fx - (P[prev].x + ux * lambda), dy = fy - (P[prev].y + uy * lambda);
-            d = dx * dx + dy * dy;
-        }
-        if (d < minDist) {
-            seg = prev;
-            lam_out = lambda;
-        }
-    }
-    *out_lambda = fminf(fmaxf(lam_out, 0.f), 1.f);
-    return seg;
+    if (!valid || nearest < 0) return 0;
+    return segment_of_vertex(P, asize, dpx, dpy, nearest, out_lambda);
 }
 
 // kForces: with the stored-energy and / or magnetic driving-force terms.
@@ -361,8 +358,12 @@ __global__ void __launch_bounds__(128, 8) k_corrector_f(NetConst C, NetState* S)
     const Box ib = S->box_prev[g];
     const uint32_t* idl = S->idPrev + S->off_prev[g];
     const bool staged = size <= kCorrMaxPts;
+    // the contour in FP32 coordinates local to the previous box (its points
+    // lie inside it), so the search's rounding is relative to the box edge
+    const int ox = ib.x0, oy = ib.y0;
     if (staged)
-        for (int k = threadIdx.x; k < size; k += blockDim.x) sp[k] = make_float2((float)P[k].x, (float)P[k].y);
+        for (int k = threadIdx.x; k < size; k += blockDim.x)
+            sp[k] = make_float2((float)(P[k].x - ox), (float)(P[k].y - oy));
     __syncthreads();
     if (staged) {
         const int npts = size - 1, nch = (npts + kChunk - 1) / kChunk;
@@ -398,6 +399,9 @@ __global__ void __launch_bounds__(128, 8) k_corrector_f(NetConst C, NetState* S)
     uint32_t st = 0;
     int wseed = 0;
     const bool far_ok = C.gamma_hagb <= 1.0 && C.m_hagb <= 1.0;
+    // rounding margin of the FP32 search (project_warp): 8 2^-24 L, L bounding
+    // every local coordinate of the contour and the pixels
+    const float eps_c = 8.f * 5.9604645e-8f * (float)(max(wi, box_h(ib)) + 2);
     // one warp per 8 x 4 tile; pixels at or below -delta are set to -delta
     for (int t = warp; t < ntiles; t += nwarps) {
         const int x = (t % ntx) * 8 + (lane & 7), y = (t / ntx) * 4 + (lane >> 3);
@@ -441,15 +445,13 @@ __global__ void __launch_bounds__(128, 8) k_corrector_f(NetConst C, NetState* S)
         if (far) out[k] = conv - se;
         const bool need = valid && !far;
         if (__ballot_sync(0xffffffffu, need) == 0u) continue;
-        float lambda = 0.f;
+        double dl = 0;
         int segment;
-        if (staged) {
-            segment = project_warp(sp, cbb, size, j, i, need, &lambda, &wseed);
-        } else {
-            double dl = 0;
+        if (staged)
+            segment = project_warp(sp, P, cbb, size, j, i, ox, oy, eps_c, need, &dl, &wseed);
+        else
             segment = project_to_boundary(P, size, (double)j, (double)i, &dl);
-            lambda = (float)dl;
-        }
+        const float lambda = (float)dl;
         if (!need) continue;
         int sid = -1;
         float interpolator = 0.f;

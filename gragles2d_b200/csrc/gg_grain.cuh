@@ -262,23 +262,16 @@ __device__ __forceinline__ int periodic(int x, int size) {
 __device__ __forceinline__ int wrap_next(int j, int real) { return j + 1 >= real ? j + 1 - real : j + 1; }
 __device__ __forceinline__ int wrap_prev(int j, int real) { return j - 1 < 0 ? j - 1 + real : j - 1; }
 
-// ExplicitGrainBoundary::projectToGrainBondary (src/grainBoundary.cpp:365-447)
-__device__ int project_to_boundary(const CPoint* P, int asize, double px, double py, double* out_lambda) {
-    double minDist = 1000000.0;
-    int minimal_segment = 0;
-    double dist = 0;
-    int nearest = -1;
-    for (int k = 0; k < asize - 1; k++) {
-        dist = len_sqr(px - P[k].x, py - P[k].y);
-        if (dist < minDist) {
-            nearest = k;
-            minDist = dist;
-            minimal_segment = k;
-        }
-    }
+// Second half of ExplicitGrainBoundary::projectToGrainBondary
+// (src/grainBoundary.cpp:383-420): given the nearest vertex, the closer of
+// its two adjacent segments (the following one first, strict <) and the
+// clamped lambda on it.  *out_lambda keeps its value if no segment is closer
+// than 1e6 (as the reference's out_lambda).
+__device__ __forceinline__ int segment_of_vertex(const CPoint* P, int asize, double px, double py, int nearest,
+                                                 double* out_lambda) {
     double lam_out = *out_lambda;
-    if (nearest < 0) return 0;  // fewer than two contour points: nothing to project on
-    minDist = 1000000.0;
+    int minimal_segment = nearest;
+    double minDist = 1000000.0, dist;
     int next = nearest + 1;
     double ux = P[next].x - P[nearest].x, uy = P[next].y - P[nearest].y;
     double lambda = (px - P[nearest].x) * ux + (py - P[nearest].y) * uy;
@@ -315,6 +308,24 @@ __device__ int project_to_boundary(const CPoint* P, int asize, double px, double
     if (lam_out < 0) lam_out = 0;
     *out_lambda = lam_out;
     return minimal_segment;
+}
+
+// ExplicitGrainBoundary::projectToGrainBondary (src/grainBoundary.cpp:365-447):
+// the first vertex at the smallest squared distance (strict <), then
+// segment_of_vertex.
+__device__ int project_to_boundary(const CPoint* P, int asize, double px, double py, double* out_lambda) {
+    double minDist = 1000000.0;
+    double dist = 0;
+    int nearest = -1;
+    for (int k = 0; k < asize - 1; k++) {
+        dist = len_sqr(px - P[k].x, py - P[k].y);
+        if (dist < minDist) {
+            nearest = k;
+            minDist = dist;
+        }
+    }
+    if (nearest < 0) return 0;  // fewer than two contour points: nothing to project on
+    return segment_of_vertex(P, asize, px, py, nearest, out_lambda);
 }
 
 // Junction projection of extractBoundaryAndJunctions (src/grainBoundary.cpp:51-61)
