@@ -41,6 +41,7 @@ WORKLOAD = dict(name="voronoi_20000g_3600_rs15", grains=20000, grid=3600, seed=1
 SMALL = dict(name="voronoi_1000g_800_iso", grains=1000, grid=800, seed=0, iso=1, mobility=0, tpd=0.0)
 CACHE = os.path.join(tempfile.gettempdir(), "gg_bench_cache")
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "gg_ref")
+REF_BIN_FFT = os.path.join(ROOT, "oracle", "_ref", "gg_ref_fft")
 
 
 def rank_info():
@@ -185,7 +186,7 @@ def aggregate_throughput(world: int, updates_per_rank: int, max_ms: float) -> fl
 
 
 def run_ours(args, rank, world, local_rank):
-    from gragles2d_b200 import gg
+    from gragles2d_b200 import accuracy, gg
 
     dist = None
     if world > 1:
@@ -235,17 +236,18 @@ def run_ours(args, rank, world, local_rank):
     upd_e2e = hb.grain_updates()
     st_b = hb.grain_stats()
     areas_b = np.array([s.area if s.state == 1 else np.nan for s in st_b])
-    reg_b = np.array([s.motion_regular for s in st_b])
     h2d = ids.nbytes + euler.nbytes + bbox.nbytes
 
     # ---- device-timed batched steps ----
     hb.step(W)
     u0 = hb.grain_updates()
+    l0, per_step = hb.kernel_launches()
     barrier()
     with ClockSampler(device) as clk:
         ms_b = hb.step(K)
     barrier()
     upd_b = hb.grain_updates() - u0
+    launches = hb.kernel_launches()[0] - l0
     # roofline of the dominant stage
     area, overlap, nex = hb.traffic()
     prof = hb.profile_steps(2)
@@ -263,31 +265,15 @@ def run_ours(args, rank, world, local_rank):
     st_p = hp.grain_stats()
     hp.step(W)
     areas_p = np.array([s.area if s.state == 1 else np.nan for s in st_p])
-    reg_p = np.array([s.motion_regular for s in st_p])
     u0p = hp.grain_updates()
     kp = max(1, min(K, args.plain_steps))
     ms_p = hp.step(kp)
     upd_p = hp.grain_updates() - u0p
     hp.close()
 
-    both = np.isfinite(areas_b) & np.isfinite(areas_p) & (areas_p > 0)
-    rel = np.abs(areas_b - areas_p) / np.where(areas_p > 0, areas_p, 1.0)
-    area_err = float(np.max(rel[both])) if both.any() else None
-    # relative error is only meaningful while a grain has some cells left:
-    # also report it over grains of at least 25 cells in both forms
-    big = both & (areas_p >= 25.0 / (w["grid"] ** 2)) & (areas_b >= 25.0 / (w["grid"] ** 2))
-    area_err_big = float(np.max(rel[big])) if big.any() else None
-    px = 1.0 / (w["grid"] ** 2)  # area of one grid cell in domain units
-    worst = [int(i) for i in np.argsort(np.where(both, rel, -1))[::-1][:5]]
-    area_diag = {"grains_compared": int(both.sum()),
-                 "alive_only_plain": int((np.isfinite(areas_p) & ~np.isfinite(areas_b)).sum()),
-                 "alive_only_batched": int((np.isfinite(areas_b) & ~np.isfinite(areas_p)).sum()),
-                 "p50": float(np.median(rel[both])), "p99": float(np.quantile(rel[both], 0.99)),
-                 "over_1e-3": int((rel[both] > 1e-3).sum()),
-                 "max_abs_px": float(np.max(np.abs(areas_b - areas_p)[both]) / px) if both.any() else None,
-                 "worst": [{"id": i + 1, "area_px_plain": float(areas_p[i] / px),
-                            "area_px_batched": float(areas_b[i] / px), "rel": float(rel[i]),
-                            "regular_plain": int(reg_p[i]), "regular_batched": int(reg_b[i])} for i in worst]}
+    # every grain alive in both forms, no size cut
+    area_diag = accuracy.area_errors(areas_p, areas_b, 1.0 / (w["grid"] ** 2))
+    area_err = area_diag.get("max")
 
     # ---- max over ranks ----
     t_ms, t_e2e = max_over_ranks([ms_b, t_e2e], dist, f"cuda:{device}")
@@ -324,9 +310,10 @@ def run_ours(args, rank, world, local_rank):
         "config": workload_config(w, world),
         "e2e": {"value": aggregate_throughput(world, upd_e2e, t_e2e * 1e3), "unit": METRIC, "h2d_bytes_per_step": h2d / K,
                 "d2h_bytes_per_step": stats_bytes / K,
-                "includes": "context creation, load from host buffers, distance initialisation, neighbour search, "
-                            "K steps each with a read of all grain statistics (after an untimed warm-up pass of "
-                            "the same calls with W steps)"},
+                "includes": "context set-up on the device, load from host buffers, distance initialisation, "
+                            "neighbour search, K steps each with a read of all grain statistics (after an untimed "
+                            "warm-up pass of the same calls with W steps, so CUDA context creation and module "
+                            "loading are not in it)"},
         "roofline": {"bound": "hbm", "kernel": kernel_names.get(dom, dom), "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
@@ -335,26 +322,38 @@ def run_ours(args, rank, world, local_rank):
         "plain_fp64": {"value": upd_p / (ms_p / 1e3), "ms_per_step": ms_p / kp, "steps": kp},
         "batched_vs_plain": (upd_b / (t_ms / 1e3)) / (upd_p / (ms_p / 1e3)),
         "area_rel_err_max": area_err,
-        "area_rel_err_max_ge_25px": area_err_big,
-        "area_err_detail": area_diag,
+        "area_err_detail": {"steps": K, **area_diag},
         "clocks": clk.summary(),
-        # per step: second-order lists, convolution, corrector (anisotropic),
-        # comparison, level set, arena allocation, neighbours, redistancing
-        # (large-box bin and the rest), end of step, work queue
-        "gpu_launches": (11 if aniso else 10) * K,
+        # kernel nodes of the captured step graph (counted by the library
+        # when it captured the graph) times the timed replays
+        "gpu_launches": launches,
+        "gpu_launches_per_step": per_step,
         "status": status_b,
     }
+    if world == 1 and not args.no_accuracy:
+        rows = accuracy.trajectory(xml, args.accuracy_steps, 50, device=device, inputs=(ids, euler, bbox))
+        keys = ("max", "p99", "over_1e-3", "compared")
+        out["accuracy_run"] = {
+            "workload": f"the same network, {args.accuracy_steps} steps of both forms from the same input "
+                        "(outside the timed region)",
+            "fp64_perturbed": "plain FP64 with every boundary energy scaled by 1 - 2^-46 (sensitivity floor)",
+            "every_50_steps": [{"step": r["step"], "fp32": {k: r["fp32"].get(k) for k in keys},
+                                "fp64_perturbed": {k: r["fp64_perturbed"].get(k) for k in keys}} for r in rows]}
     if not args.no_gradient:
         out["gradient"] = gradient_check(device)
     if not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(xml, args.cpu_steps)
+        out["cpu_baseline"] = cpu_baseline(xml, 1, args.cpu_steps)
     return out
 
 
-def cpu_baseline(xml: str, steps: int) -> dict:
-    """The reference's OpenMP path (oracle/_ref/gg_ref) on the host cores, on a
-    bounded sample of the same workload (its first `steps` timesteps)."""
-    if not os.path.exists(REF_BIN):
+def cpu_baseline(xml: str, warmup: int, steps: int) -> dict:
+    """The reference's OpenMP path on the host cores (all of them), on a
+    bounded sample of the same workload: loop 0 (the reference runs no
+    corrector there), `warmup` untimed loops, then `steps` timed loops; the
+    throughput is their grains over their summed loop times (the harness
+    times every loop of run_sim's body, src/grainhdl.cpp:1049-1142)."""
+    binary = REF_BIN_FFT if os.path.exists(REF_BIN_FFT) else REF_BIN
+    if not os.path.exists(binary):
         return {"value": None, "unit": METRIC, "cores": os.cpu_count(), "kind": "reference",
                 "sample": "unavailable: oracle/_ref/gg_ref not built"}
     d = tempfile.mkdtemp(prefix="gg_ref_")
@@ -365,35 +364,40 @@ def cpu_baseline(xml: str, steps: int) -> dict:
     txt = open(xml).read()
     import re
 
-    txt = re.sub(r"<NumberOfTimesteps>[^<]*</NumberOfTimesteps>", f"<NumberOfTimesteps> {steps - 1} </NumberOfTimesteps>",
+    total = 1 + warmup + steps  # loops 0 .. total - 1
+    txt = re.sub(r"<NumberOfTimesteps>[^<]*</NumberOfTimesteps>", f"<NumberOfTimesteps> {total - 1} </NumberOfTimesteps>",
                  txt)
     os.remove(os.path.join(d, name))
     open(os.path.join(d, name), "w").write(txt)
     env = dict(os.environ)
     cores = os.cpu_count() or 1
     env["OMP_NUM_THREADS"] = str(cores)
-    out = subprocess.run([REF_BIN, name, "-", "0", "1"], cwd=d, capture_output=True, text=True, env=env,
+    out = subprocess.run([binary, name, "-", "0", "1"], cwd=d, capture_output=True, text=True, env=env,
                          timeout=1800)
     shutil.rmtree(d, ignore_errors=True)
     info = json.loads(out.stdout.strip().splitlines()[-1])
-    return {"value": info["grain_updates"] / info["loop_s"], "unit": METRIC, "cores": info["threads"],
-            "kind": "reference",
-            "sample": f"first {info['steps']} timesteps of the same workload (reference + shim FFT, "
-                      f"{info['grain_updates']} grain-updates in {info['loop_s']:.2f} s; init excluded)"}
+    secs = info["step_s"][1 + warmup:]
+    grains = info["step_grains"][1 + warmup:]
+    fft = "O(n log n) mixed-radix / Bluestein FFT shim" if binary == REF_BIN_FFT else "direct-DFT FFT shim"
+    return {"value": sum(grains) / sum(secs), "unit": METRIC, "cores": info["threads"], "kind": "reference",
+            "steps": len(secs), "warmup": warmup,
+            "sample": f"loops {1 + warmup}..{total - 1} of the same workload after loop 0 and {warmup} warm-up "
+                      f"loops ({sum(grains)} grain-updates in {sum(secs):.2f} s; initialisation excluded); "
+                      f"the reference's C++ built with -O3 -fopenmp and the {fft} standing in for FFTW3"}
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return None
     xml, w = workload_case(WORKLOAD)
-    # a bounded sample: the reference needs seconds per step of this workload
-    steps = min(args.warmup + args.steps, args.ref_max_steps)
-    cb = cpu_baseline(xml, steps)
+    # whole steps of the workload; the reference needs a second or more per step
+    steps = max(1, min(args.steps, args.ref_max_steps))
+    cb = cpu_baseline(xml, args.warmup, steps)
     if cb["value"] is None:
         return {"impl": "reference", "unavailable": cb["sample"]}
     v = cb["value"]
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "steps": cb["steps"], "warmup": cb["warmup"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(w, world),
             "cpu_baseline": cb,
@@ -494,7 +498,9 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-gradient", action="store_true", help="skip the parameter-derivative check")
-    ap.add_argument("--ref-max-steps", type=int, default=6)
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the whole-run area-error comparison")
+    ap.add_argument("--accuracy-steps", type=int, default=500)
+    ap.add_argument("--ref-max-steps", type=int, default=40)
     ap.add_argument("--profile-case", action="store_true", help="small stage-by-stage run for ncu captures")
     ap.add_argument("--profile-plain", action="store_true")
     args = ap.parse_args()

@@ -176,22 +176,13 @@ size_t conv_sep_smem(int tmax) {
 }
 
 // Batched-form corrector: same sectors as k_corrector (built by one warp),
-// with the previous contour staged in shared memory (FP32 coordinates) and
-// the per-pixel work in FP32.  Each warp takes one 8 x 4 tile of the box at a
-// time, so its 32 pixels lie close together and the warp prunes the
-// nearest-vertex search as one: chunks of 8 contour points whose bounding box
-// is farther from the tile than every lane's best point so far are skipped
-// by all lanes together.
-constexpr int kCorrMaxPts = 512;
+// with the previous contour staged in shared memory (FP32 box-local
+// coordinates) and the per-pixel work in FP32, except the discrete decisions
+// of the projection, which follow the reference's FP64 arithmetic.  Each
+// warp takes one 8 x 4 tile of the box at a time.
+constexpr int kCorrMaxPts = 512;  // contours staged in FP32 up to this length
 
-constexpr int kChunk = 8;  // contour points per bounding box of the nearest-vertex search
-
-// Slack on the chunk bound so that a box distance which rounds a little
-// above an equal point distance does not drop the chunk (ties matter).
-constexpr float kBoundSlack = 1.0000005f;
-
-// Packed FP32 pairs (sm_100 f32x2 arithmetic): two contour points per
-// instruction in the nearest-vertex scan.
+// Packed FP32 pairs (sm_100 f32x2 arithmetic).
 __device__ __forceinline__ unsigned long long f2_pack(float a, float b) {
     unsigned long long r;
     asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
@@ -200,145 +191,213 @@ __device__ __forceinline__ unsigned long long f2_pack(float a, float b) {
 __device__ __forceinline__ void f2_unpack(unsigned long long v, float& a, float& b) {
     asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
 }
-__device__ __forceinline__ unsigned long long f2_sub(unsigned long long a, unsigned long long b) {
-    unsigned long long r;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-__device__ __forceinline__ unsigned long long f2_mul(unsigned long long a, unsigned long long b) {
-    unsigned long long r;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-__device__ __forceinline__ unsigned long long f2_fma(unsigned long long a, unsigned long long b,
-                                                     unsigned long long c) {
-    unsigned long long r;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
-    return r;
+
+// Nearest contour vertex of projectToGrainBondary (src/grainBoundary.cpp:
+// 365-381) through a uniform grid of cells over the previous box: the
+// vertices are bucketed by cell (counting sort in shared memory), and a pixel
+// measures, in FP64 from the contour itself, the vertices of the 3 x 3 cells
+// around its own.  Every vertex within `cell` of the pixel lies in that
+// window, so when the smallest distance found is at most (cell - 1e-3)^2 (the
+// margin covers the cell index of a vertex on a cell edge) it is the smallest
+// over the whole contour; ties go to the lowest index, as the reference's
+// strict < over ascending k.  Otherwise the pixel scans every vertex.
+constexpr int kCellMax = 24;          // cells per side
+constexpr int kBucketPts = kCorrMaxPts;  // vertices bucketed (the staged contours)
+struct VertexBuckets {
+    int ncx, ncy, cell;
+    int end[kCellMax * kCellMax + 1];  // after the fill: end[c + 1] = first vertex of cell c
+    short list[kBucketPts];
+};
+
+__device__ __forceinline__ int bucket_of(const VertexBuckets& B, double lx, double ly) {
+    int cx = (int)floor(lx / B.cell), cy = (int)floor(ly / B.cell);
+    cx = cx < 0 ? 0 : (cx >= B.ncx ? B.ncx - 1 : cx);
+    cy = cy < 0 ? 0 : (cy >= B.ncy ? B.ncy - 1 : cy);
+    return cy * B.ncx + cx;
 }
 
-// projectToGrainBondary (src/grainBoundary.cpp:365-447) for the pixels
-// (px, py) of the 32 lanes of a warp (all lanes call it; `valid` lanes are
-// the warp's real pixels, the others only follow along), with the reference's
-// FP64 decisions.  The search runs in FP32 on the contour staged in box-local
-// coordinates (P32, origin (ox, oy), two points per float4; coordinates up to
-// L = the box edge, so each is within 2^-24 L of the exact local value):
-//   pass 1: each lane's smallest FP32 squared distance dmin, chunks of 8
-//           points skipped by all lanes together when their bounding box is
-//           farther from the warp's pixels than every lane's best so far;
-//   pass 2: every vertex whose FP32 distance is within the rounding margin of
-//           dmin (|d32 - d| <= 3 sqrt(d) 2^-24 L + 3e-7 d, taken twice with
-//           room to spare: eps_c = 8 2^-24 L) is measured again in FP64 from
-//           the contour itself (P), in ascending index order with strict <:
-//           the reference's first vertex at the smallest distance.
-// The segment and lambda then follow in FP64 (segment_of_vertex).  A vertex
-// outside the margin is farther than the FP32 minimum's vertex in exact
-// arithmetic, so the FP64 choice is the one the reference makes on this
-// contour.  *wseed: the chunk that held the nearest vertex of the warp's
-// previous tile, searched first.
-constexpr float kFarD = 3.0e38f;
-
-__device__ __forceinline__ int project_warp(const float2* P32, const CPoint* P, const float4* cbb, int asize, int px,
-                                            int py, int ox, int oy, float eps_c, bool valid, double* out_lambda,
-                                            int* wseed) {
-    const unsigned FULL = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    const float fx = (float)(px - ox), fy = (float)(py - oy);
-    const unsigned long long FX = f2_pack(fx, fx), FY = f2_pack(fy, fy);
-    const int npts = asize - 1;
-    const int nch = (npts + kChunk - 1) / kChunk;
-    const float4* P2 = reinterpret_cast<const float4*>(P32);
-    float dmin = kFarD;
-    auto scan = [&](int ch) {
-        const int k0 = ch * kChunk, k1 = min(k0 + kChunk, npts);
-        for (int k = k0; k < k1; k += 2) {
-            const float4 v = P2[k >> 1];
-            const unsigned long long DX = f2_sub(FX, f2_pack(v.x, v.z)), DY = f2_sub(FY, f2_pack(v.y, v.w));
-            float d0, d1;
-            f2_unpack(f2_fma(DY, DY, f2_mul(DX, DX)), d0, d1);
-            dmin = fminf(dmin, d0);
-            if (k + 1 < k1) dmin = fminf(dmin, d1);
-        }
-    };
-    const int sc = *wseed < nch ? *wseed : 0;
-    scan(sc);
-    const int bx0 = __reduce_min_sync(FULL, valid ? px - ox : INT_MAX);
-    const int bx1 = __reduce_max_sync(FULL, valid ? px - ox : INT_MIN);
-    const int by0 = __reduce_min_sync(FULL, valid ? py - oy : INT_MAX);
-    const int by1 = __reduce_max_sync(FULL, valid ? py - oy : INT_MIN);
-    // squared distance from the warp's pixels to chunk ch's bounding box (a
-    // lower bound of every lane's distance to its points)
-    auto lower = [&](int ch) {
-        const float4 b = cbb[ch];
-        const float gx = fmaxf(fmaxf(b.x - (float)bx1, (float)bx0 - b.y), 0.f);
-        const float gy = fmaxf(fmaxf(b.z - (float)by1, (float)by0 - b.w), 0.f);
-        return gx * gx + gy * gy;
-    };
-    // an upper bound of the valid lanes' values v (non-negative floats)
-    auto wmax = [&](float v) { return __uint_as_float(__reduce_max_sync(FULL, valid ? __float_as_uint(v) : 0u)); };
-    float U = wmax(dmin);
-    for (int c0 = 0; c0 < nch; c0 += 32) {
-        const int ch = c0 + lane;
-        const float lb = ch < nch ? lower(ch) : kFarD;
-        unsigned mask = __ballot_sync(FULL, ch < nch && ch != sc && lb <= U * kBoundSlack);
-        while (mask) {
-            const int bit = __ffs(mask) - 1;
-            mask &= mask - 1;
-            const float lbc = __shfl_sync(FULL, lb, bit);
-            if (lbc > U * kBoundSlack) continue;
-            scan(c0 + bit);
-            U = wmax(dmin);
+// All threads: buckets of the vertices 0 .. npts-1 (P[k] in grid
+// coordinates, origin (ox, oy)).  Ends with a barrier.
+__device__ void build_buckets(VertexBuckets& B, const CPoint* P, int npts, int ox, int oy, int wi, int hi) {
+    const int cs = max(4, (max(wi, hi) + kCellMax - 1) / kCellMax);
+    const int ncx = (wi + cs - 1) / cs, ncy = (hi + cs - 1) / cs, nc = ncx * ncy;
+    if (threadIdx.x == 0) {
+        B.ncx = ncx;
+        B.ncy = ncy;
+        B.cell = cs;
+    }
+    for (int c = threadIdx.x; c <= nc; c += blockDim.x) B.end[c] = 0;
+    __syncthreads();
+    for (int k = threadIdx.x; k < npts; k += blockDim.x)
+        atomicAdd(&B.end[bucket_of(B, P[k].x - ox, P[k].y - oy) + 1], 1);
+    __syncthreads();
+    if (threadIdx.x < 32) {  // inclusive scan of the counts by one warp
+        int carry = 0;
+        for (int c0 = 1; c0 <= nc; c0 += 32) {
+            const int c = c0 + (int)threadIdx.x;
+            int v = c <= nc ? B.end[c] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, v, o);
+                if ((int)threadIdx.x >= o) v += u;
+            }
+            if (c <= nc) B.end[c] = v + carry;
+            carry += __shfl_sync(0xffffffffu, v, 31);
         }
     }
-    // pass 2: the candidates within the margin, in FP64 and index order
-    const float thr = dmin + (sqrtf(dmin) + 1.f) * eps_c + (dmin + 1.f) * 2e-6f;
-    const float T = wmax(thr) * kBoundSlack;
-    const double dpx = (double)px, dpy = (double)py;
-    double best = 1000000.0;  // the reference's initial minDist
-    int nearest = -1;
-    for (int c0 = 0; c0 < nch; c0 += 32) {
-        const int ch = c0 + lane;
-        unsigned mask = __ballot_sync(FULL, ch < nch && lower(ch) <= T);
-        while (mask) {
-            const int bit = __ffs(mask) - 1;
-            mask &= mask - 1;
-            const int k0 = (c0 + bit) * kChunk, k1 = min(k0 + kChunk, npts);
-            for (int k = k0; k < k1; k += 2) {
-                const float4 v = P2[k >> 1];
-                const unsigned long long DX = f2_sub(FX, f2_pack(v.x, v.z)), DY = f2_sub(FY, f2_pack(v.y, v.w));
-                float d0, d1;
-                f2_unpack(f2_fma(DY, DY, f2_mul(DX, DX)), d0, d1);
-                if (valid && d0 <= thr) {
-                    const double ex = dpx - P[k].x, ey = dpy - P[k].y;
-                    const double d = __dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey));
-                    if (d < best) {
-                        best = d;
-                        nearest = k;
-                    }
-                }
-                if (valid && k + 1 < k1 && d1 <= thr) {
-                    const double ex = dpx - P[k + 1].x, ey = dpy - P[k + 1].y;
-                    const double d = __dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey));
-                    if (d < best) {
-                        best = d;
-                        nearest = k + 1;
-                    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < npts; k += blockDim.x) {
+        const int pos = atomicSub(&B.end[bucket_of(B, P[k].x - ox, P[k].y - oy) + 1], 1) - 1;
+        B.list[pos] = (short)k;
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ double dist2_rn(double px, double py, const CPoint& q) {
+    const double ex = px - q.x, ey = py - q.y;
+    return __dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey));
+}
+
+__device__ __forceinline__ float tie_margin(float d, float eps_c) { return (sqrtf(d) + 1.f) * eps_c + d * 1e-6f; }
+
+constexpr unsigned kKeyIndexBits = 9;
+constexpr unsigned kKeyIndexMask = (1u << kKeyIndexBits) - 1u;
+static_assert(kBucketPts <= (1 << kKeyIndexBits), "vertex index must fit the key");
+
+// The reference's nearest vertex of the pixels (px, py) of the 32 lanes of a
+// warp (grid coordinates; all lanes call it, `need` lanes are the pixels
+// that want it).  The lanes scan together the vertices of the union of their
+// 3 x 3 cell windows in FP32 on the staged box-local contour P32 (each
+// coordinate within 2^-24 L of the exact local value, L the box edge, so a
+// squared distance d within 3 sqrt(d) 2^-24 L + 3e-7 d of the exact one):
+// each candidate is one 32-bit key, the distance's bits with the low 9
+// replaced by the vertex index, and a lane keeps its smallest key k1 and the
+// second smallest k2.  A lane whose two best lie within twice the rounding
+// bound (tie_margin with eps_c = 8 2^-24 L; the keys' truncation taken on
+// both sides) measures the candidates within that margin again in FP64 from
+// the contour itself, lowest index first at equal distance.  A lane whose
+// best distance exceeds (cell - 1e-3)^2 scans every vertex in FP64 (a vertex
+// within `cell` of the pixel lies in its window).
+__device__ int nearest_vertex_warp(const VertexBuckets& B, const float2* P32, const CPoint* P, int npts, int px,
+                                   int py, int ox, int oy, float eps_c, bool need) {
+    const unsigned FULL = 0xffffffffu;
+    const int cs = B.cell;
+    const int lx = px - ox, ly = py - oy;
+    const int cx = min(max(lx / cs, 0), B.ncx - 1), cy = min(max(ly / cs, 0), B.ncy - 1);
+    const int ux0 = max(__reduce_min_sync(FULL, need ? cx : INT_MAX) - 1, 0);
+    const int ux1 = min(__reduce_max_sync(FULL, need ? cx : INT_MIN) + 1, B.ncx - 1);
+    const int uy0 = max(__reduce_min_sync(FULL, need ? cy : INT_MAX) - 1, 0);
+    const int uy1 = min(__reduce_max_sync(FULL, need ? cy : INT_MIN) + 1, B.ncy - 1);
+    const float fx = (float)lx, fy = (float)ly;
+    unsigned k1 = 0xffffffffu, k2 = 0xffffffffu;
+    const int ncell = B.ncx * B.ncy;
+    for (int yy = uy0; yy <= uy1; ++yy) {
+        // cells ux0 .. ux1 of a row are consecutive in the list
+        const int q0 = B.end[yy * B.ncx + ux0 + 1];
+        const int cl = yy * B.ncx + ux1;
+        const int q1 = cl + 1 < ncell ? B.end[cl + 2] : npts;
+        for (int q = q0; q < q1; ++q) {
+            const int k = B.list[q];
+            const float2 v = P32[k];
+            const float dx = fx - v.x, dy = fy - v.y;
+            const float d = fmaf(dy, dy, dx * dx);
+            const unsigned key = (__float_as_uint(d) & ~kKeyIndexMask) | (unsigned)k;
+            k2 = min(k2, max(k1, key));
+            k1 = min(k1, key);
+        }
+    }
+    if (!need) return -1;
+    const float d1 = __uint_as_float(min(k1 | kKeyIndexMask, 0x7f7fffffu));
+    const float r = (float)cs - 1e-3f;
+    const bool covered = k1 != 0xffffffffu && d1 <= r * r;
+    const float thr = d1 + tie_margin(d1, eps_c);
+    const bool tie = covered && k2 != 0xffffffffu && __uint_as_float(k2 & ~kKeyIndexMask) <= thr;
+    int nearest = (int)(k1 & kKeyIndexMask);
+    if (!covered) {
+        const double dpx = (double)px, dpy = (double)py;
+        double best = 1000000.0;  // the reference's initial minDist
+        nearest = -1;
+        for (int k = 0; k < npts; ++k) {
+            const double d = dist2_rn(dpx, dpy, P[k]);
+            if (d < best) {
+                best = d;
+                nearest = k;
+            }
+        }
+    } else if (tie) {
+        const double dpx = (double)px, dpy = (double)py;
+        double best = 1000000.0;
+        nearest = -1;
+        for (int yy = max(cy - 1, 0); yy <= min(cy + 1, B.ncy - 1); ++yy) {
+            const int q0 = B.end[yy * B.ncx + max(cx - 1, 0) + 1];
+            const int cl = yy * B.ncx + min(cx + 1, B.ncx - 1);
+            const int q1 = cl + 1 < ncell ? B.end[cl + 2] : npts;
+            for (int q = q0; q < q1; ++q) {
+                const int k = B.list[q];
+                const float dx = fx - P32[k].x, dy = fy - P32[k].y;
+                if (fmaf(dy, dy, dx * dx) > thr) continue;
+                const double d = dist2_rn(dpx, dpy, P[k]);
+                if (d < best || (d == best && k < nearest)) {
+                    best = d;
+                    nearest = k;
                 }
             }
         }
     }
-    {
-        const int src = __ffs(__ballot_sync(FULL, valid && nearest >= 0)) - 1;
-        const int sn = __shfl_sync(FULL, nearest, src < 0 ? 0 : src);
-        if (src >= 0) *wseed = sn / kChunk;
-    }
-    if (!valid || nearest < 0) return 0;
-    return segment_of_vertex(P, asize, dpx, dpy, nearest, out_lambda);
+    return nearest;
 }
 
-// kForces: with the stored-energy and / or magnetic driving-force terms.
+// Distance from (fx, fy) to segment a -> b (the reference's three cases);
+// *lam receives the unclamped projection parameter.
+__device__ __forceinline__ float seg_dist32(float2 a, float2 b, float fx, float fy, float* lam) {
+    const float ux = b.x - a.x, uy = b.y - a.y;
+    const float l = ((fx - a.x) * ux + (fy - a.y) * uy) / (ux * ux + uy * uy);
+    float dx, dy;
+    if (l < 0) {
+        dx = fx - a.x;
+        dy = fy - a.y;
+    } else if (l > 1) {
+        dx = b.x - fx;
+        dy = b.y - fy;
+    } else {
+        dx = fx - (a.x + ux * l);
+        dy = fy - (a.y + uy * l);
+    }
+    *lam = l;
+    return dx * dx + dy * dy;
+}
+
+// The segment step of projectToGrainBondary (src/grainBoundary.cpp:383-420)
+// on the FP32 local contour P32: the segment after the vertex first, the one
+// before it wins only if strictly closer.  When both projections fall beyond
+// the vertex, both distances are the vertex's (equal in FP64 too) and the
+// segment after it wins with lambda 0; when the two distances lie within the
+// FP32 rounding margin (eps_c = 8 2^-24 L, L bounding the local coordinates)
+// the step is taken again in FP64 from the contour itself.
+__device__ __forceinline__ int segment_step(const float2* P32, const CPoint* P, int asize, int px, int py, int ox,
+                                           int oy, float eps_c, int nearest, float* out_lambda) {
+    const float fx = (float)(px - ox), fy = (float)(py - oy);
+    float la, lb;
+    const float da = seg_dist32(P32[nearest], P32[nearest + 1], fx, fy, &la);
+    const int nv = nearest == 0 ? asize - 1 : nearest;
+    const float db = seg_dist32(P32[nv - 1], P32[nv], fx, fy, &lb);
+    if (la <= 0.f && lb >= 1.f) {
+        *out_lambda = 0.f;
+        return nearest;
+    }
+    if (fabsf(da - db) <= 4.f * tie_margin(fminf(da, db), eps_c)) {
+        double dl = 0;
+        const int seg = segment_of_vertex(P, asize, (double)px, (double)py, nearest, &dl);
+        *out_lambda = (float)dl;
+        return seg;
+    }
+    const bool before = db < da;
+    const float lam = before ? lb : la;
+    *out_lambda = fminf(fmaxf(lam, 0.f), 1.f);
+    return before ? nv - 1 : nearest;
+}
+
 template <bool kForces>
-__global__ void __launch_bounds__(128, 8) k_corrector_f(NetConst C, NetState* S) {
+__global__ void __launch_bounds__(128, 7) k_corrector_f(NetConst C, NetState* S) {
     const int g = grain_at(S, blockIdx.x);
     if (g > C.N || C.state[g] != G_EXISTS || C.regular[g] == 0 || S->loop == 0 || halted(S)) return;
     __shared__ SectorSet sec;
@@ -347,7 +406,7 @@ __global__ void __launch_bounds__(128, 8) k_corrector_f(NetConst C, NetState* S)
     __shared__ uint32_t s_st;
     __shared__ double s_per;
     __shared__ NbTable nbt;
-    __shared__ float4 cbb[kCorrMaxPts / kChunk];
+    __shared__ VertexBuckets vb;
     __shared__ double s_seg[kSegShared];
     __shared__ SegTable stab;
     __shared__ int jl[64], jr[64];
@@ -364,20 +423,7 @@ __global__ void __launch_bounds__(128, 8) k_corrector_f(NetConst C, NetState* S)
     if (staged)
         for (int k = threadIdx.x; k < size; k += blockDim.x)
             sp[k] = make_float2((float)(P[k].x - ox), (float)(P[k].y - oy));
-    __syncthreads();
-    if (staged) {
-        const int npts = size - 1, nch = (npts + kChunk - 1) / kChunk;
-        for (int ch = threadIdx.x; ch < nch; ch += blockDim.x) {
-            float4 b = make_float4(3.0e38f, -3.0e38f, 3.0e38f, -3.0e38f);
-            for (int k = ch * kChunk; k < min(ch * kChunk + kChunk, npts); ++k) {
-                b.x = fminf(b.x, sp[k].x);
-                b.y = fmaxf(b.y, sp[k].x);
-                b.z = fminf(b.z, sp[k].y);
-                b.w = fmaxf(b.w, sp[k].y);
-            }
-            cbb[ch] = b;
-        }
-    }
+    if (staged) build_buckets(vb, P, size - 1, ox, oy, box_w(ib), box_h(ib));
     prepare_sectors(C, S, g, P, size, seg, sec, jw, &s_st, &s_per, nbt, jl, jr);
     const bool tabled = size - 1 <= kSegTable;
     if (tabled) build_seg_table(sec, seg, size, stab);
@@ -397,10 +443,9 @@ __global__ void __launch_bounds__(128, 8) k_corrector_f(NetConst C, NetState* S)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const int ntx = (w + 7) >> 3, ntiles = ntx * ((hgt + 3) >> 2);
     uint32_t st = 0;
-    int wseed = 0;
     const bool far_ok = C.gamma_hagb <= 1.0 && C.m_hagb <= 1.0;
-    // rounding margin of the FP32 search (project_warp): 8 2^-24 L, L bounding
-    // every local coordinate of the contour and the pixels
+    // rounding margin of the FP32 segment step: 8 2^-24 L, L bounding every
+    // local coordinate of the contour and the pixels
     const float eps_c = 8.f * 5.9604645e-8f * (float)(max(wi, box_h(ib)) + 2);
     // one warp per 8 x 4 tile; pixels at or below -delta are set to -delta
     for (int t = warp; t < ntiles; t += nwarps) {
@@ -445,14 +490,18 @@ __global__ void __launch_bounds__(128, 8) k_corrector_f(NetConst C, NetState* S)
         if (far) out[k] = conv - se;
         const bool need = valid && !far;
         if (__ballot_sync(0xffffffffu, need) == 0u) continue;
-        double dl = 0;
-        int segment;
-        if (staged)
-            segment = project_warp(sp, P, cbb, size, j, i, ox, oy, eps_c, need, &dl, &wseed);
-        else
+        float lambda = 0.f;
+        int segment = 0;
+        if (staged) {
+            const int nv = nearest_vertex_warp(vb, sp, P, size - 1, j, i, ox, oy, eps_c, need);
+            if (!need) continue;
+            if (nv >= 0) segment = segment_step(sp, P, size, j, i, ox, oy, eps_c, nv, &lambda);
+        } else {
+            if (!need) continue;
+            double dl = 0;
             segment = project_to_boundary(P, size, (double)j, (double)i, &dl);
-        const float lambda = (float)dl;
-        if (!need) continue;
+            lambda = (float)dl;
+        }
         int sid = -1;
         float interpolator = 0.f;
         if (tabled) {

@@ -70,6 +70,8 @@ struct gg_ctx {
     LaunchCfg cfg{256, 256, 128, 64};
 
     cudaGraphExec_t graph = nullptr;
+    int32_t graph_kernels = 0;     // kernel nodes of the captured step graph
+    int64_t kernel_launches = 0;   // graph_kernels per replay, summed
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaStream_t stream2 = nullptr;  // second branch of the captured batched step
     cudaEvent_t fork[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -1401,13 +1403,25 @@ int gg_step(gg_ctx* c, int32_t loop, int32_t nsteps) {
             cudaError_t e2 = cudaStreamEndCapture(c->stream, &gr);
             if (e != cudaSuccess) return cuda_fail(c, e, "capture");
             if (e2 != cudaSuccess) return cuda_fail(c, e2, "end capture");
-            e = cudaGraphInstantiate(&c->graph, gr, 0);
+            size_t nn = 0;
+            e = cudaGraphGetNodes(gr, nullptr, &nn);
+            std::vector<cudaGraphNode_t> nodes(nn);
+            if (e == cudaSuccess && nn) e = cudaGraphGetNodes(gr, nodes.data(), &nn);
+            int32_t kn = 0;
+            for (size_t q = 0; q < nn && e == cudaSuccess; ++q) {
+                cudaGraphNodeType t;
+                e = cudaGraphNodeGetType(nodes[q], &t);
+                if (t == cudaGraphNodeTypeKernel) ++kn;
+            }
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&c->graph, gr, 0);
             cudaGraphDestroy(gr);
             if (e != cudaSuccess) return cuda_fail(c, e, "graph instantiate");
+            c->graph_kernels = kn;
         }
         GG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
         for (int s = 0; s < nsteps; ++s) GG_CUDA(c, cudaGraphLaunch(c->graph, c->stream));
         GG_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+        c->kernel_launches += (int64_t)nsteps * c->graph_kernels;
     } else {
         GG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
         for (int s = 0; s < nsteps; ++s) {
@@ -1479,6 +1493,13 @@ int gg_traffic(gg_ctx* c, int64_t* sum_area, int64_t* sum_overlap, int32_t* n_ex
     if (sum_area) *sum_area = (int64_t)c->hS.t_area;
     if (sum_overlap) *sum_overlap = (int64_t)c->hS.t_overlap;
     if (n_exists) *n_exists = (int32_t)c->hS.t_exists;
+    return GG_OK;
+}
+
+int gg_kernel_launches(gg_ctx* c, int64_t* total, int32_t* per_step) {
+    if (!c || !total) return GG_E_INVALID;
+    *total = c->kernel_launches;
+    if (per_step) *per_step = c->graph_kernels;
     return GG_OK;
 }
 

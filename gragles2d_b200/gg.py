@@ -30,7 +30,7 @@ EXPORTS = (
     "gg_convolution", "gg_update_second_order_neighbors", "gg_comparison", "gg_level_set", "gg_redistancing",
     "gg_grain_count", "gg_step", "gg_status", "gg_read_grain_stats", "gg_tangent_enable", "gg_read_area_tangents",
     "gg_write_analysis", "gg_write_restart", "gg_dims", "gg_dump", "gg_last_step_ms",
-    "gg_grain_updates", "gg_profile_steps", "gg_traffic", "gg_convolve_box_static",
+    "gg_grain_updates", "gg_profile_steps", "gg_traffic", "gg_kernel_launches", "gg_convolve_box_static",
 )
 STATIC_CONV_MAX_N = 128
 NSTAGES = 9
@@ -126,6 +126,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "gg_grain_updates": (I, [V, P(ctypes.c_int64)]),
         "gg_profile_steps": (I, [V, I, I, P(D)]),
         "gg_traffic": (I, [V, P(ctypes.c_int64), P(ctypes.c_int64), P(I)]),
+        "gg_kernel_launches": (I, [V, P(ctypes.c_int64), P(I)]),
         "gg_convolve_box_static": (I, [V, V, I, D, I, V]),
     }
     for name, (res, args) in sig.items():
@@ -398,6 +399,13 @@ class GrainHandler:
         a, o, n = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int32()
         self._check(self.lib.gg_traffic(self.ctx, ctypes.byref(a), ctypes.byref(o), ctypes.byref(n)))
         return a.value, o.value, n.value
+
+    def kernel_launches(self) -> tuple[int, int]:
+        """(kernels launched by step() graph replays so far, kernel nodes per
+        step graph); the plain form reports (0, 0)."""
+        t, k = ctypes.c_int64(), ctypes.c_int32()
+        self._check(self.lib.gg_kernel_launches(self.ctx, ctypes.byref(t), ctypes.byref(k)))
+        return t.value, k.value
 
     def dump(self, path: str, steps_done: int = 0, append: bool = False):
         self._check(self.lib.gg_dump(self.ctx, path.encode(), steps_done, int(append)))

@@ -303,6 +303,12 @@ int gg_profile_steps(gg_ctx* ctx, int32_t loop, int32_t nsteps, double* stage_ms
  * comparison-list members, and the number of existing grains. */
 int gg_traffic(gg_ctx* ctx, int64_t* sum_area, int64_t* sum_overlap, int32_t* n_exists);
 
+/* Kernels launched by gg_step's graph replays so far (batched form): the
+ * kernel nodes of the captured step graph, counted when it is captured,
+ * times the replays.  The plain form launches its stages from the host and
+ * reports 0.  per_step (optional) receives the graph's kernel-node count. */
+int gg_kernel_launches(gg_ctx* ctx, int64_t* total, int32_t* per_step);
+
 /*
  * Allocation-free box convolution.  No counterpart in the reference: the
  * reference allocates its FFT scratch per thread.  For callers that cannot

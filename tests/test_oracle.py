@@ -17,11 +17,19 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 CASES = ["iso_v20", "iso_v60", "rs_v30", "mob_v30"]
 
 
-@pytest.fixture(scope="module")
-def shim():
-    """The FFTW-API shim compiled as a small shared library for direct calls."""
-    out = os.path.join(ORACLE, "_ref", "libfft_shim_test.so")
-    src = os.path.join(ORACLE, "shim", "fft_shim.c")
+def reference_src() -> str:
+    """The reference's src/ directory: REF_SRC from the environment, else the
+    oracle Makefile's default."""
+    out = subprocess.run(["make", "-s", "-C", ORACLE, "print-ref-src"], capture_output=True, text=True, check=True)
+    return out.stdout.strip()
+
+
+@pytest.fixture(scope="module", params=["fft_shim", "fft_fast"])
+def shim(request):
+    """An FFTW-API shim compiled as a small shared library for direct calls:
+    the direct DFT of the parity oracle or the FFT of the timing baseline."""
+    out = os.path.join(ORACLE, "_ref", f"lib{request.param}_test.so")
+    src = os.path.join(ORACLE, "shim", request.param + ".c")
     if not os.path.exists(out) or os.path.getmtime(out) < os.path.getmtime(src):
         os.makedirs(os.path.dirname(out), exist_ok=True)
         subprocess.run(["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-shared", src, "-lm", "-o", out], check=True)
@@ -60,7 +68,7 @@ def _c2r(lib, y, n1):
     return x
 
 
-@pytest.mark.parametrize("n", [1, 2, 3, 7, 16, 17, 31, 40, 41])
+@pytest.mark.parametrize("n", [1, 2, 3, 7, 16, 17, 31, 40, 41, 43, 64, 97, 100])
 def test_fft_shim_matches_dft_definition(shim, n):
     rng = np.random.default_rng(n)
     x = rng.standard_normal((n, n))
@@ -109,7 +117,7 @@ def test_golden_inputs_regenerate_identically(tmp_path):
     assert open(tmp_path / "x.bin", "rb").read() == open(os.path.join(GOLDEN, "iso_v20", "iso_v20.bin"), "rb").read()
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference/src"), reason="reference tree not present")
+@pytest.mark.skipif(not os.path.isdir(reference_src()), reason="reference tree not present")
 def test_reference_rerun_matches_committed_fixture(tmp_path):
     """Rebuilds the oracle from the reference sources and reruns one case."""
     subprocess.run(["make", "-s", "-C", ORACLE, "ref"], check=True)

@@ -11,7 +11,8 @@
 
 Checks: no device status bit, the grains still tile the domain (sum of areas
 within 2e-3 of the unit square and drifting by less than 1e-3), and for the
-first configuration the per-grain area agreement of the two forms.
+first configuration the per-grain area agreement of the two forms (every
+grain alive in both, no size cut).
 """
 import os
 
@@ -65,10 +66,11 @@ def test_50000_grains_batched_and_plain(cases):
         assert abs(r["a0"] - 1.0) < 2e-3
         assert abs(np.nansum(r["areas"]) - r["a0"]) < 1e-3
     assert np.array_equal(np.isfinite(b["areas"]), np.isfinite(p["areas"]))
-    m = np.isfinite(b["areas"]) & (p["areas"] > 25.0 / 5600**2)
+    m = np.isfinite(b["areas"]) & (p["areas"] > 0)
     rel = np.abs(b["areas"][m] - p["areas"][m]) / p["areas"][m]
-    assert np.median(rel) < 1e-5
-    assert np.quantile(rel, 0.99) < 1e-3
+    assert np.median(rel) < 1e-6
+    assert np.quantile(rel, 0.99) < 1e-5
+    assert rel.max() <= 1e-3
 
 
 def test_100000_clustered_grains_batched(cases):
