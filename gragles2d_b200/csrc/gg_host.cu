@@ -301,6 +301,11 @@ int check_status(gg_ctx* c) {
         std::snprintf(buf, sizeof buf, "device capacity exceeded (status 0x%x)", st);
         return fail(c, GG_E_CAPACITY, buf);
     }
+    if (st & S_NAN) {
+        char buf[128];
+        std::snprintf(buf, sizeof buf, "non-finite distance value or area on the device (status 0x%x)", st);
+        return fail(c, GG_E_NUMERIC, buf);
+    }
     return GG_OK;
 }
 
@@ -676,6 +681,22 @@ int gg_create(const gg_params* p, int device, gg_ctx** out) {
     if (p->domain_border_size < 1) return bad("DomainBorderSize must be >= 1");
     if (p->analysis_timestep <= 0) return bad("AnalysisTimestep must be > 0");
     if (p->discrete_sampling_rate < 0) return bad("DiscreteSamplingRate must be >= 0");
+    if (p->list_capacity < 0 || p->list_capacity > 128) return bad("list_capacity must be 0 or 1..128");
+    if (!(p->arena_factor == 0 || p->arena_factor >= 1)) return bad("arena_factor must be 0 or >= 1");
+    {
+        const double vals[] = {p->triple_point_drag, p->constant_sector_radius, p->interpolating_sector_radius,
+                               p->hagb_energy, p->hagb_mobility, p->physical_domain_size, p->time_slope,
+                               p->theta_ref_deg, p->gamma_hagb, p->m_hagb, p->dislocation_energy_per_m,
+                               p->box_default_stored_elastic_energy, p->vacuum_permeability, p->magnetic_vector[0],
+                               p->magnetic_vector[1], p->magnetic_vector[2], p->delta_mag_sys,
+                               p->magnetic_force_field, p->grid_coarsement_gradient, p->arena_factor};
+        for (double v : vals)
+            if (!std::isfinite(v)) {
+                c->err = "non-finite parameter value";
+                *out = c;
+                return GG_E_NUMERIC;
+            }
+    }
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) {
         c->err = std::string("cudaSetDevice: ") + cudaGetErrorString(e);
@@ -705,10 +726,19 @@ void gg_destroy(gg_ctx* ctx) {
 
 const char* gg_last_error(const gg_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
+// Non-finite input values are refused before anything reaches the device:
+// boxes, pixel indices and contour walks are derived from them there.
+static bool all_finite(const double* v, size_t n) {
+    for (size_t q = 0; q < n; ++q)
+        if (!std::isfinite(v[q])) return false;
+    return true;
+}
+
 int gg_load_voxels(gg_ctx* c, int32_t nn, const int32_t* ids, int32_t n_grains, const double* euler,
                    const int32_t* bbox) {
     if (!c || !ids || !euler || !bbox || nn <= 0 || n_grains <= 0) return fail(c, GG_E_INVALID, "bad voxel input");
     if (c->initialised) return fail(c, GG_E_STATE, "network already initialised");
+    if (!all_finite(euler, 3 * (size_t)n_grains)) return fail(c, GG_E_NUMERIC, "non-finite Euler angle");
     c->nn = nn;
     c->N = n_grains;
     // the ID field goes straight to the device (it is read only by the
@@ -739,6 +769,9 @@ int gg_load_contours(gg_ctx* c, int32_t n_grains, const int32_t* offsets, const 
         if (np > 0 && np < 3) return fail(c, GG_E_INVALID, "a present grain needs a polygon of 3 or more points");
     }
     if (offsets[n_grains] > 0 && !xy) return fail(c, GG_E_INVALID, "no contour points");
+    if (offsets[n_grains] > 0 && !all_finite(xy, 2 * (size_t)offsets[n_grains]))
+        return fail(c, GG_E_NUMERIC, "non-finite contour coordinate");
+    if (!all_finite(quat, 4 * (size_t)n_grains)) return fail(c, GG_E_NUMERIC, "non-finite quaternion");
     c->N = n_grains;
     c->poly_off.assign(offsets, offsets + n_grains + 1);
     c->poly_xy.resize(2 * (size_t)offsets[n_grains]);
@@ -799,6 +832,7 @@ int gg_load_stored_energy(gg_ctx* c, const double* stored, int32_t n_grains) {
     if (!c->loaded) return fail(c, GG_E_STATE, "no microstructure loaded");
     if (c->initialised) return fail(c, GG_E_STATE, "network already initialised");
     if (n_grains != c->N) return fail(c, GG_E_INVALID, "one stored energy per grain");
+    if (!all_finite(stored, (size_t)n_grains)) return fail(c, GG_E_NUMERIC, "non-finite stored energy");
     c->stored.assign(stored, stored + n_grains);
     return GG_OK;
 }
@@ -1052,9 +1086,16 @@ int gg_distance_initialisation(gg_ctx* c) {
             cc += ccap[g];
         }
     }
-    const int64_t phi_cap = std::max<int64_t>(2 * a, a + (1 << 20));
-    const int64_t spec_cap = std::max<int64_t>(2 * sp, sp + (1 << 20));
-    const int64_t cont_cap = std::max<int64_t>(2 * cc, cc + (1 << 16));
+    // arenas: twice the initial totals (and room for 2^20 more values), or
+    // exactly arena_factor times them
+    const double af = P.arena_factor;
+    auto cap = [&](int64_t total, int64_t slack) {
+        return af > 0 ? std::max<int64_t>(total, (int64_t)std::ceil(af * (double)total))
+                      : std::max<int64_t>(2 * total, total + slack);
+    };
+    const int64_t phi_cap = cap(a, 1 << 20);
+    const int64_t spec_cap = cap(sp, 1 << 20);
+    const int64_t cont_cap = cap(cc, 1 << 16);
     const size_t rsz = P.precision == GG_PRECISION_PLAIN ? sizeof(double) : sizeof(float);
 
     // constant settings
@@ -1063,7 +1104,7 @@ int gg_distance_initialisation(gg_ctx* c) {
     C.m = m;
     C.b = b;
     C.nn = c->nn;
-    C.kmax = 96;
+    C.kmax = P.list_capacity > 0 ? P.list_capacity : 96;
     C.nbmax = 48;
     C.jmax = 48;
     C.tmax = tmax;

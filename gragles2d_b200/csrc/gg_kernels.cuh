@@ -763,7 +763,11 @@ __global__ void __launch_bounds__(256) k_resample(NetConst C, NetState* S, doubl
         };
         const double ro = 1 / (xr - xl) * ((xr - pointx) * at(yo, xl) + (pointx - xl) * at(yo, xr));
         const double ru = 1 / (xr - xl) * ((xr - pointx) * at(yu, xl) + (pointx - xl) * at(yu, xr));
-        dst[p] = (R)(1 / (yo - yu) * ((yo - pointy) * ru + (pointy - yu) * ro));
+        const double v = 1 / (yo - yu) * ((yo - pointy) * ru + (pointy - yu) * ro);
+        // the reference stops on a NaN here (src/box.cpp:1470-1474); the
+        // library records it (GG_S_NAN) and the call reports GG_E_NUMERIC
+        if (v != v) set_status(S, S_NAN);
+        dst[p] = (R)v;
     }
 }
 

@@ -44,6 +44,13 @@ double* g_scratch_ptr[kMaxDevices] = {};
 
 constexpr double kPiS = 3.14159265358979323846;
 
+// A failed runtime call: consume the runtime's last error as well, so that
+// this failure is not reported again by a later, unrelated call.
+int cuda_error() {
+    (void)cudaGetLastError();
+    return GG_E_CUDA;
+}
+
 // Same expressions as the context's table builder, so the tables match bit
 // for bit.
 void twiddle(int n, int k, double* re, double* im) {
@@ -62,12 +69,14 @@ double gaussian_multiplier(int n, int i2, int j2, double dt, int nn) {
 // device (the first call on a device does this set-up).
 int scratch_on_device(double** out) {
     int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return GG_E_CUDA;
+    if (cudaGetDevice(&dev) != cudaSuccess) return cuda_error();
+    if (dev < 0 || dev >= kMaxDevices) return GG_E_CUDA;
     std::lock_guard<std::mutex> lock(g_setup_mutex);
     if (!g_scratch_ptr[dev]) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_conv_scratch);
-        if (e != cudaSuccess || !p) return GG_E_CUDA;
+        if (e != cudaSuccess) return cuda_error();
+        if (!p) return GG_E_CUDA;
         g_scratch_ptr[dev] = static_cast<double*>(p);
     }
     *out = g_scratch_ptr[dev];
@@ -173,11 +182,11 @@ extern "C" int gg_convolve_box_static(const double* d_in, double* d_out, int32_t
     for (int i2 = 0; i2 < half; ++i2)
         for (int j2 = 0; j2 < half; ++j2) G[i2 * half + j2] = gaussian_multiplier(n, i2, j2, dt, real_domain_size);
     cudaError_t e = cudaMemcpyAsync(scratch + kSpecDoubles, tables, sizeof(tables), cudaMemcpyHostToDevice, s);
-    if (e != cudaSuccess) return GG_E_CUDA;
+    if (e != cudaSuccess) return cuda_error();
     k_conv_box_static<<<1, 256, 0, s>>>(d_in, d_out, n, scratch);
     e = cudaGetLastError();
-    if (e != cudaSuccess) return GG_E_CUDA;
+    if (e != cudaSuccess) return cuda_error();
     // The host table buffer lives on this stack frame: wait for the copy.
     e = cudaStreamSynchronize(s);
-    return e == cudaSuccess ? GG_OK : GG_E_CUDA;
+    return e == cudaSuccess ? GG_OK : cuda_error();
 }

@@ -469,6 +469,7 @@ __device__ int extract_bitmap_warp(const Field<R>& f, const uint32_t* idl, uint3
     // padded bitmap: row r + 1, bit c + 1 hold pixel (r, c) of the box
     const int wpr = (w + 2 + 31) >> 5;
     if (w + 2 > 1024 || (hgt + 2) * wpr + 1 > kBitmapCap) return -1;
+    bool nonfinite = false;  // a NaN or infinity anywhere in the field
     for (int r0 = 0; r0 < hgt + 2; r0 += 8)  // eight rows of loads in flight
         for (int q = 0; q < wpr; ++q) {
             const int c = q * 32 + lane - 1;
@@ -476,7 +477,10 @@ __device__ int extract_bitmap_warp(const Field<R>& f, const uint32_t* idl, uint3
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
                 const int r = r0 + u - 1;
-                in[u] = r >= 0 && r < hgt && c >= 0 && c < w && (double)f.v[r * w + c] >= 0;
+                const bool pix = r >= 0 && r < hgt && c >= 0 && c < w;
+                const double v = pix ? (double)f.v[r * w + c] : 0.0;
+                nonfinite |= !isfinite(v);
+                in[u] = pix && v >= 0;
             }
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
@@ -485,6 +489,7 @@ __device__ int extract_bitmap_warp(const Field<R>& f, const uint32_t* idl, uint3
             }
         }
     if (lane == 0) ws.bm[(hgt + 2) * wpr] = 0u;
+    if (__any_sync(0xffffffffu, nonfinite) && lane == 0) o.status |= S_NAN;
     __syncwarp();
     // first inside pixel in row-major order
     int start = -1;
@@ -712,6 +717,7 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_levelset_w(NetConst C,
             }
             regular_motion = __shfl_sync(0xffffffffu, regular_motion, 0);
         }
+        if (lane == 0 && ok && !isfinite(newVolume)) o.status |= S_NAN;
     }
     if (ok && shared) {  // publish the contour (energy and mobility still unset, as generatePoint leaves them)
         for (int i = lane; i < o.n; i += 32) {

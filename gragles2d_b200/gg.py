@@ -58,7 +58,8 @@ class Params(ctypes.Structure):
         ("use_stored_elastic_energy", ctypes.c_int32), ("use_magnetic_field", ctypes.c_int32),
         ("discrete_sampling_rate", ctypes.c_int32), ("plot_interval", ctypes.c_int32), ("use_texture", ctypes.c_int32),
         ("execute_in_parallel", ctypes.c_int32), ("maximum_number_of_threads", ctypes.c_int32),
-        ("neighbour_tracking", ctypes.c_int32), ("grain_scheduler", ctypes.c_int32), ("reserved_i", ctypes.c_int32 * 2),
+        ("neighbour_tracking", ctypes.c_int32), ("grain_scheduler", ctypes.c_int32),
+        ("list_capacity", ctypes.c_int32), ("reserved_i", ctypes.c_int32),
         ("triple_point_drag", ctypes.c_double), ("constant_sector_radius", ctypes.c_double),
         ("interpolating_sector_radius", ctypes.c_double), ("hagb_energy", ctypes.c_double),
         ("hagb_mobility", ctypes.c_double), ("physical_domain_size", ctypes.c_double),
@@ -67,7 +68,7 @@ class Params(ctypes.Structure):
         ("box_default_stored_elastic_energy", ctypes.c_double), ("vacuum_permeability", ctypes.c_double),
         ("magnetic_vector", ctypes.c_double * 3), ("delta_mag_sys", ctypes.c_double),
         ("magnetic_force_field", ctypes.c_double), ("grid_coarsement_gradient", ctypes.c_double),
-        ("reserved_d", ctypes.c_double * 1),
+        ("arena_factor", ctypes.c_double),
         ("read_from_filename", ctypes.c_char * 512), ("additional_filename", ctypes.c_char * 512),
     ]
 

@@ -40,7 +40,8 @@ enum {
     GG_E_IO = 3,           /* file missing or malformed */
     GG_E_STATE = 4,        /* call out of order (e.g. step before load) */
     GG_E_CAPACITY = 5,     /* a device arena, list or table overflowed */
-    GG_E_NUMERIC = 6       /* NaN or walk-limit detected on the device */
+    GG_E_NUMERIC = 6       /* a non-finite input value, or a NaN / infinity in a distance field or an area on
+                              the device (GG_S_NAN) */
 };
 
 enum { GG_PRECISION_PLAIN = 0, GG_PRECISION_BATCHED = 1 };
@@ -98,7 +99,10 @@ typedef struct gg_params {
     int32_t maximum_number_of_threads;/* MaximumNumberOfThreads */
     int32_t neighbour_tracking;       /* NeighbourTracking */
     int32_t grain_scheduler;          /* GrainScheduler */
-    int32_t reserved_i[2];
+    /* library settings (no parameters.xml tag) */
+    int32_t list_capacity;            /* comparison / second-order list entries per grain, 1..128 (0: 96);
+                                         a longer list is a GG_E_CAPACITY error */
+    int32_t reserved_i;
     double triple_point_drag;         /* TriplePointDrag */
     double constant_sector_radius;    /* ConstantSectorRadius (grid points) */
     double interpolating_sector_radius; /* InterpolatingSectorRadius (grid points) */
@@ -118,7 +122,9 @@ typedef struct gg_params {
     double delta_mag_sys;             /* deltaMagSys (susceptibility difference) */
     double magnetic_force_field;      /* MagneticForceField */
     double grid_coarsement_gradient;  /* GridCoarsementGradient */
-    double reserved_d[1];
+    double arena_factor;              /* distance-field, spectrum and contour arenas hold this multiple (>= 1)
+                                         of the initial network's totals (0: twice, and at least 2^20 values
+                                         more); boxes outgrowing them stop the run with GG_E_CAPACITY */
     char read_from_filename[512];     /* ReadFromFilename (.bin ID field) */
     char additional_filename[512];    /* AdditionalFilename (.uds header) */
 } gg_params;
@@ -319,14 +325,14 @@ int gg_kernel_launches(gg_ctx* ctx, int64_t* total, int32_t* per_step);
  * result is bit-identical to that stage.
  *  - d_in, d_out: caller-owned device buffers of n*n doubles, row-major.
  *  - dt, real_domain_size: the timestep and grid edge the kernel depends on.
- *  - stream: a cudaStream_t (NULL for the default stream); the call returns
- *    after the work on that stream has finished.
+ *  - stream: a cudaStream_t (NULL for the default stream); every call waits
+ *    for that stream and returns after its work there has finished.
  * It calls no cudaMalloc, cudaFree or allocating library routine: its scratch
  * is a fixed array of about 300 KB compiled into the library, which every GPU
  * that loads the library holds until the process exits.  n must be in
  * 1..GG_STATIC_CONV_MAX_N, else GG_E_INVALID is returned.  The first call on
- * a device looks up the scratch's device address (once per device); make
- * that first call before capturing any stream.  All calls on a device share
+ * a device looks up the scratch's device address (once per device), so that
+ * first call must come before any stream capture.  All calls on a device share
  * the one scratch array, so calls that overlap on the GPU (from several host
  * threads or streams) race; serialise them.
  */

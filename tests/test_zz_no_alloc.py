@@ -127,3 +127,41 @@ def test_static_box_convolution_rejects_sizes_beyond_the_maximum():
     with pytest.raises(gg.GGError) as e:
         gg.convolve_box_static(buf.data_ptr(), buf.data_ptr(), n, 1e-5, 100)
     assert e.value.code == 1
+
+
+def _gaussian_convolution(x, dt, nn):
+    """The convolution stage's transform in numpy: the unnormalised 2-D DFT
+    times G(i2, j2) = exp(-sqrt(2/pi) (i2^2 + j2^2) 4 dt nn^2 / n^2 pi^2) / n^2
+    (i2, j2 the frequencies folded to min(k, n - k), src/box.cpp:674-687),
+    then the unnormalised inverse."""
+    n = x.shape[0]
+    k = np.arange(n)
+    f = np.minimum(k, n - k).astype(np.float64)
+    half = n // 2 + 1
+    g = np.exp(-np.sqrt(2 / np.pi) * (f[:, None] ** 2 + f[None, :half] ** 2) * 4.0 * dt * nn * nn / (n * n)
+               * np.pi * np.pi) / (n * n)
+    return np.fft.irfft2(np.fft.rfft2(x) * g, s=(n, n)) * n * n
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 2, 3, 128])
+def test_static_box_convolution_known_answer_at_the_size_limits(n):
+    """Random boxes at the smallest sizes and at the maximum, where the two
+    spectra fill the scratch's spectrum region exactly, against numpy's FFT
+    of the same transform, two calls in a row."""
+    import torch
+
+    from gragles2d_b200 import gg
+
+    rng = np.random.default_rng(n)
+    x = rng.uniform(-1.0, 1.0, (n, n))
+    dt, nn = 3.125e-6, 800
+    want = _gaussian_convolution(x, dt, nn)
+    src = torch.from_numpy(x).cuda()
+    for _ in range(2):
+        dst = torch.full_like(src, np.nan)
+        torch.cuda.synchronize()
+        gg.convolve_box_static(src.data_ptr(), dst.data_ptr(), n, dt, nn)
+        got = dst.cpu().numpy()
+        np.testing.assert_allclose(got, want, rtol=0, atol=1e-12)
+
