@@ -396,24 +396,77 @@ __device__ __forceinline__ int segment_step(const float2* P32, const CPoint* P, 
     return before ? nv - 1 : nearest;
 }
 
-template <bool kForces>
-__global__ void __launch_bounds__(128, 7) k_corrector_f(NetConst C, NetState* S) {
+// Sectors of every grain for the next corrector (batched form), built one
+// step ahead so that the corrector's warps do not wait on the serial build:
+// the same build as the plain corrector's (prepare_sectors: segment lengths,
+// neighbour table, junction weights, then setPointsOnBoundary and the
+// constant / interpolating sectors, src/grainBoundary.cpp:233-342,
+// src/contourSector.cpp), one 32-thread CTA per grain.  kCur: from the roles
+// the step just produced (contour, junctions, IDLocal of this step, run after
+// the neighbour characteristics are computed), which become the previous
+// ones at the end of the step; else from the previous roles (after
+// initialisation, grid coarsening or new neighbour lists).
+template <bool kCur>
+__global__ void __launch_bounds__(32) k_sectors(NetConst C, NetState* S) {
     const int g = grain_at(S, blockIdx.x);
-    if (g > C.N || C.state[g] != G_EXISTS || C.regular[g] == 0 || S->loop == 0 || halted(S)) return;
+    if (g > C.N || C.state[g] != G_EXISTS || halted(S)) return;
     __shared__ SectorSet sec;
-    __shared__ __align__(16) float2 sp[kCorrMaxPts];
     __shared__ double jw[64];
     __shared__ uint32_t s_st;
     __shared__ double s_per;
     __shared__ NbTable nbt;
-    __shared__ VertexBuckets vb;
     __shared__ double s_seg[kSegShared];
-    __shared__ SegTable stab;
     __shared__ int jl[64], jr[64];
-    const CPoint* P = S->contPrev + S->coff_prev[g];
+    const int64_t coff = kCur ? S->coff_cur[g] : S->coff_prev[g];
+    const CPoint* P = (kCur ? S->contCur : S->contPrev) + coff;
+    const int size = kCur ? S->cn_cur[g] : S->cn_prev[g];
+    SectorPack* pk = reinterpret_cast<SectorPack*>(C.secpack) + g;
+    if (size < 2) {
+        if (threadIdx.x == 0) {
+            pk->nconst = 0;
+            pk->ninterp = 0;
+        }
+        return;
+    }
+    // segment lengths of long contours: the corrector's scratch at this
+    // contour's offsets (no corrector reads it while this kernel runs)
+    double* seg = size - 1 <= kSegShared ? s_seg : S->segPrev + coff;
+    const Box ib = kCur ? S->box_cur[g] : S->box_prev[g];
+    const uint32_t* idl = kCur ? S->idCur + S->off_cur[g] : S->idPrev + S->off_prev[g];
+    const Junction* J = (kCur ? S->jCur : S->jPrev) + (int64_t)g * C.jmax;
+    const int nj = min(kCur ? S->jn_cur[g] : S->jn_prev[g], 64);
+    prepare_sectors_view(C, S, g, P, size, seg, sec, jw, &s_st, &s_per, nbt, jl, jr, ib, idl, J, nj);
+    const int nc = sec.nconst, ni = sec.ninterp;
+    if (threadIdx.x == 0) {
+        pk->nconst = nc;
+        pk->ninterp = ni;
+    }
+    for (int c = threadIdx.x; c < nc; c += blockDim.x) pk->cw[c] = sec.cs[c].weight;
+    for (int c = threadIdx.x; c < ni; c += blockDim.x) pk->is[c] = sec.is[c];
+    for (int q = threadIdx.x; q < size - 1; q += blockDim.x) {
+        int sid;
+        double acc;
+        seg_table_entry(sec, seg, size, q, &sid, &acc);
+        C.segsec[coff + q] = (int16_t)sid;
+        C.segacc[coff + q] = (float)acc;
+    }
+}
+
+template <bool kForces>
+__global__ void __launch_bounds__(128, 7) k_corrector_f(NetConst C, NetState* S) {
+    const int g = grain_at(S, blockIdx.x);
+    if (g > C.N || C.state[g] != G_EXISTS || C.regular[g] == 0 || S->loop == 0 || halted(S)) return;
+    __shared__ __align__(16) float2 sp[kCorrMaxPts];
+    __shared__ NbTable nbt;
+    __shared__ VertexBuckets vb;
+    __shared__ double s_cw[kMaxConstSectors];
+    __shared__ InterpSector s_is[kMaxInterpSectors];
+    __shared__ int16_t s_sid[kCorrMaxPts];
+    __shared__ float s_acc[kCorrMaxPts];
+    const int64_t coff = S->coff_prev[g];
+    const CPoint* P = S->contPrev + coff;
     const int size = S->cn_prev[g];
     if (size < 2) return;
-    double* seg = size - 1 <= kSegShared ? s_seg : S->segPrev + S->coff_prev[g];
     const Box ib = S->box_prev[g];
     const uint32_t* idl = S->idPrev + S->off_prev[g];
     const bool staged = size <= kCorrMaxPts;
@@ -423,10 +476,23 @@ __global__ void __launch_bounds__(128, 7) k_corrector_f(NetConst C, NetState* S)
     if (staged)
         for (int k = threadIdx.x; k < size; k += blockDim.x)
             sp[k] = make_float2((float)(P[k].x - ox), (float)(P[k].y - oy));
-    if (staged) build_buckets(vb, P, size - 1, ox, oy, box_w(ib), box_h(ib));
-    prepare_sectors(C, S, g, P, size, seg, sec, jw, &s_st, &s_per, nbt, jl, jr);
-    const bool tabled = size - 1 <= kSegTable;
-    if (tabled) build_seg_table(sec, seg, size, stab);
+    // the sectors, built one step ahead (k_sectors), and the per-segment table
+    const SectorPack* pk = reinterpret_cast<const SectorPack*>(C.secpack) + g;
+    const int nconst = pk->nconst, ninterp = pk->ninterp;
+    for (int c = threadIdx.x; c < nconst; c += blockDim.x) s_cw[c] = pk->cw[c];
+    for (int c = threadIdx.x; c < ninterp; c += blockDim.x) s_is[c] = pk->is[c];
+    const int16_t* tsid = C.segsec + coff;
+    const float* tacc = C.segacc + coff;
+    if (staged) {
+        for (int q = threadIdx.x; q < size - 1; q += blockDim.x) {
+            s_sid[q] = tsid[q];
+            s_acc[q] = tacc[q];
+        }
+        tsid = s_sid;
+        tacc = s_acc;
+    }
+    build_nb_table(C, g, nbt);
+    if (staged) build_buckets(vb, P, size - 1, ox, oy, box_w(ib), box_h(ib));  // ends with a barrier
     __syncthreads();
     const Box bo = S->box_cur[g];
     const int x0 = ib.x0 < bo.x0 ? bo.x0 : ib.x0;
@@ -502,27 +568,11 @@ __global__ void __launch_bounds__(128, 7) k_corrector_f(NetConst C, NetState* S)
             segment = project_to_boundary(P, size, (double)j, (double)i, &dl);
             lambda = (float)dl;
         }
-        int sid = -1;
-        float interpolator = 0.f;
-        if (tabled) {
-            sid = stab.sector[segment];
-            if (sid <= -2) interpolator = (float)stab.acc[segment];
-        } else {
-            for (int c = 0; c < sec.nconst && sid == -1; c++)
-                if (within(sec.cs[c].left, sec.cs[c].right, real, segment)) sid = c;
-            for (int c = 0; c < sec.ninterp && sid == -1; c++)
-                if (within(sec.is[c].left, sec.is[c].right, real, segment)) sid = -2 - c;
-            if (sid <= -2) {
-                int it = 0;
-                for (int kk = sec.is[-2 - sid].right; kk != segment; kk = wrap_next(kk, real)) {
-                    interpolator += (float)seg[kk];
-                    if (++it > size) break;
-                }
-            }
-        }
+        const int sid = tsid[segment];
+        float interpolator = sid <= -2 ? tacc[segment] : 0.f;
         float weight;
         if (sid >= 0) {
-            weight = (float)sec.cs[sid].weight;
+            weight = (float)s_cw[sid];
         } else if (sid == -1) {
             // getGBEnergyTimesGBMobility(i, j) through the neighbour table
             weight = 1.f;
@@ -532,7 +582,7 @@ __global__ void __launch_bounds__(128, 7) k_corrector_f(NetConst C, NetState* S)
                     break;
                 }
         } else {
-            const InterpSector& s = sec.is[-2 - sid];
+            const InterpSector& s = s_is[-2 - sid];
             const int kn = wrap_next(segment, real);
             float ax, ay;
             if (staged) {
@@ -611,6 +661,14 @@ cudaError_t batched_init(const NetConst& C, NetState* dS, const int32_t* d_ids, 
     return cudaGetLastError();
 }
 
+size_t batched_sector_pack_bytes() { return sizeof(SectorPack); }
+
+cudaError_t batched_sectors(const NetConst& C, NetState* dS, cudaStream_t s) {
+    if (C.N <= 0) return cudaSuccess;
+    k_sectors<false><<<C.N, 32, 0, s>>>(C, dS);
+    return cudaGetLastError();
+}
+
 cudaError_t batched_order(const NetConst& C, NetState* dS, cudaStream_t s) {
     if (C.N <= 0) return cudaSuccess;
     k_order<<<1, 1024, 0, s>>>(C, dS);
@@ -635,7 +693,10 @@ cudaError_t batched_stage_kernel(const NetConst& C, NetState* dS, int which, cud
         case 3: k_compare<float><<<C.N, cfg.compare_threads, 0, s>>>(C, dS); break;
         case 4: k_levelset_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS); break;
         case 5: k_alloc<<<1, 1024, 0, s>>>(C, dS, 1); break;
-        case 6: k_neighbours_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS, reinterpret_cast<PointInfo*>(C.ptinfo)); break;
+        case 6:
+            k_neighbours_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS, reinterpret_cast<PointInfo*>(C.ptinfo));
+            k_sectors<true><<<C.N, 32, 0, s>>>(C, dS);
+            break;
         case 7: launch_redistance(C, dS, s); break;
         default:
             k_finalize<<<1, 1024, 0, s>>>(C, dS, 1);
@@ -661,6 +722,7 @@ cudaError_t batched_stages(const NetConst& C, NetState* dS, int stages, cudaStre
     if (stages & ST_REDIST) {
         k_alloc<<<1, 1024, 0, s>>>(C, dS, 1);
         k_neighbours_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS, reinterpret_cast<PointInfo*>(C.ptinfo));
+        k_sectors<true><<<C.N, 32, 0, s>>>(C, dS);
         launch_redistance(C, dS, s);
         k_finalize<<<1, 1024, 0, s>>>(C, dS, 1);
         k_order<<<1, 1024, 0, s>>>(C, dS);
@@ -684,10 +746,12 @@ cudaError_t batched_step_graph(const NetConst& C, NetState* dS, cudaStream_t s, 
     k_compare<float><<<C.N, cfg.compare_threads, 0, s>>>(C, dS);
     k_levelset_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS);
     k_alloc<<<1, 1024, 0, s>>>(C, dS, 1);
-    // volume / energy / neighbours (contours, lists) beside redistancing (fields)
+    // volume / energy / neighbours (contours, lists) and the next step's
+    // sectors beside redistancing (fields)
     if ((e = cudaEventRecord(ev[2], s)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(s2, ev[2], 0)) != cudaSuccess) return e;
     k_neighbours_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s2>>>(C, dS, reinterpret_cast<PointInfo*>(C.ptinfo));
+    k_sectors<true><<<C.N, 32, 0, s2>>>(C, dS);  // the next step's sectors
     if ((e = cudaEventRecord(ev[3], s2)) != cudaSuccess) return e;
     launch_redistance(C, dS, s);
     if ((e = cudaStreamWaitEvent(s, ev[3], 0)) != cudaSuccess) return e;

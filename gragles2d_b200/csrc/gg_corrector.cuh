@@ -553,34 +553,55 @@ __device__ void build_sectors_warp(const NetConst& C, const NbTable& T, const CP
     __syncwarp();
 }
 
-__device__ void build_seg_table(const SectorSet& S, const double* seg, int size, SegTable& T) {
+// Segment q's entry of the per-segment table (see SegTable).
+__device__ __forceinline__ void seg_table_entry(const SectorSet& S, const double* seg, int size, int q, int* sid_out,
+                                                double* acc_out) {
     const int real = size - 1;
-    for (int q = threadIdx.x; q < real; q += blockDim.x) {
-        int sid = -1;
-        for (int c = 0; c < S.nconst; c++)
-            if (within(S.cs[c].left, S.cs[c].right, real, q)) {
-                sid = c;
+    int sid = -1;
+    for (int c = 0; c < S.nconst; c++)
+        if (within(S.cs[c].left, S.cs[c].right, real, q)) {
+            sid = c;
+            break;
+        }
+    if (sid < 0)
+        for (int c = 0; c < S.ninterp; c++)
+            if (within(S.is[c].left, S.is[c].right, real, q)) {
+                sid = -2 - c;
                 break;
             }
-        if (sid < 0)
-            for (int c = 0; c < S.ninterp; c++)
-                if (within(S.is[c].left, S.is[c].right, real, q)) {
-                    sid = -2 - c;
-                    break;
-                }
-        T.sector[q] = (short)sid;
-        double acc = 0;
-        if (sid <= -2) {
-            const int k0 = S.is[-2 - sid].right;
-            int it = 0;
-            for (int k = k0; k != q; k = wrap_next(k, real)) {
-                acc += seg[k];
-                if (++it > size) break;
-            }
+    double acc = 0;
+    if (sid <= -2) {
+        const int k0 = S.is[-2 - sid].right;
+        int it = 0;
+        for (int k = k0; k != q; k = wrap_next(k, real)) {
+            acc += seg[k];
+            if (++it > size) break;
         }
+    }
+    *sid_out = sid;
+    *acc_out = acc;
+}
+
+__device__ void build_seg_table(const SectorSet& S, const double* seg, int size, SegTable& T) {
+    for (int q = threadIdx.x; q < size - 1; q += blockDim.x) {
+        int sid;
+        double acc;
+        seg_table_entry(S, seg, size, q, &sid, &acc);
+        T.sector[q] = (short)sid;
         T.acc[q] = acc;
     }
 }
+
+// The sectors of a grain as the batched corrector reads them, built one step
+// ahead (k_sectors): the constant sectors' weights and the interpolating
+// sectors; the per-segment table lives beside the contour (NetConst::segsec,
+// segacc at the contour's offsets).
+struct SectorPack {
+    int32_t nconst, ninterp;
+    uint32_t status, pad;
+    double cw[kMaxConstSectors];
+    InterpSector is[kMaxInterpSectors];
+};
 
 // ExplicitGrainBoundary::getWeight (src/grainBoundary.cpp:344-363) for one pixel.
 __device__ __forceinline__ double pixel_weight(const NetConst& C, const NbTable& T, const CPoint* P,
@@ -638,13 +659,22 @@ __device__ __forceinline__ double pixel_weight(const NetConst& C, const NbTable&
 // the seg scratch, one thread per segment) and the neighbour table, junction
 // weights (one warp per junction), perimeter, then the sector build by warp
 // 0 (all its lookups in shared memory).  jl, jr: shared scratch of 64 ints.
+// The same on explicit roles: the contour P, its IDLocal map idl on box ib
+// and its junctions J (nj of them).
+__device__ void prepare_sectors_view(const NetConst& C, NetState* S, int g, const CPoint* P, int size, double* seg,
+                                     SectorSet& sec, double* jw, uint32_t* s_st, double* s_per, NbTable& T, int* jl,
+                                     int* jr, Box ib, const uint32_t* idl, const Junction* J, int nj);
+
 __device__ void prepare_sectors(const NetConst& C, NetState* S, int g, const CPoint* P, int size, double* seg,
                                 SectorSet& sec, double* jw, uint32_t* s_st, double* s_per, NbTable& T, int* jl,
                                 int* jr) {
-    const Box ib = S->box_prev[g];
-    const uint32_t* idl = S->idPrev + S->off_prev[g];
-    const Junction* J = S->jPrev + (int64_t)g * C.jmax;
-    const int nj = min(S->jn_prev[g], 64);
+    prepare_sectors_view(C, S, g, P, size, seg, sec, jw, s_st, s_per, T, jl, jr, S->box_prev[g],
+                         S->idPrev + S->off_prev[g], S->jPrev + (int64_t)g * C.jmax, min(S->jn_prev[g], 64));
+}
+
+__device__ void prepare_sectors_view(const NetConst& C, NetState* S, int g, const CPoint* P, int size, double* seg,
+                                     SectorSet& sec, double* jw, uint32_t* s_st, double* s_per, NbTable& T, int* jl,
+                                     int* jr, Box ib, const uint32_t* idl, const Junction* J, int nj) {
     if (threadIdx.x == 0) *s_st = 0;
     for (int k = threadIdx.x; k < size - 1; k += blockDim.x) {
         const double dx = P[k + 1].x - P[k].x, dy = P[k + 1].y - P[k].y;

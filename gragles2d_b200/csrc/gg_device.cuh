@@ -141,6 +141,13 @@ struct NetConst {
     void* ptinfo;            // per-contour-point probe scratch (contCur offsets), 32 bytes each
     double* dvol;            // tangent mode: d area / d p_k of the last level set, 4 per grain (else null)
     double* dseg;            // tangent mode: d segment length / d p_k, 4 per previous-contour point (scratch)
+    // batched form: sectors built one step ahead for the corrector (k_sectors):
+    // one SectorPack per grain, and per contour point (at the contour's
+    // offsets) the sector of the segment starting there and, for an
+    // interpolating sector, the arc length from the sector's right end
+    void* secpack;
+    int16_t* segsec;
+    float* segacc;
 };
 
 // Per-step rotating state, resident in device memory (kernels read it

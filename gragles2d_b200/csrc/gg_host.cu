@@ -70,6 +70,7 @@ struct gg_ctx {
     LaunchCfg cfg{256, 256, 128, 64};
 
     cudaGraphExec_t graph = nullptr;
+    bool sectors_stale = false;    // batched form: the corrector's sectors need a rebuild before the next step
     int32_t graph_kernels = 0;     // kernel nodes of the captured step graph
     int64_t kernel_launches = 0;   // graph_kernels per replay, summed
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -464,6 +465,7 @@ int coarsen_if_due(gg_ctx* c, int loop, bool* changed) {
     GG_CUDA(c, h2d(c->dS, &S, sizeof(NetState)));
     if (P.precision != GG_PRECISION_PLAIN) GG_CUDA(c, batched_order(C, c->dS, c->stream));
     GG_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->sectors_stale = true;  // new contours
     if (c->graph) {  // the captured step holds the old constants
         cudaGraphExecDestroy(c->graph);
         c->graph = nullptr;
@@ -473,6 +475,10 @@ int coarsen_if_due(gg_ctx* c, int loop, bool* changed) {
 }
 
 int launch_stages(gg_ctx* c, int stages) {
+    if (c->P.precision != GG_PRECISION_PLAIN && (stages & ST_CONV) && c->sectors_stale) {
+        GG_CUDA(c, batched_sectors(c->C, c->dS, c->stream));
+        c->sectors_stale = false;
+    }
     cudaError_t e = c->P.precision == GG_PRECISION_PLAIN ? plain_stages(c->C, c->dS, stages, c->stream, c->cfg)
                                                          : batched_stages(c->C, c->dS, stages, c->stream, c->cfg);
     if (e != cudaSuccess) return cuda_fail(c, e, "stage launch");
@@ -1247,6 +1253,13 @@ int gg_distance_initialisation(gg_ctx* c) {
         S.phiA = pa;
         S.phiB = pb;
         S.spec = sp_;
+        // sectors built one step ahead for the corrector
+        char* pk;
+        ALLOC(pk, batched_sector_pack_bytes() * (size_t)(N + 1));
+        C.secpack = pk;
+        ALLOC(C.segsec, cont_cap);
+        ALLOC(C.segacc, cont_cap);
+        c->sectors_stale = true;
     }
     (void)rsz;
     ALLOC(S.idPrev, phi_cap);
@@ -1340,6 +1353,7 @@ int gg_distance_initialisation(gg_ctx* c) {
 int gg_find_neighbors(gg_ctx* c) {
     if (!c) return GG_E_INVALID;
     if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
+    c->sectors_stale = c->P.precision != GG_PRECISION_PLAIN;  // junction weights read the neighbour lists
     GG_CUDA(c, find_neighbors_launch(c->C, c->dS, c->stream));
     return check_status(c);
 }
@@ -1348,6 +1362,7 @@ int gg_set_neighbours(gg_ctx* c, const int32_t* offsets, const int32_t* ids) {
     if (!c || !offsets || !ids) return GG_E_INVALID;
     if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
     const int N = c->N, K = c->C.kmax;
+    c->sectors_stale = c->P.precision != GG_PRECISION_PLAIN;
     std::vector<int32_t> sec((size_t)K * (N + 1), 0), n(N + 1, 0), zero(N + 1, 0);
     std::vector<Neighbour> nb((size_t)c->C.nbmax * (N + 1));
     std::vector<int32_t> nbn(N + 1, 0);
@@ -1459,6 +1474,10 @@ int gg_step(gg_ctx* c, int32_t loop, int32_t nsteps) {
             if (e != cudaSuccess) return cuda_fail(c, e, "graph instantiate");
             c->graph_kernels = kn;
         }
+        if (c->sectors_stale) {
+            GG_CUDA(c, batched_sectors(c->C, c->dS, c->stream));
+            c->sectors_stale = false;
+        }
         GG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
         for (int s = 0; s < nsteps; ++s) GG_CUDA(c, cudaGraphLaunch(c->graph, c->stream));
         GG_CUDA(c, cudaEventRecord(c->ev1, c->stream));
@@ -1502,9 +1521,13 @@ int gg_profile_steps(gg_ctx* c, int32_t loop, int32_t nsteps, double* stage_ms) 
     if (c->tangents) return fail(c, GG_E_STATE, "stage profiling runs without tangents");
     int rc = set_loop(c, loop);
     if (rc) return rc;
+    const bool plain = c->P.precision == GG_PRECISION_PLAIN;
+    if (!plain && c->sectors_stale) {
+        GG_CUDA(c, batched_sectors(c->C, c->dS, c->stream));
+        c->sectors_stale = false;
+    }
     cudaEvent_t ev[GG_NSTAGES + 1];
     for (int k = 0; k <= GG_NSTAGES; ++k) GG_CUDA(c, cudaEventCreate(&ev[k]));
-    const bool plain = c->P.precision == GG_PRECISION_PLAIN;
     for (int s = 0; s < nsteps; ++s) {
         GG_CUDA(c, cudaEventRecord(ev[0], c->stream));
         for (int k = 0; k < GG_NSTAGES; ++k) {

@@ -45,6 +45,10 @@ cudaError_t batched_init(const NetConst& C, NetState* dS, const int32_t* d_ids, 
 cudaError_t batched_init_polygon(const NetConst& C, NetState* dS, cudaStream_t s);
 // rebuilds the batched form's work queue (NetState::order) from the current boxes
 cudaError_t batched_order(const NetConst& C, NetState* dS, cudaStream_t s);
+// the sectors of the next corrector from the previous roles (after set-up,
+// grid coarsening or new neighbour lists); the step builds them itself
+cudaError_t batched_sectors(const NetConst& C, NetState* dS, cudaStream_t s);
+size_t batched_sector_pack_bytes();
 cudaError_t finalize_only(const NetConst& C, NetState* dS, int rotate, cudaStream_t s);
 // Every grain's gg_grain_stats into out[0 .. N-1] (device memory).
 cudaError_t pack_stats(const NetConst& C, const NetState* dS, gg_grain_stats* out, cudaStream_t s);
