@@ -415,7 +415,6 @@ __global__ void __launch_bounds__(32) k_sectors(NetConst C, NetState* S) {
     __shared__ uint32_t s_st;
     __shared__ double s_per;
     __shared__ NbTable nbt;
-    __shared__ double s_seg[kSegShared];
     __shared__ int jl[64], jr[64];
     const int64_t coff = kCur ? S->coff_cur[g] : S->coff_prev[g];
     const CPoint* P = (kCur ? S->contCur : S->contPrev) + coff;
@@ -428,9 +427,10 @@ __global__ void __launch_bounds__(32) k_sectors(NetConst C, NetState* S) {
         }
         return;
     }
-    // segment lengths of long contours: the corrector's scratch at this
-    // contour's offsets (no corrector reads it while this kernel runs)
-    double* seg = size - 1 <= kSegShared ? s_seg : S->segPrev + coff;
+    // segment lengths: the corrector's scratch at this contour's offsets (no
+    // corrector reads it while this kernel runs; a global buffer leaves room
+    // for more CTAs per SM than a shared one)
+    double* seg = S->segPrev + coff;
     const Box ib = kCur ? S->box_cur[g] : S->box_prev[g];
     const uint32_t* idl = kCur ? S->idCur + S->off_cur[g] : S->idPrev + S->off_prev[g];
     const Junction* J = (kCur ? S->jCur : S->jPrev) + (int64_t)g * C.jmax;
