@@ -216,6 +216,9 @@ def run_ours(args, rank, world, local_rank):
     for _ in range(W):
         hw.step(1)
         hw.grain_stats()
+    # launch bins measured on this network; the library keeps them for the
+    # contexts below (same largest box edge and grain count)
+    tuning = hw.autotune(1)
     hw.close()
     # Timed: load from the host buffers, initialise, K steps each followed by
     # a read of every grain's statistics.
@@ -293,7 +296,7 @@ def run_ours(args, rank, world, local_rank):
     achieved = dom_bytes / (stage_ms[dom] / 1e3) / 1e9 if dom_bytes else None
     kernel_names = {"convolution": "k_conv_sep", "corrector": "k_corrector_f", "comparison": "k_compare",
                     "level_set": "k_levelset_w", "redistancing": "k_redistance_s",
-                    "volume_energy_neighbours": "k_neighbours_w"}
+                    "volume_energy_neighbours": "k_neighbours_w + k_sectors"}
     out = {
         "metric": METRIC,
         "value": value,
@@ -328,6 +331,7 @@ def run_ours(args, rank, world, local_rank):
         # when it captured the graph) times the timed replays
         "gpu_launches": launches,
         "gpu_launches_per_step": per_step,
+        "launch_bins": tuning,
         "status": status_b,
     }
     if world == 1 and not args.no_accuracy:
@@ -483,8 +487,10 @@ def run_profile_case(args, local_rank):
     h.distanceInitialisation()
     h.find_neighbors()
     h.step(args.warmup)
+    area, overlap, nex = h.traffic()
     prof = h.profile_steps(2)
-    print(json.dumps({"profile_case": PROFILE_CASE["name"], "stage_ms": prof, "status": h.status()}), flush=True)
+    print(json.dumps({"profile_case": PROFILE_CASE["name"], "stage_ms": prof, "status": h.status(),
+                      "sum_box_area": area, "sum_overlap": overlap, "grains": nex}), flush=True)
     h.close()
 
 

@@ -8,7 +8,7 @@
 
 namespace gg {
 
-constexpr int kSepSmemMaxN = 64;  // intermediate in shared memory up to this edge
+constexpr int kConvSmemEdgeMax = 128;  // largest tunable edge with the intermediate in shared memory
 constexpr int kSepStrip = 4;       // outputs per thread along the convolution axis
 
 // Gaussian convolution as a separable circular convolution in real space:
@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(128) k_conv_sep(NetConst C, NetState* S) {
     const float* in = reinterpret_cast<const float*>(S->phiA) + S->off_cur[g];
     float* out = reinterpret_cast<float*>(S->phiB) + S->off_cur[g];
     const float* kg = C.ck + C.ck_off[n];
-    const bool fits = n <= kSepSmemMaxN;
+    const bool fits = n <= C.conv_smem_edge;
     float* kx = sm + 1;  // sm[0] is the guard entry kx[-1]
     const int kl = kx_len(n);
     float* T = fits ? sm + 1 + kl : reinterpret_cast<float*>(S->spec) + S->soff_cur[g];
@@ -165,11 +165,11 @@ __global__ void __launch_bounds__(128) k_conv_sep(NetConst C, NetState* S) {
     sep_pass_cols(T, out, kx, n, R);
 }
 
-size_t conv_sep_smem(int tmax) {
-    // the row-pass intermediate of a box (edge up to kSepSmemMaxN) with its
+size_t conv_sep_smem(int tmax, int edge) {
+    // the row-pass intermediate of a box (edge up to `edge`) with its
     // extended kernel, or the extended kernel alone of the largest box (whose
     // intermediate goes to the grain's scratch in device memory)
-    const int n = tmax < kSepSmemMaxN ? tmax : kSepSmemMaxN;
+    const int n = tmax < edge ? tmax : edge;
     const size_t staged = (size_t)n * n + 2 * (size_t)n + kSepStrip + 2;
     const size_t kernel_only = 2 * (size_t)tmax + kSepStrip + 2;
     return sizeof(float) * (staged > kernel_only ? staged : kernel_only);
@@ -631,7 +631,7 @@ int g_big_grid = 148;
 
 cudaError_t batched_prepare(int tmax) {
     cudaError_t e = cudaFuncSetAttribute(k_conv_sep, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)conv_sep_smem(tmax));
+                                         (int)conv_sep_smem(tmax, kConvSmemEdgeMax));
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(k_redistance_big, cudaFuncAttributeMaxDynamicSharedMemorySize, kRedistBigSmemBytes);
     if (e != cudaSuccess) return e;
@@ -687,7 +687,7 @@ cudaError_t batched_stage_kernel(const NetConst& C, NetState* dS, int which, cud
     const int wblocks = (C.N + kGrainsPerBlock - 1) / kGrainsPerBlock;
     (void)gblocks;
     switch (which) {
-        case 0: k_conv_sep<<<C.N, 128, conv_sep_smem(C.tmax), s>>>(C, dS); break;
+        case 0: k_conv_sep<<<C.N, 128, conv_sep_smem(C.tmax, C.conv_smem_edge), s>>>(C, dS); break;
         case 1: if (!C.isotropic) launch_corrector_f(C, dS, s); break;
         case 2: k_second_order_w<<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS); break;
         case 3: k_compare<float><<<C.N, cfg.compare_threads, 0, s>>>(C, dS); break;
@@ -713,7 +713,7 @@ cudaError_t batched_stages(const NetConst& C, NetState* dS, int stages, cudaStre
     const int wblocks = (C.N + kGrainsPerBlock - 1) / kGrainsPerBlock;
     (void)gblocks;
     if (stages & ST_CONV) {
-        k_conv_sep<<<C.N, 128, conv_sep_smem(C.tmax), s>>>(C, dS);
+        k_conv_sep<<<C.N, 128, conv_sep_smem(C.tmax, C.conv_smem_edge), s>>>(C, dS);
         if (!C.isotropic) launch_corrector_f(C, dS, s);
     }
     if (stages & ST_SECOND) k_second_order_w<<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS);
@@ -740,7 +740,7 @@ cudaError_t batched_step_graph(const NetConst& C, NetState* dS, cudaStream_t s, 
     if ((e = cudaStreamWaitEvent(s2, ev[0], 0)) != cudaSuccess) return e;
     k_second_order_w<<<wblocks, 32 * kGrainsPerBlock, 0, s2>>>(C, dS);
     if ((e = cudaEventRecord(ev[1], s2)) != cudaSuccess) return e;
-    k_conv_sep<<<C.N, 128, conv_sep_smem(C.tmax), s>>>(C, dS);
+    k_conv_sep<<<C.N, 128, conv_sep_smem(C.tmax, C.conv_smem_edge), s>>>(C, dS);
     if (!C.isotropic) launch_corrector_f(C, dS, s);
     if ((e = cudaStreamWaitEvent(s, ev[1], 0)) != cudaSuccess) return e;
     k_compare<float><<<C.N, cfg.compare_threads, 0, s>>>(C, dS);

@@ -104,6 +104,12 @@ struct NetConst {
     int32_t use_mobility_model;
     int32_t analysis_timestep;
     int32_t decouple;
+    // batched form's launch bins (autotuned, gg_autotune): boxes with an
+    // edge above big_edge are redistanced by the large-box kernel; the
+    // convolution keeps its row-pass intermediate in shared memory up to
+    // conv_smem_edge
+    int32_t big_edge;
+    int32_t conv_smem_edge;
     double h, delta, dt;
     double csr, isr;  // sector radii (already scaled by h)
     double ds;        // (2 CSR + 2 ISR) / realDomainSize in grid points, src/grainhdl.cpp:81-82

@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <map>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -913,6 +914,24 @@ int gg_load_voxel_files(gg_ctx* c, const char* base_dir) {
     return rc;
 }
 
+// Launch bins chosen by gg_autotune, kept for the process per (largest box
+// edge, grain count): a later context of the same network size starts with
+// them.
+struct TunedBins {
+    int compare_threads, big_edge, conv_smem_edge;
+};
+std::mutex g_tune_mutex;
+std::map<std::pair<int, int>, TunedBins> g_tuned;
+
+void apply_cached_tuning(gg_ctx* c) {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    const auto it = g_tuned.find({c->C.tmax, c->N});
+    if (it == g_tuned.end()) return;
+    c->cfg.compare_threads = it->second.compare_threads;
+    c->C.big_edge = it->second.big_edge;
+    c->C.conv_smem_edge = it->second.conv_smem_edge;
+}
+
 int gg_distance_initialisation(gg_ctx* c) {
     if (!c) return GG_E_INVALID;
     if (!c->loaded) return fail(c, GG_E_STATE, "no microstructure loaded");
@@ -1114,6 +1133,8 @@ int gg_distance_initialisation(gg_ctx* c) {
     C.nbmax = 48;
     C.jmax = 48;
     C.tmax = tmax;
+    C.big_edge = 128;
+    C.conv_smem_edge = 64;
     C.isotropic = P.is_isotropic_network ? 1 : 0;
     C.use_mobility_model = P.use_mobility_model;
     C.analysis_timestep = P.analysis_timestep;
@@ -1343,6 +1364,7 @@ int gg_distance_initialisation(gg_ctx* c) {
     }
     GG_CUDA(c, finalize_only(C, c->dS, 0, c->stream));
     if (!plain) GG_CUDA(c, batched_order(C, c->dS, c->stream));
+    if (!plain) apply_cached_tuning(c);
     rc = check_status(c);
     if (rc != GG_OK) return rc;
     c->initialised = true;
@@ -1428,6 +1450,78 @@ int gg_grain_count(gg_ctx* c, int32_t* current, double* max_volume) {
     if (rc) return rc;
     if (current) *current = c->hS.live;
     if (max_volume) *max_volume = c->hS.max_volume;
+    return GG_OK;
+}
+
+int gg_step(gg_ctx* c, int32_t loop, int32_t nsteps);
+
+int gg_autotune(gg_ctx* c, int32_t loop, int32_t steps_per_candidate, gg_tuning* out) {
+    if (!c || !out) return GG_E_INVALID;
+    if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
+    std::memset(out, 0, sizeof *out);
+    if (c->P.precision == GG_PRECISION_PLAIN) {  // the plain form has no bins to tune
+        out->compare_threads = c->cfg.compare_threads;
+        return GG_OK;
+    }
+    const int k = steps_per_candidate > 0 ? steps_per_candidate : 2;
+    int steps = 0;
+    // device ms per step of the current bins over k steps (a fresh graph
+    // for every candidate; capture is outside the timed region)
+    auto measure = [&](double* ms) -> int {
+        if (c->graph) {
+            cudaGraphExecDestroy(c->graph);
+            c->graph = nullptr;
+        }
+        double total = 0;
+        for (int s = 0; s < k; ++s) {
+            const int rc = gg_step(c, loop + steps, 1);
+            if (rc) return rc;
+            total += c->last_ms;
+            ++steps;
+        }
+        *ms = total / k;
+        return GG_OK;
+    };
+    double best = 0;
+    int rc = measure(&best);
+    if (rc) return rc;
+    out->ms_default = best;
+    // one knob at a time; a candidate replaces the current value only when
+    // it is faster by more than 1% (the network changes a little between the
+    // steps the candidates run on)
+    auto tune = [&](int* knob, std::initializer_list<int> cands) -> int {
+        const int keep = *knob;
+        int chosen = keep;
+        for (int v : cands) {
+            if (v == keep) continue;
+            *knob = v;
+            double ms = 0;
+            const int r = measure(&ms);
+            if (r) return r;
+            if (ms < 0.99 * best) {
+                best = ms;
+                chosen = v;
+            }
+        }
+        *knob = chosen;
+        return GG_OK;
+    };
+    if ((rc = tune(&c->C.big_edge, {64, 96, 128, 192, 1 << 20})) != GG_OK) return rc;
+    if ((rc = tune(&c->cfg.compare_threads, {128, 256})) != GG_OK) return rc;  // k_compare: at most 256
+    if ((rc = tune(&c->C.conv_smem_edge, {48, 64, 96, 128})) != GG_OK) return rc;
+    if (c->graph) {
+        cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+    }
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        g_tuned[{c->C.tmax, c->N}] = TunedBins{c->cfg.compare_threads, c->C.big_edge, c->C.conv_smem_edge};
+    }
+    out->compare_threads = c->cfg.compare_threads;
+    out->big_edge = c->C.big_edge;
+    out->conv_smem_edge = c->C.conv_smem_edge;
+    out->steps_run = steps;
+    out->ms_tuned = best;
     return GG_OK;
 }
 

@@ -39,7 +39,7 @@ cudaError_t batched_stages(const NetConst& C, NetState* dS, int stages, cudaStre
 // neighbours beside redistancing) forked onto s2 through the events ev[0..3].
 cudaError_t batched_step_graph(const NetConst& C, NetState* dS, cudaStream_t s, cudaStream_t s2, cudaEvent_t* ev,
                                const LaunchCfg& cfg);
-size_t conv_sep_smem(int tmax);
+size_t conv_sep_smem(int tmax, int edge);
 cudaError_t batched_prepare(int tmax);
 cudaError_t batched_init(const NetConst& C, NetState* dS, const int32_t* d_ids, cudaStream_t s);
 cudaError_t batched_init_polygon(const NetConst& C, NetState* dS, cudaStream_t s);

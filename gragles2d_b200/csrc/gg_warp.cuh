@@ -1422,29 +1422,29 @@ __device__ void redistance_grain_s(const NetConst& C, NetState* S, int g, unsign
     }
 }
 
-// Large boxes (batched form, size bin above kRedistBigEdge): k_redistance_big
-// takes them with 256 threads and up to 200 KB of shared memory, so a 168^2
-// box is staged whole and a 256^2 one sweeps 4x as many columns at a time.
-// The bin starts above the largest boxes of a uniform-seed Voronoi network
-// (edge <= 98 at 25 cells per grain), so there it is an empty launch.
-constexpr int kRedistBigEdge = 128;
+// Large boxes (batched form, size bin above NetConst::big_edge, 128 unless
+// tuned): k_redistance_big takes them with 256 threads and up to 200 KB of
+// shared memory, so a 168^2 box is staged whole and a 256^2 one sweeps 4x as
+// many columns at a time.  At 128 the bin starts above the largest boxes of a
+// uniform-seed Voronoi network (edge <= 98 at 25 cells per grain), so there
+// it is an empty launch.
 constexpr int kRedistBigThreads = 256;
 constexpr int kRedistBigSmemBytes = 200 * 1024;
 
 // One CTA of 64 threads per grain: every grain in the plain form; in the
-// batched form those whose box edge is at most kRedistBigEdge.
+// batched form those whose box edge is at most C.big_edge.
 template <typename R>
 __global__ void __launch_bounds__(kRedistThreads) k_redistance_s(NetConst C, NetState* S) {
     extern __shared__ __align__(16) unsigned char s_raw[];
     const int g = grain_at(S, blockIdx.x);
     if (g > C.N || C.state[g] != G_EXISTS || halted(S)) return;
-    if (S->order && box_w(S->box_cur[g]) > kRedistBigEdge) return;  // the large-box bin
+    if (S->order && box_w(S->box_cur[g]) > C.big_edge) return;  // the large-box bin
     redistance_grain_s<R, kRedistSmemBytes>(C, S, g, s_raw);
 }
 
 // The large-box bin of the batched form: a persistent grid walks the work
 // queue (largest boxes first) and stops at the first existing grain at or
-// below kRedistBigEdge; k_redistance_s follows it on the same stream (run
+// below C.big_edge; k_redistance_s follows it on the same stream (run
 // side by side, the two measured slower: the 64-thread kernel's blocks take
 // the SMs first).
 __global__ void __launch_bounds__(kRedistBigThreads) k_redistance_big(NetConst C, NetState* S) {
@@ -1455,7 +1455,7 @@ __global__ void __launch_bounds__(kRedistBigThreads) k_redistance_big(NetConst C
         // a grain that vanished in this step's level set keeps its place in
         // the queue; existing grains are in descending box edge
         if (C.state[g] != G_EXISTS || halted(S)) continue;
-        if (box_w(S->box_cur[g]) <= kRedistBigEdge) return;
+        if (box_w(S->box_cur[g]) <= C.big_edge) return;
         redistance_grain_s<float, kRedistBigSmemBytes>(C, S, g, s_raw);
         __syncthreads();  // the next grain reuses the shared buffers
     }

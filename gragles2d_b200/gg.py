@@ -30,7 +30,8 @@ EXPORTS = (
     "gg_convolution", "gg_update_second_order_neighbors", "gg_comparison", "gg_level_set", "gg_redistancing",
     "gg_grain_count", "gg_step", "gg_status", "gg_read_grain_stats", "gg_tangent_enable", "gg_read_area_tangents",
     "gg_write_analysis", "gg_write_restart", "gg_dims", "gg_dump", "gg_last_step_ms",
-    "gg_grain_updates", "gg_profile_steps", "gg_traffic", "gg_kernel_launches", "gg_convolve_box_static",
+    "gg_grain_updates", "gg_profile_steps", "gg_traffic", "gg_autotune", "gg_kernel_launches",
+    "gg_convolve_box_static",
 )
 STATIC_CONV_MAX_N = 128
 NSTAGES = 9
@@ -70,6 +71,13 @@ class Params(ctypes.Structure):
         ("magnetic_force_field", ctypes.c_double), ("grid_coarsement_gradient", ctypes.c_double),
         ("arena_factor", ctypes.c_double),
         ("read_from_filename", ctypes.c_char * 512), ("additional_filename", ctypes.c_char * 512),
+    ]
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [
+        ("compare_threads", ctypes.c_int32), ("big_edge", ctypes.c_int32), ("conv_smem_edge", ctypes.c_int32),
+        ("steps_run", ctypes.c_int32), ("ms_default", ctypes.c_double), ("ms_tuned", ctypes.c_double),
     ]
 
 
@@ -128,6 +136,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "gg_profile_steps": (I, [V, I, I, P(D)]),
         "gg_traffic": (I, [V, P(ctypes.c_int64), P(ctypes.c_int64), P(I)]),
         "gg_kernel_launches": (I, [V, P(ctypes.c_int64), P(I)]),
+        "gg_autotune": (I, [V, I, I, P(Tuning)]),
         "gg_convolve_box_static": (I, [V, V, I, D, I, V]),
     }
     for name, (res, args) in sig.items():
@@ -400,6 +409,14 @@ class GrainHandler:
         a, o, n = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int32()
         self._check(self.lib.gg_traffic(self.ctx, ctypes.byref(a), ctypes.byref(o), ctypes.byref(n)))
         return a.value, o.value, n.value
+
+    def autotune(self, steps_per_candidate: int = 2) -> dict:
+        """Chooses the batched form's launch bins by timing whole steps with
+        each candidate (gg_autotune); the steps it runs advance the run."""
+        t = Tuning()
+        self._check(self.lib.gg_autotune(self.ctx, self.loop, steps_per_candidate, ctypes.byref(t)))
+        self.loop += t.steps_run
+        return {f: getattr(t, f) for f, _ in Tuning._fields_}
 
     def kernel_launches(self) -> tuple[int, int]:
         """(kernels launched by step() graph replays so far, kernel nodes per

@@ -299,7 +299,8 @@ int gg_grain_updates(gg_ctx* ctx, int64_t* updates);
 /* Runs nsteps whole steps stage by stage with CUDA events between stages
  * and adds the device milliseconds of each stage to stage_ms[GG_NSTAGES]:
  * convolution, corrector, second-order lists, comparison, level set,
- * arena allocation, volume/energy/neighbours, redistancing, end of step
+ * arena allocation, volume/energy/neighbours (in the batched form with the
+ * next step's corrector sectors), redistancing, end of step
  * (the reference's stage timers, src/grainhdl.cpp:1146-1154). */
 #define GG_NSTAGES 9
 int gg_profile_steps(gg_ctx* ctx, int32_t loop, int32_t nsteps, double* stage_ms);
@@ -308,6 +309,29 @@ int gg_profile_steps(gg_ctx* ctx, int32_t loop, int32_t nsteps, double* stage_ms
  * existing grains, sum over grains of the overlap areas with their
  * comparison-list members, and the number of existing grains. */
 int gg_traffic(gg_ctx* ctx, int64_t* sum_area, int64_t* sum_overlap, int32_t* n_exists);
+
+/* Launch bins of the batched form, as gg_autotune chose them. */
+typedef struct gg_tuning {
+    int32_t compare_threads;  /* threads per CTA of the comparison */
+    int32_t big_edge;         /* boxes with a larger edge go to the large-box redistancing kernel */
+    int32_t conv_smem_edge;   /* the convolution keeps its intermediate in shared memory up to this edge */
+    int32_t steps_run;        /* timesteps the sweep ran (the network advanced by them) */
+    double ms_default;        /* device ms per step with the bins the context started with */
+    double ms_tuned;          /* device ms per step with the chosen bins */
+} gg_tuning;
+
+/* Autotuner of the batched form's launch bins (no counterpart in the
+ * reference, whose grain schedulers, src/SquaresGrainScheduler.cpp:24-147
+ * and src/IterativeGrainScheduler.cpp:13-30, split grains among threads
+ * statically).  Runs whole timesteps from `loop` as gg_step does, each
+ * candidate for steps_per_candidate steps (0: 2), one knob at a time: the
+ * large-box redistancing bin edge, the comparison's threads per CTA and the
+ * convolution's shared-memory edge; a candidate is kept when it is more than
+ * 1% faster.  No bin changes any result, so the steps it runs are ordinary
+ * steps of the run.  The choice is kept for the context and, for the
+ * process, for later contexts with the same largest box edge and grain
+ * count.  The plain form returns at once (nothing to tune). */
+int gg_autotune(gg_ctx* ctx, int32_t loop, int32_t steps_per_candidate, gg_tuning* out);
 
 /* Kernels launched by gg_step's graph replays so far (batched form): the
  * kernel nodes of the captured step graph, counted when it is captured,

@@ -81,3 +81,37 @@ def test_100000_clustered_grains_batched(cases):
     assert r["edges"].min() <= 24 and r["edges"].max() >= 200
     assert abs(r["a0"] - 1.0) < 2e-3
     assert abs(np.nansum(r["areas"]) - r["a0"]) < 1e-3
+
+
+def test_100000_clustered_autotuned_bins(cases):
+    """The launch bins chosen by gg_autotune on the clustered network (box
+    edges 16 to ~250): the same areas bit for bit as the default bins after
+    the same number of steps, and a step no slower than with the defaults."""
+    xml = cases["c3"]
+
+    def start():
+        h = gg.GrainHandler(gg.Settings(xml, precision=gg.PRECISION_BATCHED), device=0)
+        h.load_voxel_files()
+        h.distanceInitialisation()
+        h.find_neighbors()
+        return h
+
+    hd = start()  # default bins (before any tuning is cached for this network size)
+    ht = start()
+    try:
+        info = ht.autotune(1)
+        assert info["steps_run"] >= 2 and info["ms_tuned"] <= info["ms_default"]
+        total = info["steps_run"] + 2
+        ht.step(2)
+        hd.step(total)
+        a, b = hd.areas(), ht.areas()
+        assert np.array_equal(np.isnan(a), np.isnan(b))
+        m = np.isfinite(a)
+        assert np.array_equal(a[m].view(np.uint64), b[m].view(np.uint64))
+        ms_d, ms_t = hd.step(3) / 3, ht.step(3) / 3
+        print({"tuned": info, "ms_default": ms_d, "ms_tuned": ms_t})
+        assert ms_t <= 1.03 * ms_d
+        assert hd.status() == 0 and ht.status() == 0
+    finally:
+        hd.close()
+        ht.close()
