@@ -68,6 +68,14 @@ struct gg_ctx {
     std::vector<void*> allocs;
     gg_grain_stats* d_stats = nullptr;  // packed statistics (device) and their pinned host copy
     gg_grain_stats* h_stats = nullptr;
+    // statistics prefetch: once a caller has read the statistics, every
+    // gg_step gathers them and copies them, with the status word, into
+    // pinned memory after its timed region; a read with nothing changed since
+    // takes them from there
+    bool stats_wanted = false;
+    bool stats_fresh = false;
+    uint32_t* h_status = nullptr;
+    cudaEvent_t ev_done = nullptr;
     LaunchCfg cfg{256, 256, 128, 64};
 
     cudaGraphExec_t graph = nullptr;
@@ -86,6 +94,8 @@ struct gg_ctx {
             cudaStreamSynchronize(stream);
         }
         if (h_stats) cudaFreeHost(h_stats);
+        if (h_status) cudaFreeHost(h_status);
+        if (ev_done) cudaEventDestroy(ev_done);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         for (cudaEvent_t e : fork)
@@ -289,14 +299,11 @@ double gaussian_multiplier(int n, int i2, int j2, double dt, int nn) {
     return exp(-sqrt(2 / kPiH) * (i2 * i2 + j2 * j2) * 4.0 * dt * nsq / n_nsq * kPiH * kPiH) / n_nsq;
 }
 
-int check_status(gg_ctx* c) {
+int status_error(gg_ctx* c, uint32_t st) {
     // Capacity overflows invalidate the state and are errors.  The remaining
     // bits mark inputs on which the reference itself would fault or never
     // return (see GG_S_* in gg_step.h); they are kept in the status word for
     // gg_status() and do not stop the run.
-    uint32_t st = 0;
-    GG_CUDA(c, cudaMemcpyAsync(&st, &c->dS->status, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
-    GG_CUDA(c, cudaStreamSynchronize(c->stream));
     if (st & (S_ARENA_FULL | S_LIST_OVERFLOW | S_CONTOUR_OVERFLOW | S_JUNCTION_OVERFLOW | S_TABLE_RANGE |
               S_NEIGHBOUR_OVERFLOW)) {
         char buf[128];
@@ -309,6 +316,13 @@ int check_status(gg_ctx* c) {
         return fail(c, GG_E_NUMERIC, buf);
     }
     return GG_OK;
+}
+
+int check_status(gg_ctx* c) {
+    uint32_t st = 0;
+    GG_CUDA(c, cudaMemcpyAsync(&st, &c->dS->status, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
+    GG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return status_error(c, st);
 }
 
 int refresh_state(gg_ctx* c) {
@@ -934,6 +948,7 @@ void apply_cached_tuning(gg_ctx* c) {
 
 int gg_distance_initialisation(gg_ctx* c) {
     if (!c) return GG_E_INVALID;
+    c->stats_fresh = false;
     if (!c->loaded) return fail(c, GG_E_STATE, "no microstructure loaded");
     if (c->initialised) return fail(c, GG_E_STATE, "already initialised");
     GG_CUDA(c, cudaSetDevice(c->device));
@@ -1374,6 +1389,7 @@ int gg_distance_initialisation(gg_ctx* c) {
 
 int gg_find_neighbors(gg_ctx* c) {
     if (!c) return GG_E_INVALID;
+    c->stats_fresh = false;
     if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
     c->sectors_stale = c->P.precision != GG_PRECISION_PLAIN;  // junction weights read the neighbour lists
     GG_CUDA(c, find_neighbors_launch(c->C, c->dS, c->stream));
@@ -1382,6 +1398,7 @@ int gg_find_neighbors(gg_ctx* c) {
 
 int gg_set_neighbours(gg_ctx* c, const int32_t* offsets, const int32_t* ids) {
     if (!c || !offsets || !ids) return GG_E_INVALID;
+    c->stats_fresh = false;
     if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
     const int N = c->N, K = c->C.kmax;
     c->sectors_stale = c->P.precision != GG_PRECISION_PLAIN;
@@ -1419,6 +1436,7 @@ int gg_set_neighbours(gg_ctx* c, const int32_t* offsets, const int32_t* ids) {
 namespace {
 int run_stage(gg_ctx* c, int stages, bool setloop, int loop) {
     if (!c) return GG_E_INVALID;
+    c->stats_fresh = false;
     if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
     if (setloop) {
         int r = set_loop(c, loop);
@@ -1432,6 +1450,7 @@ int run_stage(gg_ctx* c, int stages, bool setloop, int loop) {
 
 int gg_convolution(gg_ctx* c, int32_t loop) {
     if (!c) return GG_E_INVALID;
+    c->stats_fresh = false;
     if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
     bool coarsened = false;
     const int rc = coarsen_if_due(c, loop, &coarsened);  // the first stage of a loop (src/grainhdl.cpp:1053)
@@ -1529,6 +1548,7 @@ int gg_step(gg_ctx* c, int32_t loop, int32_t nsteps) {
     if (!c) return GG_E_INVALID;
     if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
     if (nsteps <= 0) return GG_OK;
+    c->stats_fresh = false;
     if (c->P.grid_coarsement && nsteps > 1) {
         // the coarsening test needs the grain count between steps
         double total = 0;
@@ -1584,6 +1604,24 @@ int gg_step(gg_ctx* c, int32_t loop, int32_t nsteps) {
         }
         GG_CUDA(c, cudaEventRecord(c->ev1, c->stream));
     }
+    if (c->stats_wanted) {
+        // after the timed region: the statistics and the status word in one
+        // pinned copy each, then one wait for all of it
+        if (!c->h_status) GG_CUDA(c, cudaMallocHost(&c->h_status, sizeof(uint32_t)));
+        if (!c->ev_done) GG_CUDA(c, cudaEventCreateWithFlags(&c->ev_done, cudaEventDisableTiming));
+        GG_CUDA(c, pack_stats(c->C, c->dS, c->d_stats, c->stream));
+        GG_CUDA(c, cudaMemcpyAsync(c->h_stats, c->d_stats, sizeof(gg_grain_stats) * (size_t)c->N,
+                                   cudaMemcpyDeviceToHost, c->stream));
+        GG_CUDA(c, cudaMemcpyAsync(c->h_status, &c->dS->status, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+        GG_CUDA(c, cudaEventRecord(c->ev_done, c->stream));
+        GG_CUDA(c, cudaEventSynchronize(c->ev_done));
+        float ms = 0;
+        GG_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+        c->last_ms = ms;
+        const int rc2 = status_error(c, *c->h_status);
+        if (rc2 == GG_OK) c->stats_fresh = true;
+        return rc2;
+    }
     GG_CUDA(c, cudaEventSynchronize(c->ev1));
     float ms = 0;
     GG_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
@@ -1611,6 +1649,7 @@ int gg_grain_updates(gg_ctx* c, int64_t* updates) {
 
 int gg_profile_steps(gg_ctx* c, int32_t loop, int32_t nsteps, double* stage_ms) {
     if (!c || !stage_ms) return GG_E_INVALID;
+    c->stats_fresh = false;
     if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
     if (c->tangents) return fail(c, GG_E_STATE, "stage profiling runs without tangents");
     int rc = set_loop(c, loop);
@@ -1921,6 +1960,11 @@ int gg_read_grain_stats(gg_ctx* c, gg_grain_stats* out, int32_t capacity) {
     if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
     if (capacity < c->N) return fail(c, GG_E_INVALID, "capacity smaller than the grain count");
     const int N = c->N;
+    c->stats_wanted = true;
+    if (c->stats_fresh) {  // gathered and copied by the step that just ran
+        std::memcpy(out, c->h_stats, sizeof(gg_grain_stats) * (size_t)N);
+        return GG_OK;
+    }
     // gathered on the device, one copy through a pinned buffer
     if (!c->d_stats) {
         int rc = dalloc(c, &c->d_stats, (size_t)N);

@@ -656,7 +656,7 @@ __device__ int extract_bitmap_warp(const Field<R>& f, const uint32_t* idl, uint3
 // grainhdl::level_set -> LSbox::extractContour (src/grainhdl.cpp:830-848,
 // src/box.cpp:1089-1153), one warp per grain.
 template <typename R>
-__global__ void __launch_bounds__(32 * kGrainsPerBlock) k_levelset_w(NetConst C, NetState* S) {
+__global__ void __launch_bounds__(32 * kGrainsPerBlock, 5) k_levelset_w(NetConst C, NetState* S) {
     __shared__ double2 s_xy[kGrainsPerBlock][kWalkPts];
     __shared__ WalkShared s_walk[kGrainsPerBlock];
     const int lane = threadIdx.x & 31;
