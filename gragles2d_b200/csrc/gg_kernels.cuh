@@ -225,6 +225,15 @@ __global__ void __launch_bounds__(256) k_compare(NetConst C, NetState* S) {
     const R tube = (R)(0.7 * C.delta);
 
     int xmin = bc.x1, xmax = bc.x0, ymin = bc.y1, ymax = bc.y0;
+    // Outside the 0.7 delta tube the compared value is the grain's own value
+    // whatever its neighbours hold; there the neighbours' maximum only sets
+    // IDLocal.  In the batched form without driving-force terms every reader
+    // of IDLocal (junction corners of the contour walk, the neighbour probes,
+    // the corrector's default weights and sector samples) looks within a few
+    // cells of the zero crossing, well inside the tube, so pixels outside it
+    // skip the neighbours (their IDLocal keeps its initial value).  The plain
+    // form computes IDLocal everywhere, as the reference does.
+    const bool skip_outside = sizeof(R) == sizeof(float) && !C.stored && !C.magnetic;
     // one warp per 8 x 4 tile: the warp first picks the list members whose
     // boxes meet the tile, then every lane takes the maximum over those (in
     // list order, strict '>') with four members' loads in flight
@@ -249,7 +258,9 @@ __global__ void __launch_bounds__(256) k_compare(NetConst C, NetState* S) {
         uint32_t id = inside && p < keep ? idp[p] : 0u;
         const R in = inside ? self[p] : (R)0;
         R out = (R)-1.0;
-        for (int k0 = 0; k0 < nl; k0 += 32) {
+        const bool want = inside && !(skip_outside && !(fabs(in) < tube));  // needs the neighbours' maximum
+        const int nlt = __any_sync(FULL, want) ? nl : 0;
+        for (int k0 = 0; k0 < nlt; k0 += 32) {
             bool hit = false;
             if (k0 + lane < nl) {
                 const Box bk = s_box[k0 + lane];
@@ -272,7 +283,7 @@ __global__ void __launch_bounds__(256) k_compare(NetConst C, NetState* S) {
                 for (int u = 0; u < 4; ++u) {
                     ok[u] = false;
                     ds[u] = (R)0;
-                    if (ks[u] >= 0 && inside) {
+                    if (ks[u] >= 0 && want) {
                         const Box bk = s_box[ks[u]];
                         if (i >= bk.y0 && i < bk.y1 && j >= bk.x0 && j < bk.x1) {
                             ok[u] = true;
