@@ -653,11 +653,13 @@ void launch_redistance(const NetConst& C, NetState* dS, cudaStream_t s) {
 cudaError_t batched_init(const NetConst& C, NetState* dS, const int32_t* d_ids, cudaStream_t s) {
     if (C.N <= 0) return cudaSuccess;
     k_init_phi<float><<<C.N, 256, 0, s>>>(C, dS, d_ids);
-    k_redistance<float><<<C.N, 256, 0, s>>>(C, dS);
+    // the step's redistancing kernels take grains from the work queue, so it
+    // is built from the initial boxes first
+    k_order<<<1, 1024, 0, s>>>(C, dS);
+    launch_redistance(C, dS, s);
     cudaError_t e = swap_phi(dS, s);
     if (e != cudaSuccess) return e;
-    const int gt = 64;
-    k_init_contour<float><<<(C.N + gt - 1) / gt, gt, 0, s>>>(C, dS);
+    k_init_contour_w<float><<<(C.N + kGrainsPerBlock - 1) / kGrainsPerBlock, 32 * kGrainsPerBlock, 0, s>>>(C, dS);
     return cudaGetLastError();
 }
 

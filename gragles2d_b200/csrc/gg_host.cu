@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <map>
+#include <tuple>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -500,13 +501,71 @@ int launch_stages(gg_ctx* c, int stages) {
     return GG_OK;
 }
 
+// The tables of one box edge depend only on (form, edge, dt, grid size);
+// every context of the process computes each such table once.
+struct TableKey {
+    int plain, n;
+    uint64_t dt_bits;
+    int nn;
+    bool operator<(const TableKey& o) const {
+        return std::tie(plain, n, dt_bits, nn) < std::tie(o.plain, o.n, o.dt_bits, o.nn);
+    }
+};
+std::mutex g_table_mutex;
+std::map<TableKey, std::vector<double>> g_gk_cache;
+std::map<TableKey, std::vector<float>> g_ck_cache;
+
+TableKey table_key(const gg_ctx* c, int n) {
+    uint64_t bits;
+    std::memcpy(&bits, &c->dt, sizeof bits);
+    return TableKey{c->P.precision == GG_PRECISION_PLAIN ? 1 : 0, n, bits, c->nn};
+}
+
 // Gaussian multipliers (plain form) or separable real-space kernels with their
 // band radius (batched form) of every box edge up to tmax, for the context's
 // current dt and grid size (both change when the grid is coarsened).
+void conv_tables_compute(const gg_ctx* c, int tmax, const std::vector<int64_t>& gk_off,
+                         const std::vector<int64_t>& ck_off, std::vector<double>& gk, std::vector<float>& ck,
+                         int nlo);
+
 void conv_tables(const gg_ctx* c, int tmax, const std::vector<int64_t>& gk_off, const std::vector<int64_t>& ck_off,
                  std::vector<double>& gk, std::vector<float>& ck) {
+    const bool plain = c->P.precision == GG_PRECISION_PLAIN;
+    for (int n = 1; n <= tmax; ++n) {
+        const TableKey key = table_key(c, n);
+        {
+            std::lock_guard<std::mutex> lock(g_table_mutex);
+            if (plain) {
+                const auto it = g_gk_cache.find(key);
+                if (it != g_gk_cache.end()) {
+                    std::copy(it->second.begin(), it->second.end(), gk.begin() + gk_off[n]);
+                    continue;
+                }
+            } else {
+                const auto it = g_ck_cache.find(key);
+                if (it != g_ck_cache.end()) {
+                    std::copy(it->second.begin(), it->second.end(), ck.begin() + ck_off[n]);
+                    continue;
+                }
+            }
+        }
+        conv_tables_compute(c, n, gk_off, ck_off, gk, ck, n);
+        std::lock_guard<std::mutex> lock(g_table_mutex);
+        if (plain) {
+            const int64_t len = (int64_t)(n / 2 + 1) * (n / 2 + 1);
+            g_gk_cache[key].assign(gk.begin() + gk_off[n], gk.begin() + gk_off[n] + len);
+        } else {
+            g_ck_cache[key].assign(ck.begin() + ck_off[n], ck.begin() + ck_off[n] + n + 1);
+        }
+    }
+}
+
+// Edges nlo .. tmax.
+void conv_tables_compute(const gg_ctx* c, int tmax, const std::vector<int64_t>& gk_off,
+                         const std::vector<int64_t>& ck_off, std::vector<double>& gk, std::vector<float>& ck,
+                         int nlo) {
     if (c->P.precision == GG_PRECISION_PLAIN) {
-        for (int n = 1; n <= tmax; ++n) {
+        for (int n = nlo; n <= tmax; ++n) {
             const int half = n / 2 + 1;
             for (int i2 = 0; i2 < half; ++i2)
                 for (int j2 = i2; j2 < half; ++j2)  // G(i2, j2) = G(j2, i2): i2^2 + j2^2 is the argument
@@ -518,7 +577,7 @@ void conv_tables(const gg_ctx* c, int tmax, const std::vector<int64_t>& gk_off, 
         // k_n[r] = (1/n) sum_f g(min(f, n-f)) cos(2 pi f r / n), g(f) = exp(-kappa f^2),
         // kappa = sqrt(2/pi) 4 dt nn^2 / n^2 pi^2 (the 1/n^2 of G split over both axes)
         std::vector<double> gf, cs;
-        for (int n = 1; n <= tmax; ++n) {
+        for (int n = nlo; n <= tmax; ++n) {
             const double kappa = sqrt(2 / kPiH) * 4.0 * c->dt * (double)c->nn * (double)c->nn / ((double)n * n) *
                                  kPiH * kPiH;
             gf.assign(n, 0.0);

@@ -758,6 +758,53 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock, 5) k_levelset_w(NetConst
     S->jn_cur[g] = o.jn;
 }
 
+// Initial contours of a voxelized network (distanceInitialisation ->
+// LSbox::extractContour on the initial distance field, as k_init_contour
+// does one thread per grain): one warp per grain with the level set's
+// warp-parallel extraction (bitmap walk, points, junctions and their
+// projection across the lanes), into the previous-step roles the first
+// corrector reads.
+template <typename R>
+__global__ void __launch_bounds__(32 * kGrainsPerBlock, 5) k_init_contour_w(NetConst C, NetState* S) {
+    __shared__ double2 s_xy[kGrainsPerBlock][kWalkPts];
+    __shared__ WalkShared s_walk[kGrainsPerBlock];
+    const int lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5;
+    const int g = blockIdx.x * kGrainsPerBlock + wid + 1;
+    if (g > C.N || C.state[g] != G_EXISTS || halted(S)) return;
+    double2* xy = s_xy[wid];
+    Field<R> f{phiA_of<R>(S) + S->off_cur[g], S->box_cur[g]};
+    const uint32_t* idl = S->idPrev + S->off_prev[g];
+    ContourOut o{S->contPrev + S->coff_prev[g], S->ccap_prev[g], 0, S->jPrev + (int64_t)g * C.jmax, C.jmax, 0, 0};
+    bool shared = true;
+    const bool ok = extract_warp(f, idl, (uint32_t)g, o, lane, xy, &shared, &s_walk[wid]);
+    double vol = 0;
+    if (ok && shared) {
+        for (int i = lane; i < o.n; i += 32) {
+            CPoint q;
+            q.x = xy[i].x;
+            q.y = xy[i].y;
+            q.energy = -1.0;
+            q.mob = -1.0;
+            o.pts[i] = q;
+        }
+        vol = volume_xy(xy, o.n, C.h);
+    }
+    if (lane != 0) return;
+    if (o.status) set_status(S, o.status);
+    if (!ok) {
+        C.state[g] = G_VANISHED;
+        S->cn_prev[g] = 0;
+        S->jn_prev[g] = 0;
+        C.volume[g] = 0;
+        return;
+    }
+    if (!shared) vol = contour_volume(o.pts, o.n, C.h);
+    S->cn_prev[g] = o.n;
+    S->jn_prev[g] = o.jn;
+    C.volume[g] = vol;
+}
+
 // Per contour point result of the neighbour probe of buildDirectNeighbours.
 struct PointInfo {
     int32_t cid;
