@@ -180,7 +180,7 @@ size_t conv_sep_smem(int tmax, int edge) {
 // coordinates) and the per-pixel work in FP32, except the discrete decisions
 // of the projection, which follow the reference's FP64 arithmetic.  Each
 // warp takes one 8 x 4 tile of the box at a time.
-constexpr int kCorrMaxPts = 512;  // contours staged in FP32 up to this length
+constexpr int kCorrMaxPts = 1024;  // contours staged in FP32 up to this length
 
 // Packed FP32 pairs (sm_100 f32x2 arithmetic).
 __device__ __forceinline__ unsigned long long f2_pack(float a, float b) {
@@ -259,7 +259,7 @@ __device__ __forceinline__ double dist2_rn(double px, double py, const CPoint& q
 
 __device__ __forceinline__ float tie_margin(float d, float eps_c) { return (sqrtf(d) + 1.f) * eps_c + d * 1e-6f; }
 
-constexpr unsigned kKeyIndexBits = 9;
+constexpr unsigned kKeyIndexBits = 10;
 constexpr unsigned kKeyIndexMask = (1u << kKeyIndexBits) - 1u;
 static_assert(kBucketPts <= (1 << kKeyIndexBits), "vertex index must fit the key");
 
@@ -269,7 +269,7 @@ static_assert(kBucketPts <= (1 << kKeyIndexBits), "vertex index must fit the key
 // 3 x 3 cell windows in FP32 on the staged box-local contour P32 (each
 // coordinate within 2^-24 L of the exact local value, L the box edge, so a
 // squared distance d within 3 sqrt(d) 2^-24 L + 3e-7 d of the exact one):
-// each candidate is one 32-bit key, the distance's bits with the low 9
+// each candidate is one 32-bit key, the distance's bits with the low 10
 // replaced by the vertex index, and a lane keeps its smallest key k1 and the
 // second smallest k2.  A lane whose two best lie within twice the rounding
 // bound (tie_margin with eps_c = 8 2^-24 L; the keys' truncation taken on

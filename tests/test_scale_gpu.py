@@ -51,9 +51,12 @@ def _run(xml, precision, steps):
         a0 = np.nansum([s.area for s in h.grain_stats() if s.state == 1])
         h.step(steps)
         st = h.grain_stats()
+        live = [s for s in st if s.state == 1]
         areas = np.array([s.area if s.state == 1 else np.nan for s in st])
-        edges = np.array([s.box[1] - s.box[0] for s in st if s.state == 1])
-        return {"status": h.status(), "a0": a0, "areas": areas, "edges": edges}
+        edges = np.array([s.box[1] - s.box[0] for s in live])
+        return {"status": h.status(), "a0": a0, "areas": areas, "edges": edges,
+                "neighbours": np.array([s.n_neighbours for s in live]),
+                "points": np.array([s.contour_points for s in live])}
     finally:
         h.close()
 
@@ -79,6 +82,13 @@ def test_100000_clustered_grains_batched(cases):
     r = _run(cases["c3"], gg.PRECISION_BATCHED, 3)
     assert r["status"] == 0
     assert r["edges"].min() <= 24 and r["edges"].max() >= 200
+    # headroom of the fixed per-grain capacities on the largest grains: direct
+    # neighbours (48 rows), contour points (8 n + 64 for a box of edge n)
+    cap_points = 8 * r["edges"] + 64
+    print({"max_edge": int(r["edges"].max()), "max_neighbours": int(r["neighbours"].max()),
+           "max_points": int(r["points"].max()), "max_points_over_capacity": float((r["points"] / cap_points).max())})
+    assert r["neighbours"].max() <= 36  # of 48
+    assert (r["points"] / cap_points).max() <= 0.75
     assert abs(r["a0"] - 1.0) < 2e-3
     assert abs(np.nansum(r["areas"]) - r["a0"]) < 1e-3
 
