@@ -46,17 +46,19 @@ def _areas(h: gg.GrainHandler) -> np.ndarray:
     return np.array([s.area if s.state == 1 else np.nan for s in h.grain_stats()])
 
 
-def trajectory(xml: str, steps: int, every: int, device: int = 0, floor: bool = True, inputs=None) -> list[dict]:
+def trajectory(xml: str, steps: int, every: int, device: int = 0, floor: bool = True, inputs=None,
+               floor_scale: float = FLOOR_SCALE) -> list[dict]:
     """Runs the plain FP64 form, the batched FP32 form and (with `floor`) the
-    perturbed plain form for `steps` steps from the voxelized input of `xml`
-    (or the host arrays `inputs` = (ids, euler, bbox)); every `every` steps
-    records the batched form's errors against the plain form ("fp32") and the
-    perturbed plain form's ("fp64_perturbed")."""
+    perturbed plain form (boundary energies times `floor_scale`) for `steps`
+    steps from the voxelized input of `xml` (or the host arrays `inputs` =
+    (ids, euler, bbox)); every `every` steps records the batched form's
+    errors against the plain form ("fp32") and the perturbed plain form's
+    ("fp64_perturbed")."""
     runs = {"fp64": gg.Settings(xml, precision=gg.PRECISION_PLAIN),
             "fp32": gg.Settings(xml, precision=gg.PRECISION_BATCHED)}
     if floor:
         s = gg.Settings(xml, precision=gg.PRECISION_PLAIN)
-        s.p.gamma_hagb = s.p.gamma_hagb * FLOOR_SCALE
+        s.p.gamma_hagb = s.p.gamma_hagb * floor_scale
         runs["fp64_perturbed"] = s
     hs = {}
     try:

@@ -179,8 +179,11 @@ size_t conv_sep_smem(int tmax, int edge) {
 // with the previous contour staged in shared memory (FP32 box-local
 // coordinates) and the per-pixel work in FP32, except the discrete decisions
 // of the projection, which follow the reference's FP64 arithmetic.  Each
-// warp takes one 8 x 4 tile of the box at a time.
-constexpr int kCorrMaxPts = 1024;  // contours staged in FP32 up to this length
+// warp takes one 8 x 4 tile of the box at a time.  The main kernel stages
+// contours up to kCorrStagedPts points; the large-contour kernel, persistent
+// over NetState::big_list, up to kCorrBigPts; longer ones are read from
+// device memory in FP64.
+constexpr int kCorrBigPts = 1024;
 
 // Packed FP32 pairs (sm_100 f32x2 arithmetic).
 __device__ __forceinline__ unsigned long long f2_pack(float a, float b) {
@@ -202,14 +205,15 @@ __device__ __forceinline__ void f2_unpack(unsigned long long v, float& a, float&
 // over the whole contour; ties go to the lowest index, as the reference's
 // strict < over ascending k.  Otherwise the pixel scans every vertex.
 constexpr int kCellMax = 24;          // cells per side
-constexpr int kBucketPts = kCorrMaxPts;  // vertices bucketed (the staged contours)
+template <int kPts>  // vertices bucketed (the staged contours)
 struct VertexBuckets {
     int ncx, ncy, cell;
     int end[kCellMax * kCellMax + 1];  // after the fill: end[c + 1] = first vertex of cell c
-    short list[kBucketPts];
+    short list[kPts];
 };
 
-__device__ __forceinline__ int bucket_of(const VertexBuckets& B, double lx, double ly) {
+template <int kPts>
+__device__ __forceinline__ int bucket_of(const VertexBuckets<kPts>& B, double lx, double ly) {
     int cx = (int)floor(lx / B.cell), cy = (int)floor(ly / B.cell);
     cx = cx < 0 ? 0 : (cx >= B.ncx ? B.ncx - 1 : cx);
     cy = cy < 0 ? 0 : (cy >= B.ncy ? B.ncy - 1 : cy);
@@ -218,7 +222,8 @@ __device__ __forceinline__ int bucket_of(const VertexBuckets& B, double lx, doub
 
 // All threads: buckets of the vertices 0 .. npts-1 (P[k] in grid
 // coordinates, origin (ox, oy)).  Ends with a barrier.
-__device__ void build_buckets(VertexBuckets& B, const CPoint* P, int npts, int ox, int oy, int wi, int hi) {
+template <int kPts>
+__device__ void build_buckets(VertexBuckets<kPts>& B, const CPoint* P, int npts, int ox, int oy, int wi, int hi) {
     const int cs = max(4, (max(wi, hi) + kCellMax - 1) / kCellMax);
     const int ncx = (wi + cs - 1) / cs, ncy = (hi + cs - 1) / cs, nc = ncx * ncy;
     if (threadIdx.x == 0) {
@@ -261,7 +266,7 @@ __device__ __forceinline__ float tie_margin(float d, float eps_c) { return (sqrt
 
 constexpr unsigned kKeyIndexBits = 10;
 constexpr unsigned kKeyIndexMask = (1u << kKeyIndexBits) - 1u;
-static_assert(kBucketPts <= (1 << kKeyIndexBits), "vertex index must fit the key");
+static_assert(kCorrStagedPts <= kCorrBigPts && kCorrBigPts <= (1 << kKeyIndexBits), "vertex index must fit the key");
 
 // The reference's nearest vertex of the pixels (px, py) of the 32 lanes of a
 // warp (grid coordinates; all lanes call it, `need` lanes are the pixels
@@ -277,7 +282,8 @@ static_assert(kBucketPts <= (1 << kKeyIndexBits), "vertex index must fit the key
 // the contour itself, lowest index first at equal distance.  A lane whose
 // best distance exceeds (cell - 1e-3)^2 scans every vertex in FP64 (a vertex
 // within `cell` of the pixel lies in its window).
-__device__ int nearest_vertex_warp(const VertexBuckets& B, const float2* P32, const CPoint* P, int npts, int px,
+template <int kPts>
+__device__ int nearest_vertex_warp(const VertexBuckets<kPts>& B, const float2* P32, const CPoint* P, int npts, int px,
                                    int py, int ox, int oy, float eps_c, bool need) {
     const unsigned FULL = 0xffffffffu;
     const int cs = B.cell;
@@ -452,24 +458,41 @@ __global__ void __launch_bounds__(32) k_sectors(NetConst C, NetState* S) {
     }
 }
 
-template <bool kForces>
-__global__ void __launch_bounds__(128, 7) k_corrector_f(NetConst C, NetState* S) {
-    const int g = grain_at(S, blockIdx.x);
-    if (g > C.N || C.state[g] != G_EXISTS || C.regular[g] == 0 || S->loop == 0 || halted(S)) return;
-    __shared__ __align__(16) float2 sp[kCorrMaxPts];
-    __shared__ NbTable nbt;
-    __shared__ VertexBuckets vb;
-    __shared__ double s_cw[kMaxConstSectors];
-    __shared__ InterpSector s_is[kMaxInterpSectors];
-    __shared__ int16_t s_sid[kCorrMaxPts];
-    __shared__ float s_acc[kCorrMaxPts];
+// Shared memory of one CTA of the batched corrector.
+template <int kPts>
+struct CorrectorSmem {
+    float2 sp[kPts];  // the contour, FP32 box-local
+    NbTable nbt;
+    VertexBuckets<kPts> vb;
+    double cw[kMaxConstSectors];
+    InterpSector is[kMaxInterpSectors];
+    int16_t sid[kPts];  // per-segment sector table
+    float acc[kPts];
+};
+
+// Whether grain g is corrected at all this step (uniform over the CTA).
+__device__ __forceinline__ bool corrects(const NetConst& C, const NetState* S, int g) {
+    return g <= C.N && C.state[g] == G_EXISTS && C.regular[g] != 0 && S->loop != 0 && !halted(S);
+}
+
+// The correction of grain g by the whole CTA (all threads call it; every
+// early return is uniform over the CTA).
+template <bool kForces, int kPts>
+__device__ __forceinline__ void correct_grain(const NetConst& C, NetState* S, int g, CorrectorSmem<kPts>& sm) {
+    float2* sp = sm.sp;
+    NbTable& nbt = sm.nbt;
+    VertexBuckets<kPts>& vb = sm.vb;
+    double* s_cw = sm.cw;
+    InterpSector* s_is = sm.is;
+    int16_t* s_sid = sm.sid;
+    float* s_acc = sm.acc;
     const int64_t coff = S->coff_prev[g];
     const CPoint* P = S->contPrev + coff;
     const int size = S->cn_prev[g];
     if (size < 2) return;
     const Box ib = S->box_prev[g];
     const uint32_t* idl = S->idPrev + S->off_prev[g];
-    const bool staged = size <= kCorrMaxPts;
+    const bool staged = size <= kPts;
     // the contour in FP32 coordinates local to the previous box (its points
     // lie inside it), so the search's rounding is relative to the box edge
     const int ox = ib.x0, oy = ib.y0;
@@ -612,12 +635,68 @@ __global__ void __launch_bounds__(128, 7) k_corrector_f(NetConst C, NetState* S)
     if (st) set_status(S, st);
 }
 
+// CTA per grain from the work queue, contours staged up to kCorrStagedPts;
+// grains flagged for the large-contour kernel are left to it.
+template <bool kForces>
+__global__ void __launch_bounds__(128, 7) k_corrector_f(NetConst C, NetState* S) {
+    __shared__ __align__(16) CorrectorSmem<kCorrStagedPts> sm;
+    const int g = grain_at(S, blockIdx.x);
+    if (!corrects(C, S, g) || S->big_flag[g]) return;
+    correct_grain<kForces, kCorrStagedPts>(C, S, g, sm);
+}
 
-void launch_corrector_f(const NetConst& C, NetState* dS, cudaStream_t s) {
+// Persistent over NetState::big_list: the grains whose contour is longer than
+// the main kernel stages, up to kCorrBigPts staged; CTA b takes entries b,
+// b + G, ... (G CTAs).  The grid (kCorrBigPerSm CTAs per SM) usually covers
+// the whole list, so every such grain starts at once, and the launch has the
+// device's highest priority, so that these CTAs are placed before the
+// pending ones of the main corrector beside them.
+template <bool kForces>
+__global__ void __launch_bounds__(128) k_corrector_big(NetConst C, NetState* S) {
+    __shared__ __align__(16) CorrectorSmem<kCorrBigPts> sm;
+    const int n = S->n_big;
+    for (int q = blockIdx.x; q < n; q += gridDim.x) {
+        const int g = S->big_list[q];
+        if (corrects(C, S, g)) correct_grain<kForces, kCorrBigPts>(C, S, g, sm);
+        __syncthreads();  // the next grain overwrites the shared memory
+    }
+}
+
+// persistent grid of the large-box kernels: one CTA per SM
+int g_big_grid = 148;
+// highest stream priority of the device (numerically lowest)
+int g_high_priority = 0;
+constexpr int kCorrBigPerSm = 4;
+
+void launch_corrector_main(const NetConst& C, NetState* dS, cudaStream_t s) {
     if (C.stored || C.magnetic)
         k_corrector_f<true><<<C.N, 128, 0, s>>>(C, dS);
     else
         k_corrector_f<false><<<C.N, 128, 0, s>>>(C, dS);
+}
+
+void launch_corrector_big(const NetConst& C, NetState* dS, cudaStream_t s) {
+    const int grid = C.N < kCorrBigPerSm * g_big_grid ? C.N : kCorrBigPerSm * g_big_grid;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(128);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributePriority;
+    attr[0].val.priority = g_high_priority;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (C.stored || C.magnetic)
+        cudaLaunchKernelEx(&cfg, k_corrector_big<true>, C, dS);
+    else
+        cudaLaunchKernelEx(&cfg, k_corrector_big<false>, C, dS);
+}
+
+// Both correctors on one stream (the graph runs them on two).
+void launch_corrector_f(const NetConst& C, NetState* dS, cudaStream_t s) {
+    launch_corrector_big(C, dS, s);
+    launch_corrector_main(C, dS, s);
 }
 
 cudaError_t batched_resample(const NetConst& C, NetState* dS, double h_old, double hn, double delta_old,
@@ -625,9 +704,6 @@ cudaError_t batched_resample(const NetConst& C, NetState* dS, double h_old, doub
     if (C.N > 0) k_resample<float><<<C.N, 256, 0, s>>>(C, dS, h_old, hn, delta_old);
     return cudaGetLastError();
 }
-
-// persistent grid of the large-box redistancing bin: one CTA per SM
-int g_big_grid = 148;
 
 cudaError_t batched_prepare(int tmax) {
     cudaError_t e = cudaFuncSetAttribute(k_conv_sep, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -639,6 +715,9 @@ cudaError_t batched_prepare(int tmax) {
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
     g_big_grid = sms > 0 ? sms : 148;
+    int least = 0, greatest = 0;
+    if ((e = cudaDeviceGetStreamPriorityRange(&least, &greatest)) != cudaSuccess) return e;
+    g_high_priority = greatest;
     return cudaSuccess;
 }
 
@@ -741,9 +820,15 @@ cudaError_t batched_step_graph(const NetConst& C, NetState* dS, cudaStream_t s, 
     if ((e = cudaEventRecord(ev[0], s)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(s2, ev[0], 0)) != cudaSuccess) return e;
     k_second_order_w<<<wblocks, 32 * kGrainsPerBlock, 0, s2>>>(C, dS);
-    if ((e = cudaEventRecord(ev[1], s2)) != cudaSuccess) return e;
     k_conv_sep<<<C.N, 128, conv_sep_smem(C.tmax, C.conv_smem_edge), s>>>(C, dS);
-    if (!C.isotropic) launch_corrector_f(C, dS, s);
+    if (!C.isotropic) {
+        // the large-contour corrector beside the main one
+        if ((e = cudaEventRecord(ev[4], s)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(s2, ev[4], 0)) != cudaSuccess) return e;
+        launch_corrector_big(C, dS, s2);
+        launch_corrector_main(C, dS, s);
+    }
+    if ((e = cudaEventRecord(ev[1], s2)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(s, ev[1], 0)) != cudaSuccess) return e;
     k_compare<float><<<C.N, cfg.compare_threads, 0, s>>>(C, dS);
     k_levelset_w<float><<<wblocks, 32 * kGrainsPerBlock, 0, s>>>(C, dS);

@@ -197,7 +197,7 @@ struct NetState {
     int32_t loop;
     uint32_t status;
     int32_t live;        // grains not removed (grainhdl::currentNrGrains)
-    int32_t pad;
+    int32_t n_big;       // entries of big_list
     double max_volume;
     unsigned long long updates;   // sum over steps of grains alive at step start
     unsigned long long t_area;    // traffic model scratch (k_traffic)
@@ -216,7 +216,17 @@ struct NetState {
     // descending box edge (rebuilt after every change of the boxes); null in
     // the plain form, whose launches take grains in ID order
     int32_t* order;
+    // batched form: grains whose previous contour is longer than the main
+    // corrector stages (kCorrStagedPts), flagged per grain and listed
+    // (n_big entries) for the large-contour corrector; rebuilt with the work
+    // queue, so each grain has exactly one corrector launch
+    int32_t* big_flag;
+    int32_t* big_list;
 };
+
+// Contour points the main batched corrector stages in shared memory; longer
+// contours go to the large-contour corrector.
+constexpr int kCorrStagedPts = 512;
 
 // The grain that work slot `slot` (0-based, < N) of a per-grain launch
 // processes: largest boxes first when the queue exists, else ID order.  Every

@@ -85,7 +85,7 @@ struct gg_ctx {
     int64_t kernel_launches = 0;   // graph_kernels per replay, summed
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaStream_t stream2 = nullptr;  // second branch of the captured batched step
-    cudaEvent_t fork[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t fork[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     double last_ms = 0;
 
     ~gg_ctx() {
@@ -787,7 +787,7 @@ int gg_create(const gg_params* p, int device, gg_ctx** out) {
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking);
-    for (int k = 0; k < 4 && e == cudaSuccess; ++k) e = cudaEventCreateWithFlags(&c->fork[k], cudaEventDisableTiming);
+    for (int k = 0; k < 5 && e == cudaSuccess; ++k) e = cudaEventCreateWithFlags(&c->fork[k], cudaEventDisableTiming);
     if (e != cudaSuccess) {
         c->err = std::string("stream/event: ") + cudaGetErrorString(e);
         *out = c;
@@ -1378,6 +1378,8 @@ int gg_distance_initialisation(gg_ctx* c) {
     S.cont_cap = cont_cap;
     S.loop = P.start_time;
     if (!plain) ALLOC(S.order, N + 1);  // the batched step's work queue
+    if (!plain) ALLOC(S.big_flag, N + 1);  // grains for the large-contour corrector
+    if (!plain) ALLOC(S.big_list, N + 1);
     ALLOC(c->dS, 1);
 
 #undef ALLOC
@@ -1642,7 +1644,8 @@ int gg_step(gg_ctx* c, int32_t loop, int32_t nsteps) {
                 e = cudaGraphNodeGetType(nodes[q], &t);
                 if (t == cudaGraphNodeTypeKernel) ++kn;
             }
-            if (e == cudaSuccess) e = cudaGraphInstantiate(&c->graph, gr, 0);
+            // per-node priorities: the large-contour corrector's CTAs go first
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&c->graph, gr, cudaGraphInstantiateFlagUseNodePriority);
             cudaGraphDestroy(gr);
             if (e != cudaSuccess) return cuda_fail(c, e, "graph instantiate");
             c->graph_kernels = kn;

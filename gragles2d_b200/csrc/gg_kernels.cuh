@@ -865,32 +865,84 @@ __global__ void __launch_bounds__(1024) k_finalize(NetConst C, NetState* S, int 
 // descending box edge, then the rest, by a counting sort in one CTA.  A
 // per-grain launch then starts its longest blocks first and the short ones
 // fill the last wave.  The order within one edge length is whatever the
-// shared-memory atomics give; no result depends on it.
+// shared-memory atomics give; no result depends on it.  The same pass flags
+// and lists the grains whose contour is longer than the main corrector
+// stages (NetState::big_flag, big_list).
 constexpr int kOrderBins = 256;
+static_assert(kOrderBins % 32 == 0, "the bin scan gives each lane kOrderBins / 32 bins");
 
 __global__ void __launch_bounds__(1024) k_order(NetConst C, NetState* S) {
     int32_t* order = S->order;
     if (!order) return;
     __shared__ int s_bin[kOrderBins];
+    __shared__ int s_nbig;
     for (int q = threadIdx.x; q < kOrderBins; q += blockDim.x) s_bin[q] = 0;
+    if (threadIdx.x == 0) s_nbig = 0;
     __syncthreads();
-    auto bin_of = [&](int g) {
-        if (C.state[g] != G_EXISTS) return kOrderBins - 1;
-        const int e = min(max(box_w(S->box_cur[g]), 0), kOrderBins - 2);
-        return kOrderBins - 2 - e;
+    auto bin_from = [](int state, int edge) {
+        return state != G_EXISTS ? kOrderBins - 1 : kOrderBins - 2 - min(max(edge, 0), kOrderBins - 2);
     };
-    for (int g = threadIdx.x + 1; g <= C.N; g += blockDim.x) atomicAdd(&s_bin[bin_of(g)], 1);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int run = 0;
-        for (int q = 0; q < kOrderBins; ++q) {
-            const int c = s_bin[q];
-            s_bin[q] = run;
-            run += c;
+    // counts per bin, and the large-contour corrector's grains (list order is
+    // free); four grains per thread with their loads issued first
+    int32_t* big_flag = S->big_flag;
+    constexpr int kU = 4;
+    for (int g0 = threadIdx.x + 1; g0 <= C.N; g0 += kU * blockDim.x) {
+        int st[kU], bw[kU], cn[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int g = g0 + u * (int)blockDim.x;
+            st[u] = g <= C.N ? C.state[g] : G_GONE;
+            bw[u] = g <= C.N ? box_w(S->box_cur[g]) : 0;
+            cn[u] = g <= C.N && big_flag ? S->cn_prev[g] : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int g = g0 + u * (int)blockDim.x;
+            if (g > C.N) break;
+            atomicAdd(&s_bin[bin_from(st[u], bw[u])], 1);
+            if (big_flag) {
+                const bool big = st[u] == G_EXISTS && cn[u] > kCorrStagedPts;
+                big_flag[g] = big ? 1 : 0;
+                if (big) S->big_list[atomicAdd(&s_nbig, 1)] = g;
+            }
         }
     }
     __syncthreads();
-    for (int g = threadIdx.x + 1; g <= C.N; g += blockDim.x) order[atomicAdd(&s_bin[bin_of(g)], 1)] = g;
+    if (threadIdx.x < 32) {  // exclusive scan of the bins by one warp, 8 per lane
+        constexpr int kPer = kOrderBins / 32;
+        int c[kPer], t = 0;
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            c[k] = s_bin[threadIdx.x * kPer + k];
+            t += c[k];
+        }
+        int incl = t;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if ((int)threadIdx.x >= o) incl += v;
+        }
+        int run = incl - t;
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            s_bin[threadIdx.x * kPer + k] = run;
+            run += c[k];
+        }
+    }
+    __syncthreads();
+    for (int g0 = threadIdx.x + 1; g0 <= C.N; g0 += kU * blockDim.x) {
+        int bin[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int g = g0 + u * (int)blockDim.x;
+            bin[u] = g <= C.N ? bin_from(C.state[g], box_w(S->box_cur[g])) : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int g = g0 + u * (int)blockDim.x;
+            if (g <= C.N) order[atomicAdd(&s_bin[bin[u]], 1)] = g;
+        }
+    }
+    if (threadIdx.x == 0 && big_flag) S->n_big = s_nbig;
 }
 
 // Traffic model: box areas and comparison-list overlaps of existing grains.
