@@ -470,23 +470,28 @@ __device__ int extract_bitmap_warp(const Field<R>& f, const uint32_t* idl, uint3
     const int wpr = (w + 2 + 31) >> 5;
     if (w + 2 > 1024 || (hgt + 2) * wpr + 1 > kBitmapCap) return -1;
     bool nonfinite = false;  // a NaN or infinity anywhere in the field
-    for (int r0 = 0; r0 < hgt + 2; r0 += 8)  // eight rows of loads in flight
-        for (int q = 0; q < wpr; ++q) {
-            const int c = q * 32 + lane - 1;
-            bool in[8];
+    for (int r0 = 0; r0 < hgt + 2; r0 += 8)  // eight rows of two words: 16 loads in flight
+        for (int q0 = 0; q0 < wpr; q0 += 2) {
+            bool in[2][8];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const int r = r0 + u - 1;
-                const bool pix = r >= 0 && r < hgt && c >= 0 && c < w;
-                const double v = pix ? (double)f.v[r * w + c] : 0.0;
-                nonfinite |= !isfinite(v);
-                in[u] = pix && v >= 0;
+            for (int k = 0; k < 2; ++k) {
+                const int c = (q0 + k) * 32 + lane - 1;
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int r = r0 + u - 1;
+                    const bool pix = q0 + k < wpr && r >= 0 && r < hgt && c >= 0 && c < w;
+                    const double v = pix ? (double)f.v[r * w + c] : 0.0;
+                    nonfinite |= !isfinite(v);
+                    in[k][u] = pix && v >= 0;
+                }
             }
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const uint32_t word = __ballot_sync(0xffffffffu, in[u]);
-                if (lane == 0 && r0 + u < hgt + 2) ws.bm[(r0 + u) * wpr + q] = word;
-            }
+            for (int k = 0; k < 2; ++k)
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const uint32_t word = __ballot_sync(0xffffffffu, in[k][u]);
+                    if (lane == 0 && r0 + u < hgt + 2 && q0 + k < wpr) ws.bm[(r0 + u) * wpr + q0 + k] = word;
+                }
         }
     if (lane == 0) ws.bm[(hgt + 2) * wpr] = 0u;
     if (__any_sync(0xffffffffu, nonfinite) && lane == 0) o.status |= S_NAN;
@@ -549,63 +554,118 @@ __device__ int extract_bitmap_warp(const Field<R>& f, const uint32_t* idl, uint3
     if (nsteps < 0) return -1;
     o.status |= __shfl_sync(0xffffffffu, st, 0);
     __syncwarp();
-    // points and junctions of every step, in walk order
+    // points and junctions of every step, in walk order.  Two 32-step
+    // chunks per pass: each lane first issues the field and IDLocal loads of
+    // both its steps (generatePoint's two values, generateJunction's corners),
+    // then evaluates the steps in order.
     const unsigned lt = (1u << lane) - 1u;
     int ne = 0;
     int jn = 0;
     bool point_overflow = false;
-    for (int t0 = 0; t0 < nsteps; t0 += 32) {
-        const int t = t0 + lane;
-        bool emit = false, junc = false;
-        double px = 0, py = 0;
-        uint32_t boxes[4] = {0xFFFFFFu, 0xFFFFFFu, 0xFFFFFFu, 0xFFFFFFu};
-        int order = 0, left = 0, top = 0;
-        if (t < nsteps) {
-            // the step's direction is the move to the next recorded cell
-            const int c = ws.trace[t], cn = ws.trace[t + 1 < nsteps ? t + 1 : 0];
-            const int tr = c / cw, lc = c - tr * cw;
-            left = lc - 1 + b.x0;
-            top = tr - 1 + b.y0;
-            const int mask = cell_mask(ws.bm, wpr, tr, lc);
-            const int dcell = cn - c;
-            const int next = dcell == -cw ? MS_UP : dcell == cw ? MS_DOWN : dcell == -1 ? MS_LEFT : MS_RIGHT;
-            emit = (kMsEmit >> mask) & 1u;
-            const int right = left + 1, bottom = top + 1;
-            if (emit) ms_point(f, next, top, bottom, left, right, &px, &py);
-            if (__popc(mask) < 3 && bottom >= b.y0 && bottom < b.y1 && top >= b.y0 && top < b.y1 &&
-                left >= b.x0 && left < b.x1 && right >= b.x0 && right < b.x1) {  // generateJunction
-                insert_distinct((mask & C_BL) ? own : idl[(bottom - b.y0) * w + (left - b.x0)], boxes, order);
-                insert_distinct((mask & C_TL) ? own : idl[(top - b.y0) * w + (left - b.x0)], boxes, order);
-                insert_distinct((mask & C_BR) ? own : idl[(bottom - b.y0) * w + (right - b.x0)], boxes, order);
-                insert_distinct((mask & C_TR) ? own : idl[(top - b.y0) * w + (right - b.x0)], boxes, order);
+    for (int t0 = 0; t0 < nsteps; t0 += 64) {
+        int mask[2], next[2], left[2], top[2];
+        bool emit[2], pv[2], jv[2];
+        R va[2], vc[2];
+        uint32_t id4[2][4];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int t = t0 + 32 * k + lane;
+            mask[k] = 0;
+            next[k] = MS_UP;
+            left[k] = 0;
+            top[k] = 0;
+            emit[k] = pv[k] = jv[k] = false;
+            va[k] = vc[k] = (R)0;
+            id4[k][0] = id4[k][1] = id4[k][2] = id4[k][3] = own;
+            if (t < nsteps) {
+                // the step's direction is the move to the next recorded cell
+                const int c = ws.trace[t], cn = ws.trace[t + 1 < nsteps ? t + 1 : 0];
+                const int tr = c / cw, lc = c - tr * cw;
+                left[k] = lc - 1 + b.x0;
+                top[k] = tr - 1 + b.y0;
+                const int m = cell_mask(ws.bm, wpr, tr, lc);
+                mask[k] = m;
+                const int dcell = cn - c;
+                const int nx = dcell == -cw ? MS_UP : dcell == cw ? MS_DOWN : dcell == -1 ? MS_LEFT : MS_RIGHT;
+                next[k] = nx;
+                emit[k] = (kMsEmit >> m) & 1u;
+                const int lf = left[k], tp = top[k], right = lf + 1, bottom = tp + 1;
+                // generatePoint's values: a then c, delta = a - c (ms_point)
+                const int ra = nx == MS_RIGHT || nx == MS_UP ? tp : bottom;
+                const int ca = nx == MS_LEFT || nx == MS_UP ? lf : right;
+                const int rc = nx == MS_LEFT ? tp : nx == MS_RIGHT ? bottom : ra;
+                const int cc = nx == MS_UP ? right : nx == MS_DOWN ? lf : ca;
+                pv[k] = nx == MS_LEFT ? tp >= b.y0 : nx == MS_RIGHT ? bottom < b.y1 : nx == MS_UP ? right < b.x1 : lf >= b.x0;
+                if (emit[k] && pv[k]) {
+                    va[k] = f.v[(ra - b.y0) * w + (ca - b.x0)];
+                    vc[k] = f.v[(rc - b.y0) * w + (cc - b.x0)];
+                }
+                jv[k] = __popc(m) < 3 && bottom >= b.y0 && bottom < b.y1 && tp >= b.y0 && tp < b.y1 && lf >= b.x0 &&
+                        lf < b.x1 && right >= b.x0 && right < b.x1;
+                if (jv[k]) {  // generateJunction's corners, in its order
+                    if (!(m & C_BL)) id4[k][0] = idl[(bottom - b.y0) * w + (lf - b.x0)];
+                    if (!(m & C_TL)) id4[k][1] = idl[(tp - b.y0) * w + (lf - b.x0)];
+                    if (!(m & C_BR)) id4[k][2] = idl[(bottom - b.y0) * w + (right - b.x0)];
+                    if (!(m & C_TR)) id4[k][3] = idl[(tp - b.y0) * w + (right - b.x0)];
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int lf = left[k], tp = top[k], right = lf + 1, bottom = tp + 1;
+            double px = 0, py = 0;
+            if (emit[k]) {  // generatePoint (ms_point) on the loaded values
+                const int nx = next[k];
+                if (nx == MS_LEFT) {
+                    px = lf;
+                    py = pv[k] ? bottom - (double)va[k] / ((double)va[k] - (double)vc[k]) : (double)bottom;
+                } else if (nx == MS_RIGHT) {
+                    px = right;
+                    py = pv[k] ? top[k] + (double)va[k] / ((double)va[k] - (double)vc[k]) : (double)tp;
+                } else if (nx == MS_UP) {
+                    py = tp;
+                    px = pv[k] ? lf + (double)va[k] / ((double)va[k] - (double)vc[k]) : (double)lf;
+                } else {
+                    py = bottom;
+                    px = pv[k] ? right - (double)va[k] / ((double)va[k] - (double)vc[k]) : (double)right;
+                }
+            }
+            uint32_t boxes[4] = {0xFFFFFFu, 0xFFFFFFu, 0xFFFFFFu, 0xFFFFFFu};
+            int order = 0;
+            bool junc = false;
+            if (jv[k]) {
+                insert_distinct(id4[k][0], boxes, order);
+                insert_distinct(id4[k][1], boxes, order);
+                insert_distinct(id4[k][2], boxes, order);
+                insert_distinct(id4[k][3], boxes, order);
                 junc = order > 2;
             }
-        }
-        const uint32_t eb = __ballot_sync(0xffffffffu, emit);
-        if (emit) {
-            const int pos = ne + __popc(eb & lt);
-            if (pos < kWalkPts)
-                xy[pos] = make_double2(px, py);
-            else
-                point_overflow = true;
-        }
-        ne += __popc(eb);
-        const uint32_t jb = __ballot_sync(0xffffffffu, junc);
-        if (junc) {
-            const int pos = jn + __popc(jb & lt);
-            if (pos < o.jcap) {
-                Junction& j = o.js[pos];
-                j.type = order;
-                for (int q = 0; q < 4; ++q) j.grains[q] = q < order ? boxes[q] : 0xFFFFFFFFu;
-                j.segment = -1;
-                j.lambda = 0;
-                j.x = left + 0.5;
-                j.y = top + 0.5;
-            } else {
-                o.status |= S_JUNCTION_OVERFLOW;
+            const uint32_t eb = __ballot_sync(0xffffffffu, emit[k]);
+            if (emit[k]) {
+                const int pos = ne + __popc(eb & lt);
+                if (pos < kWalkPts)
+                    xy[pos] = make_double2(px, py);
+                else
+                    point_overflow = true;
             }
+            ne += __popc(eb);
+            const uint32_t jb = __ballot_sync(0xffffffffu, junc);
+            if (junc) {
+                const int pos = jn + __popc(jb & lt);
+                if (pos < o.jcap) {
+                    Junction& j = o.js[pos];
+                    j.type = order;
+                    for (int q = 0; q < 4; ++q) j.grains[q] = q < order ? boxes[q] : 0xFFFFFFFFu;
+                    j.segment = -1;
+                    j.lambda = 0;
+                    j.x = lf + 0.5;
+                    j.y = tp + 0.5;
+                } else {
+                    o.status |= S_JUNCTION_OVERFLOW;
+                }
+            }
+            jn += __popc(jb);
         }
-        jn += __popc(jb);
     }
     if (__any_sync(0xffffffffu, point_overflow)) return -1;
     o.jn = jn < o.jcap ? jn : o.jcap;
