@@ -317,6 +317,42 @@ __device__ __forceinline__ double perimeter_xy(const double2* P, int n, double h
     return p;
 }
 
+// The same two sums for the batched form, whose areas and perimeters need
+// not round as the reference's loop does: each lane adds its own terms, then
+// a tree to lane 0, broadcast (every lane holds the same bits).
+__device__ __forceinline__ double warp_sum_to_all(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return __shfl_sync(0xffffffffu, v, 0);
+}
+
+__device__ __forceinline__ double volume_xy_tree(const double2* P, int n, double h) {
+    double v = 0;
+    for (int i = threadIdx.x & 31; i < n - 1; i += 32) v += (P[i].y + P[i + 1].y) * (P[i].x - P[i + 1].x);
+    return fabs(warp_sum_to_all(v)) * h * h * 0.5;
+}
+
+__device__ __forceinline__ double perimeter_xy_tree(const double2* P, int n, double h) {
+    double p = 0;
+    for (int i = threadIdx.x & 31; i < n - 1; i += 32) {
+        const double dx = P[i].x - P[i + 1].x, dy = P[i].y - P[i + 1].y;
+        p += sqrt(dx * dx + dy * dy) * h;
+    }
+    return warp_sum_to_all(p);
+}
+
+// The level set's sums in the form's rounding: the reference's order in
+// FP64 (plain), the tree in the batched form.
+template <typename R>
+__device__ __forceinline__ double form_volume(const double2* P, int n, double h) {
+    if constexpr (sizeof(R) == 4) return volume_xy_tree(P, n, h);
+    else return volume_xy(P, n, h);
+}
+template <typename R>
+__device__ __forceinline__ double form_perimeter(const double2* P, int n, double h) {
+    if constexpr (sizeof(R) == 4) return perimeter_xy_tree(P, n, h);
+    else return perimeter_xy(P, n, h);
+}
+
 template <typename R>
 __device__ bool clear_area_xy(R* phi, const Box& b, const double2* P, int n, double h) {
     if (n == 0) return true;
@@ -750,7 +786,7 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock, 5) k_levelset_w(NetConst
     if (ok) {
         double newVolume = 0;
         bool regular_motion = true;
-        if (shared) newVolume = volume_xy(xy, o.n, C.h);
+        if (shared) newVolume = form_volume<R>(xy, o.n, C.h);
         if (lane == 0) {
             if (!shared) newVolume = contour_volume(o.pts, o.n, C.h);
             regular_motion = motion_regular(old_len, o.n, C.volume[g], newVolume, C.dt, &irregular);
@@ -766,7 +802,7 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock, 5) k_levelset_w(NetConst
             __syncwarp();
             ok = extract_warp(f, idl, (uint32_t)g, o, lane, xy, &shared, &s_walk[wid]);
             if (!ok) break;
-            if (shared) newVolume = volume_xy(xy, o.n, C.h);
+            if (shared) newVolume = form_volume<R>(xy, o.n, C.h);
             if (lane == 0) {
                 if (!shared) newVolume = contour_volume(o.pts, o.n, C.h);
                 regular_motion = motion_regular(old_len, o.n, C.volume[g], newVolume, C.dt, &irregular);
@@ -790,7 +826,7 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock, 5) k_levelset_w(NetConst
         }
     }
     double perim = 0;
-    if (ok && shared) perim = perimeter_xy(xy, o.n, C.h);
+    if (ok && shared) perim = form_perimeter<R>(xy, o.n, C.h);
     if (ok && !shared && lane == 0) perim = contour_perimeter(o.pts, o.n, C.h);
     if (lane != 0) return;
     if (o.status) set_status(S, o.status);
@@ -848,7 +884,7 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock, 5) k_init_contour_w(NetC
             q.mob = -1.0;
             o.pts[i] = q;
         }
-        vol = volume_xy(xy, o.n, C.h);
+        vol = form_volume<R>(xy, o.n, C.h);
     }
     if (lane != 0) return;
     if (o.status) set_status(S, o.status);
