@@ -915,7 +915,8 @@ constexpr int kNbPts = 512;  // per-warp shared buffers of the neighbour build
 // (src/box.cpp:1201-1228, src/grainBoundary.cpp:85-199), one warp per grain:
 // lanes probe contour points, evaluate the per-pair physics and the terms of
 // the area and energy sums into shared memory; lane 0 builds the neighbour
-// list and adds the terms in contour order (the reference's order).
+// list and adds the terms in contour order (the reference's order; the
+// batched form sums by trees instead).
 template <typename R>
 __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_neighbours_w(NetConst C, NetState* S, PointInfo* scratch) {
     __shared__ int s_cid[kGrainsPerBlock][kNbPts];
@@ -939,14 +940,20 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_neighbours_w(NetConst 
     auto CID = [&](int q) -> int& { return sh ? s_cid[wid][q] : info[q].cid; };
     auto LEN = [&](int q) -> double& { return sh ? s_len[wid][q] : info[q].len; };
     // area (computeVolume, src/grainBoundary.cpp:201-213): terms side by side,
-    // added in contour order
+    // added in contour order (plain) or by a tree (batched, as the sums below)
+    constexpr bool kTree = sizeof(R) == sizeof(float);
     double v = 0;
-    for (int i0 = 0; i0 < n - 1; i0 += 32) {
-        const int i = i0 + lane;
-        double t = 0;
-        if (i < n - 1) t = (P[i].y + P[i + 1].y) * (P[i].x - P[i + 1].x);
-        const int m = n - 1 - i0 < 32 ? n - 1 - i0 : 32;
-        for (int q = 0; q < m; ++q) v += __shfl_sync(FULL, t, q);
+    if constexpr (kTree) {
+        for (int i = lane; i < n - 1; i += 32) v += (P[i].y + P[i + 1].y) * (P[i].x - P[i + 1].x);
+        v = warp_sum_to_all(v);
+    } else {
+        for (int i0 = 0; i0 < n - 1; i0 += 32) {
+            const int i = i0 + lane;
+            double t = 0;
+            if (i < n - 1) t = (P[i].y + P[i + 1].y) * (P[i].x - P[i + 1].x);
+            const int m = n - 1 - i0 < 32 ? n - 1 - i0 : 32;
+            for (int q = 0; q < m; ++q) v += __shfl_sync(FULL, t, q);
+        }
     }
     const double newVolume = fabs(fabs(v) * h * h * 0.5);
     // probes; the first failing point ends the reference's loop
@@ -998,9 +1005,14 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_neighbours_w(NetConst 
             }
             term = len * energy * h;
         }
-        const int m = n - 1 - i0 < 32 ? n - 1 - i0 : 32;
-        for (int q = 0; q < m; ++q) energy_sum += __shfl_sync(FULL, term, q);
+        if constexpr (kTree) {
+            energy_sum += term;
+        } else {
+            const int m = n - 1 - i0 < 32 ? n - 1 - i0 : 32;
+            for (int q = 0; q < m; ++q) energy_sum += __shfl_sync(FULL, term, q);
+        }
     }
+    if constexpr (kTree) energy_sum = warp_sum_to_all(energy_sum);
     __syncwarp();
     // neighbour list in first-occurrence order (one entry per distinct
     // neighbour, at most `cap`; later new neighbours are dropped), then each
@@ -1028,11 +1040,27 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_neighbours_w(NetConst 
         __syncwarp();
     }
     Neighbour* nb = C.nb + (int64_t)g * C.nbmax;
+    __shared__ double s_nlen[kGrainsPerBlock][48];
+    if constexpr (kTree) {  // each neighbour's length by the whole warp
+        for (int e = 0; e < nn; ++e) {
+            const int cid = s_nid[wid][e];
+            double len = 0;
+            for (int i = lane; i < upto; i += 32)
+                if (CID(i) == cid) len += LEN(i);
+            len = warp_sum_to_all(len);
+            if (lane == 0) s_nlen[wid][e] = len;
+        }
+        __syncwarp();
+    }
     for (int e = lane; e < nn; e += 32) {
         const int cid = s_nid[wid][e];
         double len = 0;
-        for (int i = 0; i < upto; ++i)
-            if (CID(i) == cid) len += LEN(i);
+        if constexpr (kTree) {
+            len = s_nlen[wid][e];
+        } else {
+            for (int i = 0; i < upto; ++i)
+                if (CID(i) == cid) len += LEN(i);
+        }
         const double theta = grain_misorientation(qg, C.quat + 4 * (int64_t)cid);
         nb[e].id = cid;
         nb[e].length = len;
