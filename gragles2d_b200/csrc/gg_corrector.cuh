@@ -685,8 +685,11 @@ __device__ void prepare_sectors_view(const NetConst& C, NetState* S, int g, cons
     junction_weights(C, J, nj, g, jw, s_st);
     __syncthreads();
     if (threadIdx.x < 32) {
+        // the perimeter only bounds the sector walks (lap_guard): a tree sum
         double per = 0;
-        for (int k = 0; k < size - 1; ++k) per += seg[k];
+        for (int k = threadIdx.x; k < size - 1; k += 32) per += seg[k];
+        for (int o = 16; o > 0; o >>= 1) per += __shfl_down_sync(0xffffffffu, per, o);
+        per = __shfl_sync(0xffffffffu, per, 0);
         if (threadIdx.x == 0) *s_per = per;
         build_sectors_warp(C, T, P, seg, per, size, J, nj, idl, ib, sec, jw, jl, jr);
         if (threadIdx.x == 0 && (sec.status | *s_st)) set_status(S, sec.status | *s_st);
