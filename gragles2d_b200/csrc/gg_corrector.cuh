@@ -146,76 +146,84 @@ __device__ __forceinline__ double table_weight_at(const NbTable& T, const uint32
 
 // GrainJunction::getWeight (src/junction.cpp:23-192), mode 4, ResearchMode 0,
 // ResearchProject 0, no twin identification, for every junction of grain
-// `me`: one warp per junction.  Lanes 0-2 evaluate the three grain pairs
-// (me-n0, n0-n1, me-n1) side by side and the warp scans n0's characteristics
-// for n1 together; lane 0 then combines the terms in the reference's order,
+// `me`: a group of three lanes per junction, ten junctions per warp at once.
+// The group's lanes evaluate the three grain pairs (me-n0, n0-n1, me-n1) side
+// by side, the second one also finding n1 in n0's characteristics (first
+// match); the first lane then combines the terms in the reference's order,
 // so each weight is the value the sequential routine computes.
 __device__ void junction_weights(const NetConst& C, const Junction* J, int nj, int me, double* jw,
                                  uint32_t* s_status) {
-    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    for (int q = threadIdx.x >> 5; q < nj; q += nw) {
-        const int type = J[q].type;
-        uint32_t nbr[4] = {0xFFFFFFu, 0xFFFFFFu, 0xFFFFFFu, 0xFFFFFFu};
-        for (int i = 0, j = 0; i < type && i < 4; i++) {
-            const uint32_t gi = J[q].grains[i];
-            if ((uint32_t)me != gi) {
-                nbr[j] = gi;
-                j++;
-            }
-        }
-        if (nbr[0] == 0xFFFFFFu || nbr[1] == 0xFFFFFFu) {
-            if (lane == 0) jw[q] = 1;
-            continue;
-        }
-        const int n0 = (int)nbr[0], n1 = (int)nbr[1];
-        if (n0 > C.N || n1 > C.N) {
-            if (lane == 0) {
-                jw[q] = 1;
-                atomicOr(s_status, S_INDEX);
-            }
-            continue;
-        }
-        // characteristics of n1 in n0's list (find_characteristic, first match)
-        bool c01_ok = !(n1 != 0 && C.state[n1] == G_GONE) && n0 != 0;
-        double c01_mob = 1.0;
-        if (c01_ok) {
-            const Neighbour* nb = C.nb + (int64_t)n0 * C.nbmax;
-            const int n = C.nb_n[n0];
-            int first = -1;
-            for (int e0 = 0; e0 < n && first < 0; e0 += 32) {
-                const int e = e0 + lane;
-                const unsigned hit = __ballot_sync(0xffffffffu, e < n && nb[e].id == n1);
-                if (hit) first = e0 + __ffs(hit) - 1;
-            }
-            if (first >= 0) c01_mob = nb[first].mobility;
-        }
-        double mob = 0, gam = 0;
-        if (lane < 3) {
-            const double* pa = C.quat + 4 * (int64_t)(lane == 1 ? n0 : me);
-            const double* pb = C.quat + 4 * (int64_t)(lane == 0 ? n0 : n1);
-            const double theta = grain_misorientation(pa, pb);
-            gam = read_shockley(theta, C);
-            mob = lane == 1 ? c01_mob : mobility_model(theta, C);
-        }
-        const double m1 = __shfl_sync(0xffffffffu, mob, 1), m2 = __shfl_sync(0xffffffffu, mob, 2);
-        const double g1 = __shfl_sync(0xffffffffu, gam, 1), g2 = __shfl_sync(0xffffffffu, gam, 2);
-        if (lane == 0) {
-            if ((n0 != 0 && C.state[n0] == G_GONE) || (n1 != 0 && C.state[n1] == G_GONE))
-                atomicOr(s_status, S_INDEX);
-            double averageMobility = 0;
-            averageMobility += mob;
-            averageMobility += m1;
-            averageMobility += m2;
-            double sigma = gam - g1 + g2;
-            if (!C.isotropic) {
-                if (C.use_mobility_model > 0 && C.tpd > 0) {
-                    averageMobility /= 3;
-                    const double drag = 1 / ((1 / (C.ds * C.tpd)) + 1 / averageMobility);
-                    sigma *= drag;
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int grp = lane / 3, role = lane - 3 * grp;  // lanes 30 and 31 have no junction
+    for (int q0 = warp * 10; q0 < nj; q0 += nw * 10) {
+        const int q = q0 + grp;
+        const bool act = grp < 10 && q < nj;
+        int n0 = 0, n1 = 0;
+        bool missing = true, bad_index = false;
+        if (act) {
+            const int type = J[q].type;
+            uint32_t nbr[4] = {0xFFFFFFu, 0xFFFFFFu, 0xFFFFFFu, 0xFFFFFFu};
+            for (int i = 0, j = 0; i < type && i < 4; i++) {
+                const uint32_t gi = J[q].grains[i];
+                if ((uint32_t)me != gi) {
+                    nbr[j] = gi;
+                    j++;
                 }
             }
-            if (sigma < 0.01) sigma = 0.01;
-            jw[q] = sigma;
+            missing = nbr[0] == 0xFFFFFFu || nbr[1] == 0xFFFFFFu;
+            if (!missing) {
+                n0 = (int)nbr[0];
+                n1 = (int)nbr[1];
+                bad_index = n0 > C.N || n1 > C.N;
+            }
+        }
+        double mob = 0, gam = 0;
+        if (act && !missing && !bad_index) {
+            double c01_mob = 1.0;
+            if (role == 1 && !(n1 != 0 && C.state[n1] == G_GONE) && n0 != 0) {
+                // characteristics of n1 in n0's list (find_characteristic, first match)
+                const Neighbour* nb = C.nb + (int64_t)n0 * C.nbmax;
+                const int n = C.nb_n[n0];
+                for (int e = 0; e < n; ++e)
+                    if (nb[e].id == n1) {
+                        c01_mob = nb[e].mobility;
+                        break;
+                    }
+            }
+            const double* pa = C.quat + 4 * (int64_t)(role == 1 ? n0 : me);
+            const double* pb = C.quat + 4 * (int64_t)(role == 0 ? n0 : n1);
+            const double theta = grain_misorientation(pa, pb);
+            gam = read_shockley(theta, C);
+            mob = role == 1 ? c01_mob : mobility_model(theta, C);
+        }
+        const int l1 = lane + 1 < 32 ? lane + 1 : 31, l2 = lane + 2 < 32 ? lane + 2 : 31;
+        const double m1 = __shfl_sync(FULL, mob, l1), m2 = __shfl_sync(FULL, mob, l2);
+        const double g1 = __shfl_sync(FULL, gam, l1), g2 = __shfl_sync(FULL, gam, l2);
+        if (act && role == 0) {
+            if (missing) {
+                jw[q] = 1;
+            } else if (bad_index) {
+                jw[q] = 1;
+                atomicOr(s_status, S_INDEX);
+            } else {
+                if ((n0 != 0 && C.state[n0] == G_GONE) || (n1 != 0 && C.state[n1] == G_GONE))
+                    atomicOr(s_status, S_INDEX);
+                double averageMobility = 0;
+                averageMobility += mob;
+                averageMobility += m1;
+                averageMobility += m2;
+                double sigma = gam - g1 + g2;
+                if (!C.isotropic) {
+                    if (C.use_mobility_model > 0 && C.tpd > 0) {
+                        averageMobility /= 3;
+                        const double drag = 1 / ((1 / (C.ds * C.tpd)) + 1 / averageMobility);
+                        sigma *= drag;
+                    }
+                }
+                if (sigma < 0.01) sigma = 0.01;
+                jw[q] = sigma;
+            }
         }
     }
 }
