@@ -488,13 +488,14 @@ __global__ void __launch_bounds__(1024) k_alloc(NetConst C, NetState* S, int spe
     const int slots = N + 1;
     const int run = ((slots + nw - 1) / nw + 31) & ~31;
     const int r0 = warp * run, r1 = min(slots, r0 + run);
-    auto sizes = [&](int g, int64_t* a, int64_t* sp, int64_t* c, int* cc, bool* range) {
+    // sizes of slot g from its state and new box (loaded first: kU slots of
+    // 32 per warp have their loads in flight together)
+    auto sizes = [&](bool live, const Box& bx, int64_t* a, int64_t* sp, int64_t* c, int* cc, bool* range) {
         *a = 0;
         *sp = 0;
         *c = 0;
         *cc = 0;
-        if (g >= 1 && g <= N && C.state[g] == G_EXISTS) {
-            const Box bx = S->box_new[g];
+        if (live) {
             const int n = box_w(bx);
             *a = box_area(bx);
             *sp = (int64_t)spec_per_complex * 2 * (int64_t)n * (n / 2 + 1);
@@ -503,15 +504,28 @@ __global__ void __launch_bounds__(1024) k_alloc(NetConst C, NetState* S, int spe
             if (n > C.tmax) *range = true;
         }
     };
+    constexpr int kU = 4;
+    auto load = [&](int g, bool* live, Box* bx) {
+        const bool in = g >= 1 && g <= N && g < r1;
+        *live = in && C.state[g] == G_EXISTS;
+        *bx = in ? S->box_new[g] : Box{0, 0, 0, 0};
+    };
     bool range = false;
     int64_t ta = 0, ts = 0, tc = 0;
-    for (int g0 = r0; g0 < r1; g0 += 32) {
-        int64_t a, sp, c;
-        int cc;
-        sizes(g0 + lane < r1 ? g0 + lane : -1, &a, &sp, &c, &cc, &range);
-        ta += a;
-        ts += sp;
-        tc += c;
+    for (int g0 = r0; g0 < r1; g0 += 32 * kU) {
+        bool live[kU];
+        Box bx[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) load(g0 + 32 * u + lane, &live[u], &bx[u]);
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            int64_t a, sp, c;
+            int cc;
+            sizes(live[u], bx[u], &a, &sp, &c, &cc, &range);
+            ta += a;
+            ts += sp;
+            tc += c;
+        }
     }
     for (int o = 16; o > 0; o >>= 1) {
         ta += __shfl_xor_sync(0xffffffffu, ta, o);
@@ -545,30 +559,39 @@ __global__ void __launch_bounds__(1024) k_alloc(NetConst C, NetState* S, int spe
     }
     __syncthreads();
     int64_t ba = s_base[warp][0], bs = s_base[warp][1], bc = s_base[warp][2];
-    for (int g0 = r0; g0 < r1; g0 += 32) {
-        const int g = g0 + lane;
-        int64_t a, sp, c;
-        int cc;
-        sizes(g < r1 ? g : -1, &a, &sp, &c, &cc, &range);
-        int64_t ia = a, is = sp, ic = c;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int64_t ua = __shfl_up_sync(0xffffffffu, ia, o), us = __shfl_up_sync(0xffffffffu, is, o),
-                          uc = __shfl_up_sync(0xffffffffu, ic, o);
-            if (lane >= o) {
-                ia += ua;
-                is += us;
-                ic += uc;
+    for (int g00 = r0; g00 < r1; g00 += 32 * kU) {
+        bool live[kU];
+        Box bx[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) load(g00 + 32 * u + lane, &live[u], &bx[u]);
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int g0 = g00 + 32 * u;
+            if (g0 >= r1) break;  // uniform over the warp
+            const int g = g0 + lane;
+            int64_t a, sp, c;
+            int cc;
+            sizes(live[u], bx[u], &a, &sp, &c, &cc, &range);
+            int64_t ia = a, is = sp, ic = c;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int64_t ua = __shfl_up_sync(0xffffffffu, ia, o), us = __shfl_up_sync(0xffffffffu, is, o),
+                              uc = __shfl_up_sync(0xffffffffu, ic, o);
+                if (lane >= o) {
+                    ia += ua;
+                    is += us;
+                    ic += uc;
+                }
             }
+            if (g < r1) {
+                S->off_new[g] = ba + ia - a;
+                S->soff_new[g] = bs + is - sp;
+                S->coff_new[g] = bc + ic - c;
+                S->ccap_new[g] = cc;
+            }
+            ba += __shfl_sync(0xffffffffu, ia, 31);
+            bs += __shfl_sync(0xffffffffu, is, 31);
+            bc += __shfl_sync(0xffffffffu, ic, 31);
         }
-        if (g < r1) {
-            S->off_new[g] = ba + ia - a;
-            S->soff_new[g] = bs + is - sp;
-            S->coff_new[g] = bc + ic - c;
-            S->ccap_new[g] = cc;
-        }
-        ba += __shfl_sync(0xffffffffu, ia, 31);
-        bs += __shfl_sync(0xffffffffu, is, 31);
-        bc += __shfl_sync(0xffffffffu, ic, 31);
     }
     if (range) set_status(S, S_TABLE_RANGE);
 }
