@@ -814,11 +814,22 @@ __global__ void __launch_bounds__(1024) k_finalize(NetConst C, NetState* S, int 
     __shared__ double s_max[32];
     int cnt = 0;
     double mx = 0.0;
-    for (int g = threadIdx.x + 1; g <= C.N; g += blockDim.x) {
-        if (C.state[g] != G_GONE) {
-            cnt++;
-            mx = fmax(mx, C.volume[g]);
+    constexpr int kU = 4;  // four grains' state and volume loads in flight
+    for (int g0 = threadIdx.x + 1; g0 <= C.N; g0 += kU * blockDim.x) {
+        int st[kU];
+        double vol[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int g = g0 + u * (int)blockDim.x;
+            st[u] = g <= C.N ? C.state[g] : G_GONE;
+            vol[u] = g <= C.N ? C.volume[g] : 0.0;
         }
+#pragma unroll
+        for (int u = 0; u < kU; ++u)
+            if (st[u] != G_GONE) {
+                cnt++;
+                mx = fmax(mx, vol[u]);
+            }
     }
     for (int o = 16; o > 0; o >>= 1) {
         cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
