@@ -33,6 +33,35 @@ struct DevBuf {
     size_t bytes = 0;
 };
 
+// Page-locked host buffers kept by the process for its next contexts, as the
+// device memory pool keeps device memory: page-locking costs milliseconds, so
+// a context takes the smallest free buffer that is large enough (else
+// allocates one, portable to every device) and gives it back when destroyed.
+std::mutex g_pinned_mutex;
+std::vector<DevBuf> g_pinned_free;
+
+cudaError_t pinned_take(void** out, size_t bytes) {
+    {
+        std::lock_guard<std::mutex> lock(g_pinned_mutex);
+        int best = -1;
+        for (int i = 0; i < (int)g_pinned_free.size(); ++i)
+            if (g_pinned_free[i].bytes >= bytes && (best < 0 || g_pinned_free[i].bytes < g_pinned_free[best].bytes))
+                best = i;
+        if (best >= 0) {
+            *out = g_pinned_free[best].p;
+            g_pinned_free.erase(g_pinned_free.begin() + best);
+            return cudaSuccess;
+        }
+    }
+    return cudaHostAlloc(out, bytes, cudaHostAllocPortable);
+}
+
+void pinned_give(void* p, size_t bytes) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(g_pinned_mutex);
+    g_pinned_free.push_back(DevBuf{p, bytes});
+}
+
 }  // namespace
 
 struct gg_ctx {
@@ -69,6 +98,7 @@ struct gg_ctx {
     std::vector<void*> allocs;
     gg_grain_stats* d_stats = nullptr;  // packed statistics (device) and their pinned host copy
     gg_grain_stats* h_stats = nullptr;
+    size_t h_stats_bytes = 0;
     // statistics prefetch: once a caller has read the statistics, every
     // gg_step gathers them and copies them, with the status word, into
     // pinned memory after its timed region; a read with nothing changed since
@@ -94,8 +124,8 @@ struct gg_ctx {
             for (void* p : allocs) cudaFreeAsync(p, stream);  // back to the library's pool
             cudaStreamSynchronize(stream);
         }
-        if (h_stats) cudaFreeHost(h_stats);
-        if (h_status) cudaFreeHost(h_status);
+        pinned_give(h_stats, h_stats_bytes);  // to the process's pinned buffers
+        pinned_give(h_status, sizeof(uint32_t));
         if (ev_done) cudaEventDestroy(ev_done);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -1666,10 +1696,10 @@ int gg_step(gg_ctx* c, int32_t loop, int32_t nsteps) {
         }
         GG_CUDA(c, cudaEventRecord(c->ev1, c->stream));
     }
-    if (c->stats_wanted) {
+    if (c->stats_wanted && c->d_stats && c->h_stats) {
         // after the timed region: the statistics and the status word in one
         // pinned copy each, then one wait for all of it
-        if (!c->h_status) GG_CUDA(c, cudaMallocHost(&c->h_status, sizeof(uint32_t)));
+        if (!c->h_status) GG_CUDA(c, pinned_take(reinterpret_cast<void**>(&c->h_status), sizeof(uint32_t)));
         if (!c->ev_done) GG_CUDA(c, cudaEventCreateWithFlags(&c->ev_done, cudaEventDisableTiming));
         GG_CUDA(c, pack_stats(c->C, c->dS, c->d_stats, c->stream));
         GG_CUDA(c, cudaMemcpyAsync(c->h_stats, c->d_stats, sizeof(gg_grain_stats) * (size_t)c->N,
@@ -2031,7 +2061,10 @@ int gg_read_grain_stats(gg_ctx* c, gg_grain_stats* out, int32_t capacity) {
     if (!c->d_stats) {
         int rc = dalloc(c, &c->d_stats, (size_t)N);
         if (rc) return rc;
-        GG_CUDA(c, cudaMallocHost(&c->h_stats, sizeof(gg_grain_stats) * (size_t)(N > 0 ? N : 1)));
+    }
+    if (!c->h_stats) {
+        c->h_stats_bytes = sizeof(gg_grain_stats) * (size_t)(N > 0 ? N : 1);
+        GG_CUDA(c, pinned_take(reinterpret_cast<void**>(&c->h_stats), c->h_stats_bytes));
     }
     GG_CUDA(c, pack_stats(c->C, c->dS, c->d_stats, c->stream));
     GG_CUDA(c, cudaMemcpyAsync(c->h_stats, c->d_stats, sizeof(gg_grain_stats) * (size_t)N, cudaMemcpyDeviceToHost,
