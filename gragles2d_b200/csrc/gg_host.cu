@@ -14,6 +14,8 @@
 #include <cstring>
 #include <fstream>
 #include <mutex>
+#include <system_error>
+#include <thread>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -185,8 +187,12 @@ int library_pool(gg_ctx* c, cudaMemPool_t* out) {
     return GG_OK;
 }
 
+// Device memory from the library's pool, zero-filled unless `zero` is false
+// (arenas whose every read is of a value a kernel wrote before: fields read
+// inside the boxes they were written for, contour data up to the written
+// counts).
 template <typename T>
-int dalloc(gg_ctx* c, T** out, size_t count) {
+int dalloc(gg_ctx* c, T** out, size_t count, bool zero = true) {
     void* p = nullptr;
     const size_t bytes = sizeof(T) * (count > 0 ? count : 1);
     cudaMemPool_t pool = nullptr;
@@ -194,7 +200,7 @@ int dalloc(gg_ctx* c, T** out, size_t count) {
     if (rc) return rc;
     cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, pool, c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaMallocFromPoolAsync");
-    e = cudaMemsetAsync(p, 0, bytes, c->stream);
+    e = zero ? cudaMemsetAsync(p, 0, bytes, c->stream) : cudaSuccess;
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaMemset");
     c->allocs.push_back(p);
     *out = reinterpret_cast<T*>(p);
@@ -1060,13 +1066,37 @@ int gg_distance_initialisation(gg_ctx* c) {
     // (src/box.cpp:112)
     c->quat.assign(4 * (size_t)(c->N + 1), 0.0);
     c->quat[0] = 1.0;
-    for (int g = 1; g <= c->N; ++g) {
-        double* q = &c->quat[4 * (size_t)g];
-        if (poly)
-            for (int k = 0; k < 4; ++k) q[k] = c->poly_quat[4 * (size_t)(g - 1) + k];
-        else
-            euler2quaternion(&c->euler[3 * (size_t)(g - 1)], q);
+    auto convert = [c, poly](int g0, int g1) {
+        for (int g = g0; g < g1; ++g) {
+            double* q = &c->quat[4 * (size_t)g];
+            if (poly)
+                for (int k = 0; k < 4; ++k) q[k] = c->poly_quat[4 * (size_t)(g - 1) + k];
+            else
+                euler2quaternion(&c->euler[3 * (size_t)(g - 1)], q);
+        }
+    };
+    // each grain's conversion is independent (six trigonometric calls): large
+    // inputs are split over up to 8 host threads, the same calls per grain
+    const int nthreads =
+        c->N >= 4096 ? (int)std::min(8u, std::max(1u, std::thread::hardware_concurrency())) : 1;
+    bool converted = false;
+    if (nthreads > 1) {
+        std::vector<std::thread> workers;
+        try {
+            const int per = (c->N + nthreads - 1) / nthreads;
+            for (int t = 0; t < nthreads; ++t) {
+                const int g0 = 1 + t * per, g1 = std::min(c->N + 1, g0 + per);
+                if (g0 < g1) workers.emplace_back(convert, g0, g1);
+            }
+            converted = true;
+        } catch (const std::system_error&) {
+            converted = false;  // no threads: the rest below, on this one
+        }
+        for (std::thread& w : workers) w.join();
+        if (!converted) convert(1, c->N + 1);
+        converted = true;
     }
+    if (!converted) convert(1, c->N + 1);
     auto present = [&](int g) {
         return poly ? c->poly_off[g] > c->poly_off[g - 1] : c->bbox[5 * (size_t)(g - 1) + 4] != 0;
     };
@@ -1257,6 +1287,8 @@ int gg_distance_initialisation(gg_ctx* c) {
     int rc;
 #define ALLOC(ptr, cnt) \
     if ((rc = dalloc(c, &(ptr), (cnt))) != GG_OK) return rc
+#define ALLOC_UNZEROED(ptr, cnt) \
+    if ((rc = dalloc(c, &(ptr), (cnt), false)) != GG_OK) return rc
     ALLOC(C.state, N + 1);
     ALLOC(C.regular, N + 1);
     ALLOC(C.inter_bnd, N + 1);
@@ -1372,9 +1404,9 @@ int gg_distance_initialisation(gg_ctx* c) {
         }
     } else {
         float *pa, *pb, *sp_;
-        ALLOC(pa, phi_cap);
-        ALLOC(pb, phi_cap);
-        ALLOC(sp_, spec_cap);
+        ALLOC_UNZEROED(pa, phi_cap);  // fields and the convolution's scratch: read only inside written boxes
+        ALLOC_UNZEROED(pb, phi_cap);
+        ALLOC_UNZEROED(sp_, spec_cap);
         S.phiA = pa;
         S.phiB = pb;
         S.spec = sp_;
@@ -1389,12 +1421,12 @@ int gg_distance_initialisation(gg_ctx* c) {
     (void)rsz;
     ALLOC(S.idPrev, phi_cap);
     ALLOC(S.idCur, phi_cap);
-    ALLOC(S.contPrev, cont_cap);
-    ALLOC(S.contCur, cont_cap);
-    ALLOC(S.segPrev, cont_cap);
+    ALLOC_UNZEROED(S.contPrev, cont_cap);  // contour data: read up to the written counts
+    ALLOC_UNZEROED(S.contCur, cont_cap);
+    ALLOC_UNZEROED(S.segPrev, cont_cap);
     {
         double* pt;
-        ALLOC(pt, 4 * (size_t)cont_cap);  // PointInfo: 32 bytes per contour point
+        ALLOC_UNZEROED(pt, 4 * (size_t)cont_cap);  // PointInfo: 32 bytes per contour point
         C.ptinfo = pt;
     }
     ALLOC(S.cn_prev, N + 1);
@@ -1413,6 +1445,7 @@ int gg_distance_initialisation(gg_ctx* c) {
     ALLOC(c->dS, 1);
 
 #undef ALLOC
+#undef ALLOC_UNZEROED
 
     // initial per-grain data
     const std::vector<double>& quat = c->quat;
