@@ -224,6 +224,18 @@ struct NetState {
     int32_t* big_list;
 };
 
+// The initial neighbour search's grid of grain bins (kNeighbourBin cells a
+// side, nc x nc of them): counts, starts (nc * nc + 1) and the binned grain
+// IDs, with the total written back for the host to size `items`.
+constexpr int kNeighbourBin = 64;
+struct NeighbourBins {
+    int nc;
+    int* count;
+    int* start;
+    int* items;
+    int* total;
+};
+
 // Contour points the main batched corrector stages in shared memory; longer
 // contours go to the large-contour corrector.
 constexpr int kCorrStagedPts = 512;

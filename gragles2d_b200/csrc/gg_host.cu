@@ -98,6 +98,13 @@ struct gg_ctx {
     NetState* dS = nullptr;
     int32_t* d_ids = nullptr;     // ID field of the loaded microstructure (device)
     std::vector<void*> allocs;
+    // bins of the initial neighbour search (from the pool, kept for later calls)
+    int* nbin_count = nullptr;
+    int* nbin_start = nullptr;
+    int* nbin_total = nullptr;
+    int* nbin_items = nullptr;
+    int nbin_nc = 0;
+    int64_t nbin_items_cap = 0;
     gg_grain_stats* d_stats = nullptr;  // packed statistics (device) and their pinned host copy
     gg_grain_stats* h_stats = nullptr;
     size_t h_stats_bytes = 0;
@@ -1516,7 +1523,27 @@ int gg_find_neighbors(gg_ctx* c) {
     c->stats_fresh = false;
     if (!c->initialised) return fail(c, GG_E_STATE, "not initialised");
     c->sectors_stale = c->P.precision != GG_PRECISION_PLAIN;  // junction weights read the neighbour lists
-    GG_CUDA(c, find_neighbors_launch(c->C, c->dS, c->stream));
+    // the grains binned by the cells their boxes cover: counts and starts,
+    // then the binned IDs, sized by the count read back
+    const int nc = c->C.m / kNeighbourBin + 1;
+    int rc;
+    if (nc > c->nbin_nc) {
+        if ((rc = dalloc(c, &c->nbin_count, (size_t)nc * nc)) != GG_OK) return rc;
+        if ((rc = dalloc(c, &c->nbin_start, (size_t)nc * nc + 1)) != GG_OK) return rc;
+        if ((rc = dalloc(c, &c->nbin_total, 1)) != GG_OK) return rc;
+        c->nbin_nc = nc;
+    }
+    NeighbourBins B{nc, c->nbin_count, c->nbin_start, c->nbin_items, c->nbin_total};
+    GG_CUDA(c, neighbour_bins_count(c->C, c->dS, B, c->stream));
+    int total = 0;
+    GG_CUDA(c, cudaMemcpyAsync(&total, c->nbin_total, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    GG_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (total > c->nbin_items_cap || !c->nbin_items) {
+        if ((rc = dalloc(c, &c->nbin_items, (size_t)std::max(total, 1))) != GG_OK) return rc;
+        c->nbin_items_cap = std::max(total, 1);
+    }
+    B.items = c->nbin_items;
+    GG_CUDA(c, find_neighbors_launch(c->C, c->dS, B, c->stream));
     return check_status(c);
 }
 

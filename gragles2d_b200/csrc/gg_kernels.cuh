@@ -1117,14 +1117,48 @@ __global__ void __launch_bounds__(256) k_polygon_phi(NetConst C, NetState* S) {
 // grainhdl::find_neighbors + LSbox::computeDirectNeighbours
 // (src/grainhdl.cpp:1258-1283, src/box.cpp:2220-2237): every other grain whose
 // closed box overlaps (RTree::Overlap, src/RTree.h:1092-1105), ascending ID.
-// One warp per grain: the lanes test 32 consecutive IDs at a time (coalesced
-// box loads) and a ballot keeps the hits in ascending order.
+// The grains are first binned by the kNeighbourBin x kNeighbourBin cells
+// their boxes cover; a warp per grain then tests the grains of its own cells,
+// keeping an overlapping pair only in the cell that holds the lower-left
+// corner of the two boxes' overlap (so each pair once), and ranks its hits
+// into ascending order.  A grain with more than kFindCandidates hits tests
+// every grain instead, 32 consecutive IDs at a time.
 constexpr int kFindWarps = 4;
+constexpr int kFindCandidates = 256;
 
-__global__ void __launch_bounds__(32 * kFindWarps) k_find_neighbors(NetConst C, NetState* S) {
-    const int lane = threadIdx.x & 31;
-    const int g = blockIdx.x * kFindWarps + (threadIdx.x >> 5) + 1;
-    if (g > C.N || C.state[g] == G_GONE) return;
+__device__ __forceinline__ bool boxes_overlap_closed(const Box& a, const Box& b) {
+    return !(a.x0 > b.x1 || b.x0 > a.x1 || a.y0 > b.y1 || b.y0 > a.y1);
+}
+
+__device__ __forceinline__ int bin_of(int v, int nc) { return min(max(v / kNeighbourBin, 0), nc - 1); }
+
+// Writes grain g's list of ns hits (ids[0 .. min(ns, kmax)), ascending) as
+// the reference's find_neighbors leaves it: comparison list, direct
+// neighbours with zero characteristics, no comparison members yet.
+__device__ void write_neighbour_list(const NetConst& C, NetState* S, int g, const int* ids, int ns, int lane) {
+    int* sec = C.sec_ids + (int64_t)g * C.kmax;
+    Neighbour* nb = C.nb + (int64_t)g * C.nbmax;
+    for (int pos = lane; pos < ns; pos += 32) {
+        const int k = ids[pos];
+        if (pos < C.kmax) sec[pos] = k;
+        if (pos < C.nbmax) {
+            nb[pos].id = k;
+            nb[pos].length = 0;
+            nb[pos].energy = 0;
+            nb[pos].misori = 0;
+            nb[pos].mobility = 0;
+        }
+    }
+    if (lane == 0) {
+        C.sec_n[g] = ns < C.kmax ? ns : C.kmax;
+        C.cmp_n[g] = 0;
+        C.nb_n[g] = ns < C.nbmax ? ns : C.nbmax;
+        if (ns > C.kmax) set_status(S, S_LIST_OVERFLOW);
+    }
+}
+
+// Every grain tested, in ID order (the fallback).
+__device__ void find_neighbors_scan(const NetConst& C, NetState* S, int g, int lane) {
     const Box a = S->box_cur[g];
     int ns = 0;
     bool overflow = false;
@@ -1133,10 +1167,7 @@ __global__ void __launch_bounds__(32 * kFindWarps) k_find_neighbors(NetConst C, 
     for (int k0 = 1; k0 <= C.N; k0 += 32) {
         const int k = k0 + lane;
         bool hit = false;
-        if (k <= C.N && k != g && C.state[k] != G_GONE) {
-            const Box b = S->box_cur[k];
-            hit = !(a.x0 > b.x1 || b.x0 > a.x1 || a.y0 > b.y1 || b.y0 > a.y1);
-        }
+        if (k <= C.N && k != g && C.state[k] != G_GONE) hit = boxes_overlap_closed(a, S->box_cur[k]);
         const unsigned mask = __ballot_sync(0xffffffffu, hit);
         if (hit) {
             const int pos = ns + __popc(mask & ((1u << lane) - 1u));
@@ -1158,6 +1189,111 @@ __global__ void __launch_bounds__(32 * kFindWarps) k_find_neighbors(NetConst C, 
         C.nb_n[g] = ns < C.nbmax ? ns : C.nbmax;
         if (overflow) set_status(S, S_LIST_OVERFLOW);
     }
+}
+
+// Bins: count, then (after the scan) fill, the grains of every cell.
+__global__ void k_bin_grains(NetConst C, NetState* S, NeighbourBins B, int fill) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (g > C.N || C.state[g] == G_GONE) return;
+    const Box a = S->box_cur[g];
+    const int cx0 = bin_of(a.x0, B.nc), cx1 = bin_of(a.x1, B.nc), cy0 = bin_of(a.y0, B.nc), cy1 = bin_of(a.y1, B.nc);
+    for (int cy = cy0; cy <= cy1; ++cy)
+        for (int cx = cx0; cx <= cx1; ++cx) {
+            const int c = cy * B.nc + cx;
+            const int pos = atomicAdd(&B.count[c], 1);
+            if (fill) B.items[B.start[c] + pos] = g;
+        }
+}
+
+// Exclusive scan of the cell counts into starts (start[ncell] = total), the
+// counts reset for the fill; one CTA.
+__global__ void __launch_bounds__(1024) k_bin_scan(NeighbourBins B) {
+    __shared__ int s_warp[32];
+    __shared__ int s_run;
+    const int ncell = B.nc * B.nc;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (threadIdx.x == 0) s_run = 0;
+    __syncthreads();
+    for (int base = 0; base < ncell; base += blockDim.x) {
+        const int c = base + (int)threadIdx.x;
+        const int v = c < ncell ? B.count[c] : 0;
+        int incl = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += u;
+        }
+        if (lane == 31) s_warp[warp] = incl;
+        __syncthreads();
+        int before = s_run;
+        for (int w = 0; w < warp; ++w) before += s_warp[w];
+        if (c < ncell) {
+            B.start[c] = before + incl - v;
+            B.count[c] = 0;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int t = 0;
+            for (int w = 0; w < nw; ++w) t += s_warp[w];
+            s_run += t;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        B.start[ncell] = s_run;
+        *B.total = s_run;
+    }
+}
+
+__global__ void __launch_bounds__(32 * kFindWarps) k_find_neighbors(NetConst C, NetState* S, NeighbourBins B) {
+    __shared__ int s_hit[kFindWarps][kFindCandidates];
+    __shared__ int s_ord[kFindWarps][kFindCandidates];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int g = blockIdx.x * kFindWarps + wid + 1;
+    if (g > C.N || C.state[g] == G_GONE) return;
+    const Box a = S->box_cur[g];
+    const int nc = B.nc;
+    const int cx0 = bin_of(a.x0, nc), cx1 = bin_of(a.x1, nc), cy0 = bin_of(a.y0, nc), cy1 = bin_of(a.y1, nc);
+    int* hit_ids = s_hit[wid];
+    int n = 0;
+    for (int cy = cy0; cy <= cy1; ++cy)
+        for (int cx = cx0; cx <= cx1; ++cx) {
+            const int c = cy * nc + cx;
+            const int q1 = B.start[c + 1];
+            for (int q0 = B.start[c]; q0 < q1; q0 += 32) {
+                const int q = q0 + lane;
+                int k = 0;
+                bool hit = false;
+                if (q < q1) {
+                    k = B.items[q];
+                    if (k != g) {
+                        const Box b = S->box_cur[k];
+                        hit = boxes_overlap_closed(a, b) &&
+                              bin_of(max(a.y0, b.y0), nc) * nc + bin_of(max(a.x0, b.x0), nc) == c;
+                    }
+                }
+                const unsigned mask = __ballot_sync(0xffffffffu, hit);
+                if (hit) {
+                    const int pos = n + __popc(mask & ((1u << lane) - 1u));
+                    if (pos < kFindCandidates) hit_ids[pos] = k;
+                }
+                n += __popc(mask);
+            }
+        }
+    __syncwarp();
+    if (n > kFindCandidates) {  // uniform over the warp
+        find_neighbors_scan(C, S, g, lane);
+        return;
+    }
+    // ascending ID: each hit's rank among the (distinct) hits
+    int* ord = s_ord[wid];
+    for (int i = lane; i < n; i += 32) {
+        const int v = hit_ids[i];
+        int r = 0;
+        for (int j = 0; j < n; ++j) r += hit_ids[j] < v;
+        ord[r] = v;
+    }
+    __syncwarp();
+    write_neighbour_list(C, S, g, ord, n, lane);
 }
 
 }  // namespace

@@ -58,7 +58,10 @@ cudaError_t plain_resample(const NetConst& C, NetState* dS, double h_old, double
 cudaError_t batched_resample(const NetConst& C, NetState* dS, double h_old, double hn, double delta_old,
                              cudaStream_t s);
 cudaError_t swap_phi(NetState* dS, cudaStream_t s);
-cudaError_t find_neighbors_launch(const NetConst& C, NetState* dS, cudaStream_t s);
+// Counts and scans the bins (stream-ordered; *B.total set on the device).
+cudaError_t neighbour_bins_count(const NetConst& C, NetState* dS, const NeighbourBins& B, cudaStream_t s);
+// Fills the bins (B.items sized for the total) and runs the search.
+cudaError_t find_neighbors_launch(const NetConst& C, NetState* dS, const NeighbourBins& B, cudaStream_t s);
 cudaError_t traffic_launch(const NetConst& C, NetState* dS, cudaStream_t s);
 // One launch of a single stage kernel (index 0..8 as in GG_NSTAGES order).
 cudaError_t plain_stage_kernel(const NetConst& C, NetState* dS, int which, cudaStream_t s, const LaunchCfg& cfg);

@@ -62,8 +62,18 @@ cudaError_t finalize_only(const NetConst& C, NetState* dS, int rotate, cudaStrea
     return cudaGetLastError();
 }
 
-cudaError_t find_neighbors_launch(const NetConst& C, NetState* dS, cudaStream_t s) {
-    k_find_neighbors<<<(C.N + kFindWarps - 1) / kFindWarps, 32 * kFindWarps, 0, s>>>(C, dS);
+cudaError_t neighbour_bins_count(const NetConst& C, NetState* dS, const NeighbourBins& B, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(B.count, 0, sizeof(int) * (size_t)B.nc * B.nc, s);
+    if (e != cudaSuccess) return e;
+    if (C.N > 0) k_bin_grains<<<(C.N + 255) / 256, 256, 0, s>>>(C, dS, B, 0);
+    k_bin_scan<<<1, 1024, 0, s>>>(B);
+    return cudaGetLastError();
+}
+
+cudaError_t find_neighbors_launch(const NetConst& C, NetState* dS, const NeighbourBins& B, cudaStream_t s) {
+    if (C.N <= 0) return cudaSuccess;
+    k_bin_grains<<<(C.N + 255) / 256, 256, 0, s>>>(C, dS, B, 1);
+    k_find_neighbors<<<(C.N + kFindWarps - 1) / kFindWarps, 32 * kFindWarps, 0, s>>>(C, dS, B);
     return cudaGetLastError();
 }
 
