@@ -986,34 +986,6 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_neighbours_w(NetConst 
     first_bad = warp_min_i(first_bad);
     const int upto = first_bad < n - 1 ? first_bad : n - 1;
     __syncwarp();
-    // physics of the points before the first failure; energy terms of all
-    // points, added in contour order (computeEnergy, src/grainBoundary.cpp:215-222)
-    double energy_sum = 0;
-    for (int i0 = 0; i0 < n - 1; i0 += 32) {
-        const int i = i0 + lane;
-        double term = 0;
-        if (i < n - 1) {
-            const double dx = P[i].x - P[i + 1].x, dy = P[i].y - P[i + 1].y;
-            const double len = sqrt(dx * dx + dy * dy);
-            double energy = -1.0;  // generatePoint's value, kept where the loop never reached
-            if (i < upto) {
-                const double theta = grain_misorientation(qg, C.quat + 4 * (int64_t)CID(i));
-                P[i].mob = mobility_model(theta, C);
-                energy = read_shockley(theta, C);
-                P[i].energy = energy;
-                LEN(i) = len * h;
-            }
-            term = len * energy * h;
-        }
-        if constexpr (kTree) {
-            energy_sum += term;
-        } else {
-            const int m = n - 1 - i0 < 32 ? n - 1 - i0 : 32;
-            for (int q = 0; q < m; ++q) energy_sum += __shfl_sync(FULL, term, q);
-        }
-    }
-    if constexpr (kTree) energy_sum = warp_sum_to_all(energy_sum);
-    __syncwarp();
     // neighbour list in first-occurrence order (one entry per distinct
     // neighbour, at most `cap`; later new neighbours are dropped), then each
     // entry's length summed over its points in contour order
@@ -1039,6 +1011,55 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_neighbours_w(NetConst 
         nn = min(nn + __popc(fb), cap);
         __syncwarp();
     }
+    // each listed neighbour's misorientation, energy and mobility, once
+    __shared__ double s_nth[kGrainsPerBlock][48], s_nen[kGrainsPerBlock][48], s_nmob[kGrainsPerBlock][48];
+    for (int e = lane; e < nn; e += 32) {
+        const double theta = grain_misorientation(qg, C.quat + 4 * (int64_t)s_nid[wid][e]);
+        s_nth[wid][e] = theta;
+        s_nen[wid][e] = read_shockley(theta, C);
+        s_nmob[wid][e] = mobility_model(theta, C);
+    }
+    __syncwarp();
+    // physics of the points before the first failure; energy terms of all
+    // points, added in contour order (computeEnergy, src/grainBoundary.cpp:215-222)
+    double energy_sum = 0;
+    for (int i0 = 0; i0 < n - 1; i0 += 32) {
+        const int i = i0 + lane;
+        double term = 0;
+        if (i < n - 1) {
+            const double dx = P[i].x - P[i + 1].x, dy = P[i].y - P[i + 1].y;
+            const double len = sqrt(dx * dx + dy * dy);
+            double energy = -1.0;  // generatePoint's value, kept where the loop never reached
+            if (i < upto) {
+                // the neighbour's physics, evaluated once per neighbour above
+                // (the same calls on the same orientations)
+                const int cid = CID(i);
+                int e = 0;
+                while (e < nn && s_nid[wid][e] != cid) ++e;
+                double mob;
+                if (e < nn) {
+                    mob = s_nmob[wid][e];
+                    energy = s_nen[wid][e];
+                } else {  // beyond the list's capacity
+                    const double theta = grain_misorientation(qg, C.quat + 4 * (int64_t)cid);
+                    mob = mobility_model(theta, C);
+                    energy = read_shockley(theta, C);
+                }
+                P[i].mob = mob;
+                P[i].energy = energy;
+                LEN(i) = len * h;
+            }
+            term = len * energy * h;
+        }
+        if constexpr (kTree) {
+            energy_sum += term;
+        } else {
+            const int m = n - 1 - i0 < 32 ? n - 1 - i0 : 32;
+            for (int q = 0; q < m; ++q) energy_sum += __shfl_sync(FULL, term, q);
+        }
+    }
+    if constexpr (kTree) energy_sum = warp_sum_to_all(energy_sum);
+    __syncwarp();
     Neighbour* nb = C.nb + (int64_t)g * C.nbmax;
     __shared__ double s_nlen[kGrainsPerBlock][48];
     if constexpr (kTree) {  // each neighbour's length by the whole warp
@@ -1061,12 +1082,11 @@ __global__ void __launch_bounds__(32 * kGrainsPerBlock) k_neighbours_w(NetConst 
             for (int i = 0; i < upto; ++i)
                 if (CID(i) == cid) len += LEN(i);
         }
-        const double theta = grain_misorientation(qg, C.quat + 4 * (int64_t)cid);
         nb[e].id = cid;
         nb[e].length = len;
-        nb[e].energy = read_shockley(theta, C);
-        nb[e].misori = theta;
-        nb[e].mobility = mobility_model(theta, C);
+        nb[e].energy = s_nen[wid][e];
+        nb[e].misori = s_nth[wid][e];
+        nb[e].mobility = s_nmob[wid][e];
     }
     if (lane != 0) return;
     C.nb_n[g] = nn;
