@@ -220,10 +220,11 @@ __device__ __forceinline__ int bucket_of(const VertexBuckets<kPts>& B, double lx
     return cy * B.ncx + cx;
 }
 
-// All threads: buckets of the vertices 0 .. npts-1 (P[k] in grid
-// coordinates, origin (ox, oy)).  Ends with a barrier.
+// All threads: buckets of the vertices 0 .. npts-1 from their staged FP32
+// box-local coordinates P32 (each within 2^-24 L of the exact one, far inside
+// the search's 1e-3 cell margin).  Ends with a barrier.
 template <int kPts>
-__device__ void build_buckets(VertexBuckets<kPts>& B, const CPoint* P, int npts, int ox, int oy, int wi, int hi) {
+__device__ void build_buckets(VertexBuckets<kPts>& B, const float2* P32, int npts, int wi, int hi) {
     const int cs = max(4, (max(wi, hi) + kCellMax - 1) / kCellMax);
     const int ncx = (wi + cs - 1) / cs, ncy = (hi + cs - 1) / cs, nc = ncx * ncy;
     if (threadIdx.x == 0) {
@@ -234,7 +235,7 @@ __device__ void build_buckets(VertexBuckets<kPts>& B, const CPoint* P, int npts,
     for (int c = threadIdx.x; c <= nc; c += blockDim.x) B.end[c] = 0;
     __syncthreads();
     for (int k = threadIdx.x; k < npts; k += blockDim.x)
-        atomicAdd(&B.end[bucket_of(B, P[k].x - ox, P[k].y - oy) + 1], 1);
+        atomicAdd(&B.end[bucket_of(B, (double)P32[k].x, (double)P32[k].y) + 1], 1);
     __syncthreads();
     if (threadIdx.x < 32) {  // inclusive scan of the counts by one warp
         int carry = 0;
@@ -251,7 +252,7 @@ __device__ void build_buckets(VertexBuckets<kPts>& B, const CPoint* P, int npts,
     }
     __syncthreads();
     for (int k = threadIdx.x; k < npts; k += blockDim.x) {
-        const int pos = atomicSub(&B.end[bucket_of(B, P[k].x - ox, P[k].y - oy) + 1], 1) - 1;
+        const int pos = atomicSub(&B.end[bucket_of(B, (double)P32[k].x, (double)P32[k].y) + 1], 1) - 1;
         B.list[pos] = (short)k;
     }
     __syncthreads();
@@ -515,7 +516,7 @@ __device__ __forceinline__ void correct_grain(const NetConst& C, NetState* S, in
         tacc = s_acc;
     }
     build_nb_table(C, g, nbt);
-    if (staged) build_buckets(vb, P, size - 1, ox, oy, box_w(ib), box_h(ib));  // ends with a barrier
+    if (staged) build_buckets(vb, sp, size - 1, box_w(ib), box_h(ib));  // ends with a barrier
     __syncthreads();
     const Box bo = S->box_cur[g];
     const int x0 = ib.x0 < bo.x0 ? bo.x0 : ib.x0;

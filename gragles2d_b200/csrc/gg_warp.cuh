@@ -516,9 +516,9 @@ __device__ int extract_bitmap_warp(const Field<R>& f, const uint32_t* idl, uint3
                 for (int u = 0; u < 8; ++u) {
                     const int r = r0 + u - 1;
                     const bool pix = q0 + k < wpr && r >= 0 && r < hgt && c >= 0 && c < w;
-                    const double v = pix ? (double)f.v[r * w + c] : 0.0;
+                    const R v = pix ? f.v[r * w + c] : (R)0;  // tested in the field's own type
                     nonfinite |= !isfinite(v);
-                    in[k][u] = pix && v >= 0;
+                    in[k][u] = pix && v >= (R)0;
                 }
             }
 #pragma unroll
