@@ -126,7 +126,7 @@ def test_calibration_loss_gradient(base, golden_dir):
 
 def test_batched_fp32_loss_gradient_against_the_fp64_tangents(base, golden_dir):
     """The gradient error of the batched FP32 form: central differences of
-    its calibration loss with h = 1e-4 relative (north_star's step) against
+    its calibration loss with a step of 1e-4 relative to each parameter against
     the FP64 tangent gradient of the same loss, within 5e-3 relative for
     every parameter [measured 0.9e-3 .. 1.6e-3; FP64 central differences at
     the same h: <= 2.5e-7, and 1.8e-3 for HAGB_RelativeEnergy, where that
