@@ -168,10 +168,16 @@ extern "C" int gg_convolve_box_static(const double* d_in, double* d_out, int32_t
                                       int32_t real_domain_size, void* stream) {
     if (n < 1 || n > kMaxN) return GG_E_INVALID;
     if (!d_in || !d_out || real_domain_size < 1 || !(dt > 0)) return GG_E_INVALID;
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // A call copies its tables from this stack frame and waits for the
+    // stream, neither of which a stream capture admits: a capturing stream
+    // is refused before anything is issued on it, so the capture stays valid.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) return cuda_error();
+    if (cap != cudaStreamCaptureStatusNone) return GG_E_INVALID;
     double* scratch = nullptr;
     const int rc = scratch_on_device(&scratch);
     if (rc != GG_OK) return rc;
-    const cudaStream_t s = static_cast<cudaStream_t>(stream);
     // Tables for this n, built on the host stack (no heap allocation) and
     // copied into the scratch; every value the kernel reads is rewritten by
     // this call, so nothing has to be cleared between calls.

@@ -354,9 +354,10 @@ int gg_kernel_launches(gg_ctx* ctx, int64_t* total, int32_t* per_step);
  * It calls no cudaMalloc, cudaFree or allocating library routine: its scratch
  * is a fixed array of about 300 KB compiled into the library, which every GPU
  * that loads the library holds until the process exits.  n must be in
- * 1..GG_STATIC_CONV_MAX_N, else GG_E_INVALID is returned.  The first call on
- * a device looks up the scratch's device address (once per device), so that
- * first call must come before any stream capture.  All calls on a device share
+ * 1..GG_STATIC_CONV_MAX_N, else GG_E_INVALID is returned.  No call can be
+ * captured into a CUDA graph (each copies its tables from host memory and
+ * waits for the stream): on a capturing stream it returns GG_E_INVALID and
+ * issues nothing, so the capture stays valid.  All calls on a device share
  * the one scratch array, so calls that overlap on the GPU (from several host
  * threads or streams) race; serialise them.
  */

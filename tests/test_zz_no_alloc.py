@@ -165,3 +165,40 @@ def test_static_box_convolution_known_answer_at_the_size_limits(n):
         got = dst.cpu().numpy()
         np.testing.assert_allclose(got, want, rtol=0, atol=1e-12)
 
+
+
+@pytest.mark.gpu
+def test_static_box_convolution_refuses_a_capturing_stream():
+    """A call on a stream that is being captured into a CUDA graph returns
+    GG_E_INVALID and issues nothing there: the capture around it completes,
+    its graph replays, and a call after the capture succeeds."""
+    import torch
+
+    from gragles2d_b200 import gg
+
+    gg.load_library()  # loaded before the capture starts
+    n = 8
+    src = torch.from_numpy(np.random.default_rng(5).uniform(-1.0, 1.0, (n, n))).cuda()
+    dst = torch.zeros_like(src)
+    x = torch.arange(16, dtype=torch.float64, device="cuda")
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        y = x * 2.0
+    torch.cuda.current_stream().wait_stream(side)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        y = x * 2.0
+        with pytest.raises(gg.GGError) as e:
+            gg.convolve_box_static(src.data_ptr(), dst.data_ptr(), n, 3.125e-6, 800,
+                                   stream=torch.cuda.current_stream().cuda_stream)
+        assert e.value.code == 1
+    x.add_(1.0)
+    graph.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(y, (x * 2.0))
+    assert torch.count_nonzero(dst).item() == 0
+    gg.convolve_box_static(src.data_ptr(), dst.data_ptr(), n, 3.125e-6, 800)
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(dst.cpu().numpy(), _gaussian_convolution(src.cpu().numpy(), 3.125e-6, 800),
+                               rtol=0, atol=1e-12)
