@@ -47,6 +47,29 @@ __device__ __forceinline__ void band_ranges(int c0, int n, int R, int* s0, int* 
     }
 }
 
+// The taps of band_ranges as one walk of the same length for every strip of
+// a box, so that the lanes of a warp run one loop together (the row pass,
+// whose strips differ within a warp): the walk starts at c' = *first and
+// wraps from n - 1 to 0, *taps steps, with the kernel window starting at kx
+// index *base.  In a banded box every strip starts at R + n - 1, one period
+// of k_n above the first range's index when that range wraps; kx holds k_n
+// periodically below index 2n - 1, so every stored output meets the same
+// kernel values in the same order as over the two ranges (the window's
+// extra entries past the row end feed only the unstored outputs of a last,
+// partial strip).
+__device__ __forceinline__ void band_walk(int c0, int n, int R, int* first, int* taps, int* base) {
+    if (2 * R + kSepStrip >= n) {
+        *first = 0;
+        *taps = n;
+        *base = c0 + n - 1;
+        return;
+    }
+    const int lo = c0 - R;
+    *first = lo < 0 ? lo + n : lo;
+    *taps = 2 * R + kSepStrip;
+    *base = R + n - 1;
+}
+
 // rows: two rows per thread share each kernel window load
 __device__ __forceinline__ void sep_pass_rows(const float* __restrict__ X, float* __restrict__ T,
                                               const float* __restrict__ kx, int n, int R) {
@@ -59,28 +82,26 @@ __device__ __forceinline__ void sep_pass_rows(const float* __restrict__ X, float
         const float* xa = X + r * n;
         const float* xb = two ? xa + n : xa;
         float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f, b0 = 0.f, b1 = 0.f, b2 = 0.f, b3 = 0.f;
-        int rs[2], re[2];
-        band_ranges(c0, n, R, &rs[0], &re[0], &rs[1], &re[1]);
-        for (int q = 0; q < 2; ++q) {
-            int base = c0 + n - 1 - rs[q];  // kx index of (c0 - c') at c' = rs[q]
-            float w0 = kx[base], w1 = kx[base + 1], w2 = kx[base + 2], w3 = kx[base + 3];
+        int cp, taps, base;
+        band_walk(c0, n, R, &cp, &taps, &base);
+        float w0 = kx[base], w1 = kx[base + 1], w2 = kx[base + 2], w3 = kx[base + 3];
 #pragma unroll 4
-            for (int cp = rs[q]; cp < re[q]; ++cp) {
-                const float x = xa[cp], y = xb[cp];
-                a0 = fmaf(x, w0, a0);
-                a1 = fmaf(x, w1, a1);
-                a2 = fmaf(x, w2, a2);
-                a3 = fmaf(x, w3, a3);
-                b0 = fmaf(y, w0, b0);
-                b1 = fmaf(y, w1, b1);
-                b2 = fmaf(y, w2, b2);
-                b3 = fmaf(y, w3, b3);
-                --base;
-                w3 = w2;
-                w2 = w1;
-                w1 = w0;
-                w0 = kx[base];
-            }
+        for (int k = 0; k < taps; ++k) {
+            const float x = xa[cp], y = xb[cp];
+            a0 = fmaf(x, w0, a0);
+            a1 = fmaf(x, w1, a1);
+            a2 = fmaf(x, w2, a2);
+            a3 = fmaf(x, w3, a3);
+            b0 = fmaf(y, w0, b0);
+            b1 = fmaf(y, w1, b1);
+            b2 = fmaf(y, w2, b2);
+            b3 = fmaf(y, w3, b3);
+            cp = cp + 1 == n ? 0 : cp + 1;
+            --base;
+            w3 = w2;
+            w2 = w1;
+            w1 = w0;
+            w0 = kx[base];
         }
         float* ta = T + r * n + c0;
         ta[0] = a0;
