@@ -17,10 +17,11 @@ constexpr int kSepStrip = 4;       // outputs per thread along the convolution a
 // (src/box.cpp:674-687, G(i2, j2) = g(i2) g(j2) / n^2).  One CTA per grain.
 // The kernel is laid out once as kx[j] = k_n[(j - (n-1)) mod n], j < 2n-1
 // (zero-padded), so output c of a row is sum_c' X[c'] kx[c - c' + n - 1]:
-// each thread accumulates a strip of 4 consecutive outputs while a 4-entry
-// register window slides down kx (one shared-memory load per 4 FMAs).  Taps
-// farther than R (circularly) from the strip are left out: the host sets R
-// so that every dropped k_n entry is below 2^-26 k_n[0].
+// each thread accumulates strips of 4 consecutive outputs of two rows (or
+// columns) while a 4-entry register window slides down kx (one shared-memory
+// load of the kernel per 8 FMAs).  Taps farther than R (circularly) from the
+// strip are left out: the host sets R so that every dropped k_n entry is
+// below 2^-26 k_n[0].
 
 // The (at most two) index ranges of c' within circular distance R of the
 // strip [c0, c0 + 4), as [s0, e0) and [s1, e1).
@@ -118,12 +119,16 @@ __device__ __forceinline__ void sep_pass_rows(const float* __restrict__ X, float
     }
 }
 
+// columns: columns c and c + ceil(n/2) per thread share each kernel window load
 __device__ __forceinline__ void sep_pass_cols(const float* __restrict__ T, float* __restrict__ out,
                                               const float* __restrict__ kx, int n, int R) {
     const int nb = (n + kSepStrip - 1) / kSepStrip;
-    for (int t = threadIdx.x; t < n * nb; t += blockDim.x) {
-        const int rb = t / n, c = t - rb * n, r0 = rb * kSepStrip;
-        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+    const int half = (n + 1) >> 1;
+    for (int t = threadIdx.x; t < half * nb; t += blockDim.x) {
+        const int rb = t / half, c = t - rb * half, r0 = rb * kSepStrip;
+        const bool two = c + half < n;
+        const int c2 = two ? c + half : c;
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f, b0 = 0.f, b1 = 0.f, b2 = 0.f, b3 = 0.f;
         int rs[2], re[2];
         band_ranges(r0, n, R, &rs[0], &re[0], &rs[1], &re[1]);
         for (int q = 0; q < 2; ++q) {
@@ -131,11 +136,15 @@ __device__ __forceinline__ void sep_pass_cols(const float* __restrict__ T, float
             float w0 = kx[base], w1 = kx[base + 1], w2 = kx[base + 2], w3 = kx[base + 3];
 #pragma unroll 4
             for (int rp = rs[q]; rp < re[q]; ++rp) {
-                const float x = T[rp * n + c];
+                const float x = T[rp * n + c], y = T[rp * n + c2];
                 a0 = fmaf(w0, x, a0);
                 a1 = fmaf(w1, x, a1);
                 a2 = fmaf(w2, x, a2);
                 a3 = fmaf(w3, x, a3);
+                b0 = fmaf(w0, y, b0);
+                b1 = fmaf(w1, y, b1);
+                b2 = fmaf(w2, y, b2);
+                b3 = fmaf(w3, y, b3);
                 --base;
                 w3 = w2;
                 w2 = w1;
@@ -147,6 +156,12 @@ __device__ __forceinline__ void sep_pass_cols(const float* __restrict__ T, float
         if (r0 + 1 < n) out[(r0 + 1) * n + c] = a1;
         if (r0 + 2 < n) out[(r0 + 2) * n + c] = a2;
         if (r0 + 3 < n) out[(r0 + 3) * n + c] = a3;
+        if (two) {
+            out[r0 * n + c2] = b0;
+            if (r0 + 1 < n) out[(r0 + 1) * n + c2] = b1;
+            if (r0 + 2 < n) out[(r0 + 2) * n + c2] = b2;
+            if (r0 + 3 < n) out[(r0 + 3) * n + c2] = b3;
+        }
     }
 }
 
